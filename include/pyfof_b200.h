@@ -1,0 +1,90 @@
+/*
+ * libpyfof_b200 -- C-ABI of the B200 friends-of-friends + unbinding library.
+ *
+ * The library replaces the compiled extension module `fof_fortran` of
+ * py_fof.  Its main entry point pyfof_run() has the argument list and the
+ * error codes of the f2py binding of
+ *     subroutine fof_fortran(xp_halo, vp_halo, mp_halo, np_halo, nhalo, L_Box,
+ *        linking_length, np_halo_min, bound_check, verbose, softening, a_val,
+ *        b_val, s_15_val, n_threads, total_np, in_halo, halo_id, ang_mom,
+ *        ierr, ng_val, ng_global_val)          (fof_fortran.f90:10-58)
+ * as called by _fof_core (py_fof/__init__.py:331-336), with the intent(out)
+ * arrays passed in by the caller and ierr returned.
+ *
+ * Error codes (py_fof/__init__.py:338-348): 0 ok, 1 invalid input or
+ * configuration, 2 candidate span exceeds s_15, 3 allocation failure,
+ * 4 non-finite values, 10 n_threads > 256, 20 CUDA runtime failure.
+ * pyfof_last_error() returns a message for the calling thread's last error.
+ *
+ * All pointers are plain host pointers unless the function name says
+ * "device".  The caller owns every buffer; nothing is retained after return.
+ * Calls on one device are serialised internally; the library keeps device
+ * memory cached between calls.
+ */
+#ifndef PYFOF_B200_H
+#define PYFOF_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PYFOF_B200_ABI_VERSION 1
+
+/* Memory layout of the (3,N) float64 coordinate/velocity arrays. */
+#define PYFOF_LAYOUT_AOS 0 /* Fortran order, x[3*i+d]: the f2py xp_halo layout */
+#define PYFOF_LAYOUT_SOA 1 /* C order,       x[d*N+i]: numpy hstack output */
+
+/* ABI version of the loaded library (PYFOF_B200_ABI_VERSION). */
+int32_t pyfof_version(void);
+
+/* Select the CUDA device used by later calls and create its context.
+ * No reference counterpart (the reference is a CPU module). */
+int32_t pyfof_init(int32_t device);
+
+/* Release all device contexts and cached device memory. */
+int32_t pyfof_shutdown(void);
+
+/* Copies the calling thread's last error message into buf (NUL-terminated,
+ * truncated to len) and returns its full length. */
+int32_t pyfof_last_error(char *buf, int64_t len);
+
+/* Library options: "unbind_fp64" (1 = plain FP64 unbinding path, 0 = FP32
+ * product path), "timing" (1 = record stage times). */
+int32_t pyfof_set_option(const char *key, int64_t value);
+
+/* Device time of the linking kernel of the last call, when timing is on. */
+int32_t pyfof_last_link_ms(float *ms);
+
+/* Replaces fof_fortran.fof_fortran (fof_fortran.f90:10-58).
+ *   xp, vp    (3,total_np) float64 in `layout`; vp may be NULL (all zero,
+ *             the value _fof_core passes when vp_list is None,
+ *             py_fof/__init__.py:233), but not when bound_check != 0
+ *   mp        (total_np) float64, NULL means unit masses
+ *   np_halo   (nhalo) particle count of every input region
+ *   in_halo, halo_id  (total_np) int32 outputs; ang_mom (3,nhalo) float64
+ *             Fortran order (ang_mom[3*h+d]) output
+ * Returns ierr. */
+int32_t pyfof_run(const double *xp, const double *vp, const double *mp, int32_t layout,
+                  const int32_t *np_halo, int32_t nhalo, int64_t total_np, double L_Box,
+                  double linking_length, int32_t np_halo_min, int32_t bound_check,
+                  int32_t verbose, double softening, double a_val, double b_val,
+                  double s_15_val, int32_t n_threads, int64_t ng_val, double ng_global_val,
+                  int32_t *in_halo, int32_t *halo_id, double *ang_mom);
+
+/* Same as pyfof_run with xp/vp/mp/in_halo/halo_id in device memory of the
+ * selected device (np_halo and ang_mom stay on the host).  The inputs must
+ * be complete before the call (synchronise the producing stream). */
+int32_t pyfof_run_device(const double *d_xp, const double *d_vp, const double *d_mp,
+                         int32_t layout, const int32_t *np_halo, int32_t nhalo, int64_t total_np,
+                         double L_Box, double linking_length, int32_t np_halo_min,
+                         int32_t bound_check, int32_t verbose, double softening, double a_val,
+                         double b_val, double s_15_val, int32_t n_threads, int64_t ng_val,
+                         double ng_global_val, int32_t *d_in_halo, int32_t *d_halo_id,
+                         double *ang_mom);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,146 @@
+"""ctypes binding of libpyfof_b200.so (declarations in include/pyfof_b200.h).
+
+The shared library is built in place by ``python -m py_fof_b200.build``.
+There is no fallback: if the library is missing or cannot be loaded, every
+call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpyfof_b200.so")
+ABI_VERSION = 1
+LAYOUT_AOS = 0
+LAYOUT_SOA = 1
+
+_lib = None
+_lock = threading.Lock()
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+
+_RUN_ARGS = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, _i32p,
+             ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
+             ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+             ctypes.c_double, ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p,
+             ctypes.c_void_p, _dp]
+
+# every symbol include/pyfof_b200.h declares
+EXPORTED = ("pyfof_version", "pyfof_init", "pyfof_shutdown", "pyfof_last_error",
+            "pyfof_set_option", "pyfof_last_link_ms", "pyfof_run", "pyfof_run_device")
+
+
+class NativeLibraryError(RuntimeError):
+    pass
+
+
+def load():
+    """Load the library (once) and declare the C-ABI signatures."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise NativeLibraryError(
+                f"{LIB_PATH} is missing; build it with `python -m py_fof_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        L.pyfof_version.restype = ctypes.c_int32
+        L.pyfof_init.restype = ctypes.c_int32
+        L.pyfof_init.argtypes = [ctypes.c_int32]
+        L.pyfof_shutdown.restype = ctypes.c_int32
+        L.pyfof_last_error.restype = ctypes.c_int32
+        L.pyfof_last_error.argtypes = [ctypes.c_char_p, ctypes.c_int64]
+        L.pyfof_set_option.restype = ctypes.c_int32
+        L.pyfof_set_option.argtypes = [ctypes.c_char_p, ctypes.c_int64]
+        L.pyfof_last_link_ms.restype = ctypes.c_int32
+        L.pyfof_last_link_ms.argtypes = [ctypes.POINTER(ctypes.c_float)]
+        L.pyfof_run.restype = ctypes.c_int32
+        L.pyfof_run.argtypes = _RUN_ARGS
+        L.pyfof_run_device.restype = ctypes.c_int32
+        L.pyfof_run_device.argtypes = _RUN_ARGS
+        v = L.pyfof_version()
+        if v != ABI_VERSION:
+            raise NativeLibraryError(f"ABI version mismatch: library {v}, binding {ABI_VERSION}")
+        _lib = L
+        return L
+
+
+def last_error() -> str:
+    L = load()
+    buf = ctypes.create_string_buffer(2048)
+    L.pyfof_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def set_option(key: str, value: int) -> None:
+    if load().pyfof_set_option(key.encode(), int(value)) != 0:
+        raise ValueError(last_error())
+
+
+def last_link_ms() -> float:
+    v = ctypes.c_float(0.0)
+    load().pyfof_last_link_ms(ctypes.byref(v))
+    return float(v.value)
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def run(xp, vp, mp, np_halo, nhalo, L_Box, link, np_halo_min, bound_check, verbose, softening,
+        a_val, b_val, s_15_val, n_threads, total_np, ng_val=256, ng_global_val=512.0):
+    """Host-memory call with the f2py argument order of fof_fortran.fof_fortran.
+
+    xp, vp: (3,N) float64 arrays, C- or Fortran-contiguous (vp may be None);
+    mp: (N,) float64 or None.  Returns (in_halo, halo_id, ang_mom, ierr).
+    """
+    L = load()
+    n = int(total_np)
+    if xp.flags.c_contiguous:
+        layout = LAYOUT_SOA
+    elif xp.flags.f_contiguous:
+        layout = LAYOUT_AOS
+    else:
+        xp = np.ascontiguousarray(xp)
+        layout = LAYOUT_SOA
+    if vp is not None:
+        vp = np.asarray(vp, dtype=np.float64)
+        vp = np.ascontiguousarray(vp) if layout == LAYOUT_SOA else np.asfortranarray(vp)
+    if mp is not None:
+        mp = np.ascontiguousarray(mp, dtype=np.float64)
+    nph = np.ascontiguousarray(np_halo, dtype=np.int32)
+    in_halo = np.zeros(n, dtype=np.int32)
+    halo_id = np.zeros(n, dtype=np.int32)
+    ang_mom = np.zeros((3, max(int(nhalo), 0)), dtype=np.float64, order="F")
+    ierr = L.pyfof_run(_ptr(xp), _ptr(vp), _ptr(mp), layout, nph.ctypes.data_as(_i32p),
+                       int(nhalo), n, float(L_Box), float(link), int(np_halo_min),
+                       int(bound_check), int(verbose), float(softening), float(a_val),
+                       float(b_val), float(s_15_val), int(n_threads), int(ng_val),
+                       float(ng_global_val), _ptr(in_halo), _ptr(halo_id),
+                       ang_mom.ctypes.data_as(_dp))
+    return in_halo, halo_id, ang_mom, int(ierr)
+
+
+def run_device(xp_ptr, vp_ptr, mp_ptr, layout, np_halo, nhalo, total_np, L_Box, link,
+               np_halo_min, bound_check, verbose, softening, a_val, b_val, s_15_val, n_threads,
+               in_halo_ptr, halo_id_ptr, ng_val=256, ng_global_val=512.0):
+    """Device-memory call: pointers are integers (e.g. torch ``data_ptr()``).
+    Returns (ang_mom, ierr)."""
+    L = load()
+    nph = np.ascontiguousarray(np_halo, dtype=np.int32)
+    ang_mom = np.zeros((3, max(int(nhalo), 0)), dtype=np.float64, order="F")
+    vp_c = ctypes.c_void_p(vp_ptr) if vp_ptr else None
+    mp_c = ctypes.c_void_p(mp_ptr) if mp_ptr else None
+    ierr = L.pyfof_run_device(ctypes.c_void_p(xp_ptr), vp_c, mp_c, int(layout),
+                              nph.ctypes.data_as(_i32p), int(nhalo), int(total_np),
+                              float(L_Box), float(link), int(np_halo_min), int(bound_check),
+                              int(verbose), float(softening), float(a_val), float(b_val),
+                              float(s_15_val), int(n_threads), int(ng_val), float(ng_global_val),
+                              ctypes.c_void_p(in_halo_ptr), ctypes.c_void_p(halo_id_ptr),
+                              ang_mom.ctypes.data_as(_dp))
+    return ang_mom, int(ierr)

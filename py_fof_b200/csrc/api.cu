@@ -1,0 +1,318 @@
+// C-ABI of libpyfof_b200.so (declared in include/pyfof_b200.h), per-device
+// contexts and error reporting.
+#include <cstdarg>
+#include <cstring>
+
+#include "context.cuh"
+#include "fof.cuh"
+#include "fof_internal.cuh"
+#include "../../include/pyfof_b200.h"
+
+namespace pyfof {
+
+namespace {
+thread_local std::string g_last_error;
+std::mutex g_ctx_mu;
+Context *g_ctx[64] = {};
+int g_default_device = 0;
+int g_bound_fp64 = 0;
+int g_timing = 0;
+}  // namespace
+
+void set_error(const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+}
+
+std::string last_error() { return g_last_error; }
+
+Context::~Context() {
+  if (stream) {
+    cudaStreamSynchronize(stream);
+    work.release();
+    cudaStreamDestroy(stream);
+  }
+  for (auto &e : ev) if (e) cudaEventDestroy(e);
+  if (d_flags) cudaFree(d_flags);
+  if (h_flags) cudaFreeHost(h_flags);
+}
+
+int32_t get_context(int device, Context **out) {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (device < 0 || device >= 64) {
+    set_error("invalid device %d", device);
+    return kInvalid;
+  }
+  if (!g_ctx[device]) {
+    int ndev = 0;
+    PYFOF_CUDA(cudaGetDeviceCount(&ndev));
+    if (device >= ndev) {
+      set_error("device %d not present (%d devices)", device, ndev);
+      return kInvalid;
+    }
+    PYFOF_CUDA(cudaSetDevice(device));
+    Context *c = new Context();
+    c->device = device;
+    PYFOF_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    PYFOF_CUDA(cudaMalloc(&c->d_flags, sizeof(int32_t) * FLAG_COUNT));
+    PYFOF_CUDA(cudaMallocHost(&c->h_flags, sizeof(int32_t) * FLAG_COUNT));
+    for (auto &e : c->ev) PYFOF_CUDA(cudaEventCreate(&e));
+    cudaMemPool_t pool;
+    PYFOF_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t thr = UINT64_MAX;  // keep freed blocks cached in the pool
+    PYFOF_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    c->work.stream = c->stream;
+    g_ctx[device] = c;
+  }
+  *out = g_ctx[device];
+  return kOk;
+}
+
+void destroy_contexts() {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  for (auto &c : g_ctx) {
+    if (c) {
+      cudaSetDevice(c->device);
+      delete c;
+      c = nullptr;
+    }
+  }
+}
+
+static int32_t validate(int32_t nhalo, int64_t total_np, const int32_t *np_halo,
+                        int32_t n_threads) {
+  if (n_threads > 256) {
+    set_error("n_threads exceeds maximum supported slots (256)");
+    return kThreads;
+  }
+  if (nhalo > 0 && !np_halo) {
+    set_error("np_halo is null");
+    return kInvalid;
+  }
+  int64_t s = 0;
+  for (int32_t h = 0; h < nhalo; ++h) {
+    if (np_halo[h] < 0) {
+      set_error("np_halo[%d] < 0", h);
+      return kInvalid;
+    }
+    s += np_halo[h];
+  }
+  if (nhalo > 0 && s != total_np) {
+    set_error("sum(np_halo) != total_np");
+    return kInvalid;
+  }
+  if (total_np >= (int64_t)INT32_MAX) {
+    set_error("total_np must be below 2**31");
+    return kInvalid;
+  }
+  return kOk;
+}
+
+static int32_t run_common(Context &ctx, FofArgs &a) {
+  ctx.timing = g_timing != 0;
+  a.bound_fp64 = g_bound_fp64;
+  int32_t r = fof_run(ctx, a);
+  cudaError_t e = cudaStreamSynchronize(ctx.stream);
+  if (r == kOk && e != cudaSuccess) {
+    set_error("CUDA failure: %s", cudaGetErrorString(e));
+    r = kCuda;
+  }
+  if (ctx.timing && r == kOk) cudaEventElapsedTime(&ctx.stage_ms[0], ctx.ev[0], ctx.ev[1]);
+  ctx.work.release();
+  cudaStreamSynchronize(ctx.stream);
+  return r;
+}
+
+}  // namespace pyfof
+
+using namespace pyfof;
+
+extern "C" {
+
+int32_t pyfof_version(void) { return PYFOF_B200_ABI_VERSION; }
+
+int32_t pyfof_init(int32_t device) {
+  Context *c;
+  int32_t r = get_context(device, &c);
+  if (r == kOk) g_default_device = device;
+  return r;
+}
+
+int32_t pyfof_shutdown(void) {
+  destroy_contexts();
+  return kOk;
+}
+
+int32_t pyfof_last_error(char *buf, int64_t len) {
+  if (!buf || len <= 0) return (int32_t)g_last_error.size();
+  std::strncpy(buf, g_last_error.c_str(), (size_t)len - 1);
+  buf[len - 1] = 0;
+  return (int32_t)g_last_error.size();
+}
+
+int32_t pyfof_set_option(const char *key, int64_t value) {
+  if (!key) return kInvalid;
+  if (!std::strcmp(key, "unbind_fp64")) { g_bound_fp64 = value != 0; return kOk; }
+  if (!std::strcmp(key, "timing")) { g_timing = value != 0; return kOk; }
+  set_error("unknown option %s", key);
+  return kInvalid;
+}
+
+int32_t pyfof_last_link_ms(float *ms) {
+  Context *c;
+  if (get_context(g_default_device, &c) != kOk || !ms) return kInvalid;
+  *ms = c->stage_ms[0];
+  return kOk;
+}
+
+int32_t pyfof_run(const double *xp, const double *vp, const double *mp, int32_t layout,
+                  const int32_t *np_halo, int32_t nhalo, int64_t total_np, double L_Box,
+                  double linking_length, int32_t np_halo_min, int32_t bound_check,
+                  int32_t verbose, double softening, double a_val, double b_val,
+                  double s_15_val, int32_t n_threads, int64_t ng_val, double ng_global_val,
+                  int32_t *in_halo, int32_t *halo_id, double *ang_mom) {
+  if (total_np > 0) {
+    if (in_halo) std::memset(in_halo, 0, sizeof(int32_t) * (size_t)total_np);
+    if (halo_id) std::memset(halo_id, 0, sizeof(int32_t) * (size_t)total_np);
+  }
+  if (ang_mom && nhalo > 0) std::memset(ang_mom, 0, sizeof(double) * 3 * (size_t)nhalo);
+  int32_t r = validate(nhalo, total_np, np_halo, n_threads);
+  if (r != kOk) return r;
+  if (nhalo <= 0 || total_np <= 0) return kOk;
+  if (!xp || !in_halo || !halo_id || !ang_mom) {
+    set_error("null argument");
+    return kInvalid;
+  }
+  if (bound_check && !vp) {
+    set_error("vp is required when bound_check is set");
+    return kInvalid;
+  }
+  Context *cp;
+  PYFOF_TRY(get_context(g_default_device, &cp));
+  Context &ctx = *cp;
+  std::lock_guard<std::mutex> lk(ctx.mu);
+  PYFOF_CUDA(cudaSetDevice(ctx.device));
+  cudaStream_t s = ctx.stream;
+  const size_t n = (size_t)total_np;
+  FofArgs a;
+  a.xp = ctx.work.carve<double>(3 * n);
+  a.vp = vp ? ctx.work.carve<double>(3 * n) : nullptr;
+  a.mp = mp ? ctx.work.carve<double>(n) : nullptr;
+  a.in_halo = ctx.work.carve<int32_t>(n);
+  a.halo_id = ctx.work.carve<int32_t>(n);
+  if (!a.xp || (vp && !a.vp) || (mp && !a.mp) || !a.in_halo || !a.halo_id) {
+    ctx.work.release();
+    set_error("device allocation failed for %zu particles", n);
+    return kAlloc;
+  }
+  PYFOF_CUDA(cudaMemcpyAsync((void *)a.xp, xp, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+  if (vp)
+    PYFOF_CUDA(cudaMemcpyAsync((void *)a.vp, vp, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+  if (mp) PYFOF_CUDA(cudaMemcpyAsync((void *)a.mp, mp, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  PYFOF_CUDA(cudaMemsetAsync(a.in_halo, 0, sizeof(int32_t) * n, s));
+  PYFOF_CUDA(cudaMemsetAsync(a.halo_id, 0, sizeof(int32_t) * n, s));
+  a.soa = layout == PYFOF_LAYOUT_SOA ? 1 : 0;
+  a.np_halo = np_halo;
+  a.nhalo = nhalo;
+  a.total_np = total_np;
+  a.L_Box = L_Box;
+  a.link = linking_length;
+  a.np_halo_min = np_halo_min;
+  a.bound_check = bound_check;
+  a.verbose = verbose;
+  a.softening = softening;
+  a.a_val = a_val;
+  a.b_val = b_val;
+  a.s15 = s_15_val;
+  a.n_threads = n_threads;
+  a.ng = ng_val;
+  a.ng_global = ng_global_val;
+  a.ang_mom = ang_mom;
+  ctx.timing = g_timing != 0;
+  a.bound_fp64 = g_bound_fp64;
+  r = fof_run(ctx, a);
+  if (r == kOk) {
+    cudaMemcpyAsync(in_halo, a.in_halo, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(halo_id, a.halo_id, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);
+  }
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (r == kOk && e != cudaSuccess) {
+    set_error("CUDA failure: %s", cudaGetErrorString(e));
+    r = kCuda;
+  }
+  if (ctx.timing && r == kOk) cudaEventElapsedTime(&ctx.stage_ms[0], ctx.ev[0], ctx.ev[1]);
+  ctx.work.release();
+  cudaStreamSynchronize(s);
+  if (r != kOk) {
+    std::memset(in_halo, 0, sizeof(int32_t) * n);
+    std::memset(halo_id, 0, sizeof(int32_t) * n);
+    std::memset(ang_mom, 0, sizeof(double) * 3 * (size_t)nhalo);
+  }
+  return r;
+}
+
+int32_t pyfof_run_device(const double *d_xp, const double *d_vp, const double *d_mp,
+                         int32_t layout, const int32_t *np_halo, int32_t nhalo, int64_t total_np,
+                         double L_Box, double linking_length, int32_t np_halo_min,
+                         int32_t bound_check, int32_t verbose, double softening, double a_val,
+                         double b_val, double s_15_val, int32_t n_threads, int64_t ng_val,
+                         double ng_global_val, int32_t *d_in_halo, int32_t *d_halo_id,
+                         double *ang_mom) {
+  if (ang_mom && nhalo > 0) std::memset(ang_mom, 0, sizeof(double) * 3 * (size_t)nhalo);
+  int32_t r = validate(nhalo, total_np, np_halo, n_threads);
+  if (r != kOk) return r;
+  if (nhalo <= 0 || total_np <= 0) return kOk;
+  if (!d_xp || !d_in_halo || !d_halo_id || !ang_mom) {
+    set_error("null argument");
+    return kInvalid;
+  }
+  if (bound_check && !d_vp) {
+    set_error("vp is required when bound_check is set");
+    return kInvalid;
+  }
+  Context *cp;
+  PYFOF_TRY(get_context(g_default_device, &cp));
+  Context &ctx = *cp;
+  std::lock_guard<std::mutex> lk(ctx.mu);
+  PYFOF_CUDA(cudaSetDevice(ctx.device));
+  const size_t n = (size_t)total_np;
+  PYFOF_CUDA(cudaMemsetAsync(d_in_halo, 0, sizeof(int32_t) * n, ctx.stream));
+  PYFOF_CUDA(cudaMemsetAsync(d_halo_id, 0, sizeof(int32_t) * n, ctx.stream));
+  FofArgs a;
+  a.xp = d_xp;
+  a.vp = d_vp;
+  a.mp = d_mp;
+  a.soa = layout == PYFOF_LAYOUT_SOA ? 1 : 0;
+  a.np_halo = np_halo;
+  a.nhalo = nhalo;
+  a.total_np = total_np;
+  a.L_Box = L_Box;
+  a.link = linking_length;
+  a.np_halo_min = np_halo_min;
+  a.bound_check = bound_check;
+  a.verbose = verbose;
+  a.softening = softening;
+  a.a_val = a_val;
+  a.b_val = b_val;
+  a.s15 = s_15_val;
+  a.n_threads = n_threads;
+  a.ng = ng_val;
+  a.ng_global = ng_global_val;
+  a.in_halo = d_in_halo;
+  a.halo_id = d_halo_id;
+  a.ang_mom = ang_mom;
+  r = run_common(ctx, a);
+  if (r != kOk) {
+    cudaMemsetAsync(d_in_halo, 0, sizeof(int32_t) * n, ctx.stream);
+    cudaMemsetAsync(d_halo_id, 0, sizeof(int32_t) * n, ctx.stream);
+    cudaStreamSynchronize(ctx.stream);
+    std::memset(ang_mom, 0, sizeof(double) * 3 * (size_t)nhalo);
+  }
+  return r;
+}
+
+}  // extern "C"

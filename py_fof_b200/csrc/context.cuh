@@ -1,0 +1,33 @@
+// Per-device execution context: stream, scratch arenas, cached tables.
+#pragma once
+
+#include <map>
+#include <memory>
+#include <mutex>
+
+#include "common.cuh"
+
+namespace pyfof {
+
+struct GreenTable;  // unbinding Green's function cache entry (unbind.cu)
+
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Arena work;    // per-call device memory, released at the end of every call
+  int32_t *d_flags = nullptr;  // device status words (error codes, counters)
+  int32_t *h_flags = nullptr;  // pinned mirror
+  std::mutex mu;
+  std::map<int64_t, std::shared_ptr<GreenTable>> green;  // keyed by grid size and kind
+  cudaEvent_t ev[8] = {};
+  // timing of the last call's stages (ms), filled when timing is enabled
+  bool timing = false;
+  float stage_ms[16] = {};
+  ~Context();
+};
+
+// Returns the context of `device`, creating it on first use.
+int32_t get_context(int device, Context **out);
+void destroy_contexts();
+
+}  // namespace pyfof

@@ -1,0 +1,696 @@
+// Friends-of-friends linking on the device.
+//
+// Replaces process_single_region + the fof_fortran driver
+// (fof_fortran.f90:109-362, :496-949) and atomic_dsu.c.  All input regions of
+// a call are processed together:
+//   1. fof_bbox_kernel    per-region unwrap about the first particle + bbox
+//   2. host               reference cell geometry per region (same formulas,
+//                         same libm pow) -> region table
+//   3. fof_key_kernel     global cell key per particle + cell histogram
+//   4. stable radix sort  (cell key, particle index): the reference CRS order
+//   5. fof_gather_kernel  FP32 sorted coordinates (real(x_rel,4))
+//   6. fof_link_kernel    pair tests over the reference's neighbour cells,
+//                         lock-free atomicCAS union (lower index wins)
+//   7. fof_root_kernel    full compression + warp-aggregated group sizes
+//   8. scan of root flags -> candidate ranks (region order, then root CRS
+//                         position: the reference halo numbering)
+//   9. outputs, FP64 centre-of-mass / angular momentum per candidate
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "context.cuh"
+#include "fof.cuh"
+#include "fof_internal.cuh"
+#include "primitives.cuh"
+#include "unbind.cuh"
+
+namespace pyfof {
+
+namespace {
+
+constexpr int TILE = 8192;
+constexpr int BLK = 256;
+
+__device__ __forceinline__ int region_of_key(const uint64_t *cell_off, int nreg, uint64_t key) {
+  int lo = 0, hi = nreg;  // first r with cell_off[r] > key, minus one
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (cell_off[mid] <= key) lo = mid + 1; else hi = mid;
+  }
+  return lo - 1;
+}
+
+__device__ __forceinline__ void warp_minmax(double &mn, double &mx) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+}
+
+__global__ void __launch_bounds__(BLK) fof_bbox_kernel(Coords xp, const RegionDev *__restrict__ R,
+                                                       const Tile *__restrict__ T, double L,
+                                                       double half,
+                                                       unsigned long long *__restrict__ bbox,
+                                                       int32_t *flags) {
+  const Tile t = T[blockIdx.x];
+  const RegionDev &r = R[t.region];
+  if (!r.active) return;
+  double anc[3], mn[3], mx[3];
+  for (int d = 0; d < 3; ++d) {
+    anc[d] = xp.get(r.start, d);
+    mn[d] = INFINITY;
+    mx[d] = -INFINITY;
+  }
+  bool bad = false;
+  for (int64_t i = t.begin + threadIdx.x; i < t.end; i += BLK) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      double x = xp.get(i, d);
+      bad |= !isfinite(x);
+      double v = unwrap(x, anc[d], half, L);
+      mn[d] = fmin(mn[d], v);
+      mx[d] = fmax(mx[d], v);
+    }
+  }
+  if (bad) atomicExch(&flags[FLAG_ERR], kNonFinite);
+  __shared__ double smn[3][BLK / 32], smx[3][BLK / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int d = 0; d < 3; ++d) {
+    warp_minmax(mn[d], mx[d]);
+    if (lane == 0) { smn[d][warp] = mn[d]; smx[d][warp] = mx[d]; }
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int d = threadIdx.x;
+    double a = INFINITY, b = -INFINITY;
+    for (int w = 0; w < BLK / 32; ++w) { a = fmin(a, smn[d][w]); b = fmax(b, smx[d][w]); }
+    if (a <= b) {
+      atomicMin(&bbox[6 * (int64_t)t.region + d], dbl_to_ord(a));
+      atomicMax(&bbox[6 * (int64_t)t.region + 3 + d], dbl_to_ord(b));
+    }
+  }
+}
+
+__device__ __forceinline__ int64_t cell_coord(double x, double origin, double size, int32_t n) {
+  double f = floor(__ddiv_rn(__dadd_rn(x, -origin), size)) + 1.0;
+  if (!(f >= 1.0)) f = 1.0;
+  if (f > (double)n) f = (double)n;
+  return (int64_t)f - 1;
+}
+
+__global__ void __launch_bounds__(BLK) fof_key_kernel(Coords xp, const RegionDev *__restrict__ R,
+                                                      const Tile *__restrict__ T, double L,
+                                                      double half, uint32_t sentinel,
+                                                      uint32_t *__restrict__ keys,
+                                                      uint32_t *__restrict__ counts) {
+  const Tile t = T[blockIdx.x];
+  const RegionDev &r = R[t.region];
+  if (!r.active) {
+    for (int64_t i = t.begin + threadIdx.x; i < t.end; i += BLK) keys[i] = sentinel;
+    return;
+  }
+  double anc[3];
+  for (int d = 0; d < 3; ++d) anc[d] = xp.get(r.start, d);
+  for (int64_t i = t.begin + threadIdx.x; i < t.end; i += BLK) {
+    int64_t c[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      c[d] = cell_coord(unwrap(xp.get(i, d), anc[d], half, L), r.origin[d], r.size[d], r.N[d]);
+    uint64_t key = r.cell_off + (uint64_t)(c[0] + (int64_t)r.N[0] * (c[1] + (int64_t)r.N[1] * c[2]));
+    keys[i] = (uint32_t)key;
+    atomicAdd(&counts[key], 1u);
+  }
+}
+
+__global__ void __launch_bounds__(BLK) fof_gather_kernel(
+    Coords xp, const RegionDev *__restrict__ R, const uint64_t *__restrict__ cell_off, int nreg,
+    const uint32_t *__restrict__ skey, const uint32_t *__restrict__ sidx, int64_t n_active,
+    double L, double half, float4 *__restrict__ pos, uint32_t *__restrict__ prid) {
+  for (int64_t p = (int64_t)blockIdx.x * BLK + threadIdx.x; p < n_active;
+       p += (int64_t)gridDim.x * BLK) {
+    const int rid = nreg == 1 ? 0 : region_of_key(cell_off, nreg, skey[p]);
+    const RegionDev &r = R[rid];
+    const int64_t i = sidx[p];
+    float v[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      v[d] = __double2float_rn(unwrap(xp.get(i, d), xp.get(r.start, d), half, L));
+    pos[p] = make_float4(v[0], v[1], v[2], __int_as_float((int)i));
+    prid[p] = (uint32_t)rid;
+  }
+}
+
+// ---- lock-free disjoint-set union over sorted positions -------------------
+// parent[x] == x marks a root; parent pointers only ever point to smaller
+// indices, so the root of every set is its minimum element, exactly as in
+// atomic_dsu.c (a higher root is hung under a lower one by CAS).
+
+__device__ __forceinline__ int dsu_find(int *parent, int x) {
+  int y = __ldcg(parent + x);
+  while (y != x) {
+    int z = __ldcg(parent + y);
+    if (z != y) parent[x] = z;  // path halving; z is an ancestor of x
+    x = y;
+    y = z;
+  }
+  return x;
+}
+
+__device__ __forceinline__ void dsu_union(int *parent, int a, int b, int32_t *flags) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    a = dsu_find(parent, a);
+    b = dsu_find(parent, b);
+    if (a == b) return;
+    if (a > b) { int t = a; a = b; b = t; }
+    int old = atomicCAS(parent + b, b, a);
+    if (old == b) return;
+  }
+  atomicExch(&flags[FLAG_ERR], kInvalid);  // unreachable: retry cap as a safety net
+}
+
+struct LinkParams {
+  double L, half, rp2;
+  float rp2_open;   // largest float f with (double)f <= link^2
+  float rp2_lo, rp2_hi;  // FP32 fast-path brackets of link^2 for periodic tests
+  int fast_periodic;
+};
+
+// Exact reference distance tests.  Open regions: FP32 differences, squares
+// and sum (fof_fortran.f90:636).  Periodic regions: dist2_pbc
+// (fof_fortran.f90:483-491) in FP64; an FP32 estimate settles all pairs
+// whose distance is far from the linking length and only the rest take the
+// FP64 path, which decides them exactly.
+__device__ __forceinline__ bool linked_open(float4 a, float4 b, float thr) {
+  float d0 = __fsub_rn(a.x, b.x), d1 = __fsub_rn(a.y, b.y), d2 = __fsub_rn(a.z, b.z);
+  float s = __fmul_rn(d0, d0);
+  s = __fadd_rn(s, __fmul_rn(d1, d1));
+  s = __fadd_rn(s, __fmul_rn(d2, d2));
+  return s <= thr;
+}
+
+__device__ __forceinline__ bool linked_pbc(float4 a, float4 b, const LinkParams &P) {
+  float d0 = __fsub_rn(a.x, b.x), d1 = __fsub_rn(a.y, b.y), d2 = __fsub_rn(a.z, b.z);
+  if (P.fast_periodic) {
+    const float hf = (float)P.half, Lf = (float)P.L;
+    float e0 = fabsf(d0), e1 = fabsf(d1), e2 = fabsf(d2);
+    e0 = e0 > hf ? Lf - e0 : e0;
+    e1 = e1 > hf ? Lf - e1 : e1;
+    e2 = e2 > hf ? Lf - e2 : e2;
+    float s = e0 * e0 + e1 * e1 + e2 * e2;
+    if (s < P.rp2_lo) return true;
+    if (s > P.rp2_hi) return false;
+  }
+  double x = fabs((double)d0), y = fabs((double)d1), z = fabs((double)d2);
+  if (x > P.half) x = __dadd_rn(P.L, -x);
+  if (y > P.half) y = __dadd_rn(P.L, -y);
+  if (z > P.half) z = __dadd_rn(P.L, -z);
+  double r2 = __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+  return r2 <= P.rp2;
+}
+
+__global__ void __launch_bounds__(BLK) fof_link_kernel(
+    const float4 *__restrict__ pos, const uint32_t *__restrict__ skey,
+    const uint32_t *__restrict__ prid, const RegionDev *__restrict__ R,
+    const uint32_t *__restrict__ cell_start, int *parent, int64_t n_active, LinkParams P,
+    int32_t *flags) {
+  for (int64_t p = (int64_t)blockIdx.x * BLK + threadIdx.x; p < n_active;
+       p += (int64_t)gridDim.x * BLK) {
+    const float4 me = pos[p];
+    const RegionDev &r = R[prid[p]];
+    const int64_t local = (int64_t)skey[p] - (int64_t)r.cell_off;
+    const int64_t N0 = r.N[0], N1 = r.N[1], N2 = r.N[2];
+    const int64_t ix = local % N0, iy = (local / N0) % N1, iz = local / (N0 * N1);
+    const bool per = r.periodic != 0;
+    int lo[3], hi[3];
+    const int64_t Nd[3] = {N0, N1, N2};
+    for (int d = 0; d < 3; ++d) {
+      if (Nd[d] == 1) { lo[d] = 0; hi[d] = 0; }
+      else if (((r.pdim >> d) & 1) && Nd[d] == 2) { lo[d] = 0; hi[d] = 1; }
+      else { lo[d] = -1; hi[d] = 1; }
+    }
+    const int ip = (int)p;
+    for (int dz = lo[2]; dz <= hi[2]; ++dz) {
+      int64_t jz = iz + dz;
+      if ((r.pdim >> 2) & 1) jz = (jz + N2) % N2;
+      else if (jz < 0 || jz >= N2) continue;
+      for (int dy = lo[1]; dy <= hi[1]; ++dy) {
+        int64_t jy = iy + dy;
+        if ((r.pdim >> 1) & 1) jy = (jy + N1) % N1;
+        else if (jy < 0 || jy >= N1) continue;
+        for (int dx = lo[0]; dx <= hi[0]; ++dx) {
+          int64_t jx = ix + dx;
+          if (r.pdim & 1) jx = (jx + N0) % N0;
+          else if (jx < 0 || jx >= N0) continue;
+          const int64_t jl = jx + N0 * (jy + N1 * jz);
+          if (jl < local) continue;
+          const uint64_t jc = r.cell_off + (uint64_t)jl;
+          int64_t b = cell_start[jc];
+          const int64_t e = cell_start[jc + 1];
+          if (jl == local) b = p + 1;
+          for (int64_t q = b; q < e; ++q) {
+            const float4 o = pos[q];
+            const bool lk = per ? linked_pbc(me, o, P) : linked_open(me, o, P.rp2_open);
+            if (lk) dsu_union(parent, ip, (int)q, flags);
+          }
+        }
+      }
+    }
+  }
+}
+
+__global__ void fof_init_parent(int *parent, int64_t n) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x)
+    parent[p] = (int)p;
+}
+
+__global__ void __launch_bounds__(BLK) fof_root_kernel(int *parent, uint32_t *gsize, int64_t n) {
+  for (int64_t base = (int64_t)blockIdx.x * BLK; base < n; base += (int64_t)gridDim.x * BLK) {
+    const int64_t p = base + threadIdx.x;
+    int root = -1;
+    if (p < n) {
+      root = dsu_find(parent, (int)p);
+      parent[p] = root;
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, root);
+    const int leader = __ffs(peers) - 1;
+    if (root >= 0 && (int)(threadIdx.x & 31) == leader) atomicAdd(&gsize[root], (uint32_t)__popc(peers));
+  }
+}
+
+__global__ void fof_cand_flag_kernel(const int *parent, const uint32_t *gsize, int64_t n,
+                                     uint32_t np_min, uint32_t *flag) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x)
+    flag[p] = (parent[p] == (int)p && gsize[p] >= np_min) ? 1u : 0u;
+}
+
+// Candidate of every sorted particle (-1 if its group is too small), plus
+// the no-unbinding outputs (fof_fortran.f90:207-222).
+__global__ void fof_member_kernel(const int *parent, const uint32_t *gsize,
+                                  const uint32_t *crank, const float4 *pos, int64_t n,
+                                  uint32_t np_min, int write_out, int32_t *pcand,
+                                  int32_t *in_halo, int32_t *halo_id) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int r = parent[p];
+    int32_t c = -1;
+    if (gsize[r] >= np_min) c = (int32_t)crank[r];
+    pcand[p] = c;
+    if (write_out && c >= 0) {
+      const int i = __float_as_int(pos[p].w);
+      in_halo[i] = 1;
+      halo_id[i] = c + 1;
+    }
+  }
+}
+
+// Per-candidate weighted sums for the centre of mass and mean velocity
+// (fof_fortran.f90:225-238): acc[c] = {w, w*dx, w*dv}.
+__global__ void __launch_bounds__(BLK) fof_com_kernel(Coords xp, Coords vp, const double *mp,
+                                                      const float4 *pos, const int32_t *pcand,
+                                                      const int64_t *cand_anchor, int64_t n,
+                                                      double L, double half, double *acc) {
+  for (int64_t base = (int64_t)blockIdx.x * BLK; base < n; base += (int64_t)gridDim.x * BLK) {
+    const int64_t p = base + threadIdx.x;
+    int32_t c = p < n ? pcand[p] : -1;
+    double v[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (c >= 0) {
+      const int64_t i = __float_as_int(pos[p].w);
+      const int64_t a = cand_anchor[c];
+      const double w = mp ? mp[i] : 1.0;
+      v[0] = w;
+      for (int d = 0; d < 3; ++d) {
+        v[1 + d] = w * unwrap(xp.get(i, d), xp.get(a, d), half, L);
+        v[4 + d] = w * vp.get(i, d);
+      }
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, c);
+    if (peers == 0xffffffffu) {
+      for (int k = 0; k < 7; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+      if ((threadIdx.x & 31) == 0 && c >= 0)
+        for (int k = 0; k < 7; ++k) atomicAdd(&acc[7 * (int64_t)c + k], v[k]);
+    } else if (c >= 0) {
+      for (int k = 0; k < 7; ++k) atomicAdd(&acc[7 * (int64_t)c + k], v[k]);
+    }
+  }
+}
+
+// Angular momentum about the candidate centre (fof_fortran.f90:239-247),
+// accumulated per candidate.
+__global__ void __launch_bounds__(BLK) fof_angmom_kernel(Coords xp, Coords vp, const double *mp,
+                                                         const float4 *pos, const int32_t *pcand,
+                                                         const int64_t *cand_anchor,
+                                                         const double *acc, int64_t n, double L,
+                                                         double half, double *am) {
+  for (int64_t base = (int64_t)blockIdx.x * BLK; base < n; base += (int64_t)gridDim.x * BLK) {
+    const int64_t p = base + threadIdx.x;
+    int32_t c = p < n ? pcand[p] : -1;
+    double v[3] = {0, 0, 0};
+    if (c >= 0 && acc[7 * (int64_t)c] > 0.0) {
+      const int64_t i = __float_as_int(pos[p].w);
+      const int64_t a = cand_anchor[c];
+      const double ws = acc[7 * (int64_t)c];
+      const double w = mp ? mp[i] : 1.0;
+      double dx[3], dv[3];
+      for (int d = 0; d < 3; ++d) {
+        dx[d] = unwrap(xp.get(i, d), xp.get(a, d), half, L) - acc[7 * (int64_t)c + 1 + d] / ws;
+        dv[d] = vp.get(i, d) - acc[7 * (int64_t)c + 4 + d] / ws;
+      }
+      v[0] = w * (dx[1] * dv[2] - dx[2] * dv[1]);
+      v[1] = w * (dx[2] * dv[0] - dx[0] * dv[2]);
+      v[2] = w * (dx[0] * dv[1] - dx[1] * dv[0]);
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, c);
+    if (peers == 0xffffffffu) {
+      for (int k = 0; k < 3; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+      if ((threadIdx.x & 31) == 0 && c >= 0)
+        for (int k = 0; k < 3; ++k) atomicAdd(&am[3 * (int64_t)c + k], v[k]);
+    } else if (c >= 0) {
+      for (int k = 0; k < 3; ++k) atomicAdd(&am[3 * (int64_t)c + k], v[k]);
+    }
+  }
+}
+
+// anchor (first member in CRS order = the root) and region of each candidate
+__global__ void fof_cand_info_kernel(const uint32_t *flag, const uint32_t *crank,
+                                     const float4 *pos, const uint32_t *prid,
+                                     const uint32_t *gsize, int64_t n, int64_t *cand_anchor,
+                                     int32_t *cand_region, int32_t *cand_np, int32_t *cand_root) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x)
+    if (flag[p]) {
+      const uint32_t c = crank[p];
+      cand_anchor[c] = __float_as_int(pos[p].w);
+      cand_region[c] = (int32_t)prid[p];
+      cand_np[c] = (int32_t)gsize[p];
+      cand_root[c] = (int32_t)p;
+    }
+}
+
+int bits_for(uint64_t v) {
+  int b = 0;
+  while (b < 64 && (v >> b) != 0) ++b;
+  return b;
+}
+
+}  // namespace
+
+// ------------------------------------------------------- host geometry
+
+// Reference cell geometry of one region (fof_fortran.f90:528-570) from its
+// unwrapped bounding box.  64-bit integers are used where the reference's
+// default integers would overflow (N >= 2**29).
+void region_geometry(double L, double link, int32_t np, const double *xmin, const double *xmax,
+                     RegionDev &r) {
+  const double half = 0.5 * L;
+  double range[3];
+  int pd = 0;
+  for (int d = 0; d < 3; ++d) {
+    range[d] = xmax[d] - xmin[d];
+    if (range[d] + 2.0 * link >= L) pd |= 1 << d;
+  }
+  const double vol = std::max(range[0], link) * std::max(range[1], link) * std::max(range[2], link);
+  auto geom = [&](double L_mesh, int64_t *N) {
+    for (int d = 0; d < 3; ++d) {
+      if ((pd >> d) & 1) {
+        r.origin[d] = -half;
+        int64_t a = (int64_t)(L / link), b = (int64_t)(L / L_mesh);
+        N[d] = std::max<int64_t>(1, std::min(a, b));
+        r.size[d] = L / (double)N[d];
+      } else {
+        r.origin[d] = xmin[d];
+        N[d] = std::max<int64_t>(1, (int64_t)std::ceil(range[d] / L_mesh));
+        r.size[d] = L_mesh;
+      }
+    }
+  };
+  int64_t N[3];
+  double L_mesh = std::max(link, std::pow(vol / (double)std::max(1, np), 1.0 / 3.0));
+  geom(L_mesh, N);
+  const int64_t cap = std::max<int64_t>(262144, 4 * (int64_t)np);
+  if ((double)N[0] * (double)N[1] * (double)N[2] > (double)cap) {
+    L_mesh = std::pow(vol / (double)((int64_t)std::max(1, np) * 2), 1.0 / 3.0);
+    L_mesh = std::max(link, L_mesh);
+    geom(L_mesh, N);
+  }
+  for (int d = 0; d < 3; ++d) r.N[d] = (int32_t)std::min<int64_t>(N[d], INT32_MAX);
+  r.pdim = pd;
+  r.periodic = pd != 0;
+  r.ncell = N[0] * N[1] * N[2];
+}
+
+int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
+  cudaStream_t s = ctx.stream;
+  Arena &W = ctx.work;
+  const int64_t n = a.total_np;
+  const int nreg = a.nhalo;
+  const double L = a.L_Box, half = 0.5 * a.L_Box;
+  st.n = n;
+  st.nreg = nreg;
+  Coords xp{a.xp, n, a.soa};
+
+  // --- region table and tiles (host)
+  std::vector<RegionDev> reg(nreg);
+  std::vector<Tile> tiles;
+  int64_t start = 0;
+  for (int r = 0; r < nreg; ++r) {
+    RegionDev &R = reg[r];
+    memset(&R, 0, sizeof(R));
+    R.start = start;
+    R.np = a.np_halo[r];
+    R.active = (R.np >= a.np_halo_min && R.np > 0) ? 1 : 0;
+    for (int64_t b = start; b < start + R.np; b += TILE)
+      tiles.push_back(Tile{r, 0, b, std::min<int64_t>(start + R.np, b + TILE)});
+    start += R.np;
+  }
+  if (start != n) {
+    set_error("sum(np_halo)=%lld != total_np=%lld", (long long)start, (long long)n);
+    return kInvalid;
+  }
+  const int64_t ntiles = (int64_t)tiles.size();
+  RegionDev *dR = W.carve<RegionDev>(nreg);
+  Tile *dT = W.carve<Tile>(std::max<int64_t>(ntiles, 1));
+  unsigned long long *dbb = W.carve<unsigned long long>(6 * (size_t)nreg);
+  if (!dR || !dT || !dbb) { set_error("workspace exhausted (regions)"); return kAlloc; }
+  PYFOF_CUDA(cudaMemcpyAsync(dR, reg.data(), sizeof(RegionDev) * nreg, cudaMemcpyHostToDevice, s));
+  if (ntiles)
+    PYFOF_CUDA(cudaMemcpyAsync(dT, tiles.data(), sizeof(Tile) * ntiles, cudaMemcpyHostToDevice, s));
+  {
+    std::vector<unsigned long long> init(6 * (size_t)nreg);
+    for (int r = 0; r < nreg; ++r)
+      for (int d = 0; d < 3; ++d) { init[6 * r + d] = ~0ull; init[6 * r + 3 + d] = 0ull; }
+    PYFOF_CUDA(cudaMemcpyAsync(dbb, init.data(), sizeof(unsigned long long) * init.size(),
+                               cudaMemcpyHostToDevice, s));
+  }
+  PYFOF_CUDA(cudaMemsetAsync(ctx.d_flags, 0, sizeof(int32_t) * FLAG_COUNT, s));
+  if (ntiles) {
+    fof_bbox_kernel<<<(unsigned)ntiles, BLK, 0, s>>>(xp, dR, dT, L, half, dbb, ctx.d_flags);
+    PYFOF_CUDA(cudaGetLastError());
+  }
+  std::vector<unsigned long long> bb(6 * (size_t)nreg);
+  PYFOF_CUDA(cudaMemcpyAsync(bb.data(), dbb, sizeof(unsigned long long) * bb.size(),
+                             cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t) * FLAG_COUNT,
+                             cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaStreamSynchronize(s));
+  if (ctx.h_flags[FLAG_ERR]) {
+    set_error("non-finite particle coordinates");
+    return ctx.h_flags[FLAG_ERR];
+  }
+
+  // --- reference geometry per region (host)
+  uint64_t total_cells = 0;
+  int64_t n_active = 0;
+  std::vector<uint64_t> cell_off(nreg + 1);
+  for (int r = 0; r < nreg; ++r) {
+    RegionDev &R = reg[r];
+    cell_off[r] = total_cells;
+    R.cell_off = total_cells;
+    if (!R.active) continue;
+    double xmin[3], xmax[3];
+    for (int d = 0; d < 3; ++d) {
+      xmin[d] = ord_to_dbl(bb[6 * r + d]);
+      xmax[d] = ord_to_dbl(bb[6 * r + 3 + d]);
+    }
+    region_geometry(L, a.link, R.np, xmin, xmax, R);
+    total_cells += (uint64_t)R.ncell;
+    n_active += R.np;
+  }
+  cell_off[nreg] = total_cells;
+  if (total_cells >= 0xffffffffull) {
+    set_error("total cell count %llu exceeds the 32-bit key range",
+              (unsigned long long)total_cells);
+    return kAlloc;
+  }
+  st.n_active = n_active;
+  st.total_cells = total_cells;
+  PYFOF_CUDA(cudaMemcpyAsync(dR, reg.data(), sizeof(RegionDev) * nreg, cudaMemcpyHostToDevice, s));
+  uint64_t *dcoff = W.carve<uint64_t>(nreg + 1);
+  uint32_t *keys = W.carve<uint32_t>(std::max<int64_t>(n, 1));
+  uint32_t *cstart = W.carve<uint32_t>(total_cells + 2);
+  uint32_t *ka = W.carve<uint32_t>(std::max<int64_t>(n, 1));
+  uint32_t *va = W.carve<uint32_t>(std::max<int64_t>(n, 1));
+  uint32_t *kb = W.carve<uint32_t>(std::max<int64_t>(n, 1));
+  uint32_t *vb = W.carve<uint32_t>(std::max<int64_t>(n, 1));
+  if (!dcoff || !keys || !cstart || !ka || !va || !kb || !vb) {
+    set_error("workspace exhausted (keys)");
+    return kAlloc;
+  }
+  PYFOF_CUDA(cudaMemcpyAsync(dcoff, cell_off.data(), sizeof(uint64_t) * (nreg + 1),
+                             cudaMemcpyHostToDevice, s));
+  PYFOF_CUDA(cudaMemsetAsync(cstart, 0, sizeof(uint32_t) * (total_cells + 2), s));
+  const uint32_t sentinel = (uint32_t)total_cells;
+  if (ntiles) {
+    fof_key_kernel<<<(unsigned)ntiles, BLK, 0, s>>>(xp, dR, dT, L, half, sentinel, keys, cstart);
+    PYFOF_CUDA(cudaGetLastError());
+  }
+  PYFOF_TRY(exclusive_scan_u32(cstart, cstart, (int64_t)total_cells + 1, nullptr, W, s));
+  uint32_t *skey, *sidx;
+  PYFOF_TRY(radix_sort_pairs(keys, nullptr, n, bits_for(total_cells), ka, va, kb, vb, &skey, &sidx,
+                             W, s));
+  // --- sorted FP32 coordinates, DSU
+  float4 *pos = W.carve<float4>(std::max<int64_t>(n_active, 1));
+  uint32_t *prid = W.carve<uint32_t>(std::max<int64_t>(n_active, 1));
+  int *parent = W.carve<int>(std::max<int64_t>(n_active, 1));
+  if (!pos || !prid || !parent) { set_error("workspace exhausted (link)"); return kAlloc; }
+  const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(std::max<int64_t>(n_active, 1), BLK),
+                                                    (int64_t)kNumSMs * 16);
+  if (n_active > 0) {
+    fof_gather_kernel<<<grid, BLK, 0, s>>>(xp, dR, dcoff, nreg, skey, sidx, n_active, L, half, pos,
+                                           prid);
+    PYFOF_CUDA(cudaGetLastError());
+    fof_init_parent<<<grid, BLK, 0, s>>>(parent, n_active);
+    PYFOF_CUDA(cudaGetLastError());
+    LinkParams P;
+    P.L = L;
+    P.half = half;
+    P.rp2 = a.link * a.link;
+    {
+      float f = (float)P.rp2;
+      if ((double)f > P.rp2) f = std::nextafter(f, -INFINITY);
+      P.rp2_open = f;
+    }
+    P.fast_periodic = (P.rp2 > 1e-20 && P.rp2 < 1e20 && L < 1e30) ? 1 : 0;
+    P.rp2_lo = (float)(P.rp2 * (1.0 - 4e-6));
+    P.rp2_hi = (float)(P.rp2 * (1.0 + 4e-6));
+    if (ctx.timing) cudaEventRecord(ctx.ev[0], s);
+    fof_link_kernel<<<grid, BLK, 0, s>>>(pos, skey, prid, dR, cstart, parent, n_active, P,
+                                         ctx.d_flags);
+    PYFOF_CUDA(cudaGetLastError());
+    if (ctx.timing) cudaEventRecord(ctx.ev[1], s);
+  }
+  st.dR = dR;
+  st.pos = pos;
+  st.prid = prid;
+  st.parent = parent;
+  st.skey = skey;
+  st.sidx = sidx;
+  st.cell_start = cstart;
+  st.keys_free = keys;
+  st.reg = reg;
+  return kOk;
+}
+
+int32_t fof_candidates_stage(Context &ctx, const FofArgs &a, FofState &st, bool write_plain) {
+  cudaStream_t s = ctx.stream;
+  Arena &W = ctx.work;
+  const int64_t na = st.n_active;
+  uint32_t *gsize = W.carve<uint32_t>(std::max<int64_t>(na, 1));
+  uint32_t *flag = W.carve<uint32_t>(std::max<int64_t>(na, 1) + 1);
+  uint32_t *crank = W.carve<uint32_t>(std::max<int64_t>(na, 1) + 1);
+  int32_t *pcand = W.carve<int32_t>(std::max<int64_t>(na, 1));
+  if (!gsize || !flag || !crank || !pcand) { set_error("workspace exhausted (labels)"); return kAlloc; }
+  st.ncand = 0;
+  if (na > 0) {
+    const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(na, BLK), (int64_t)kNumSMs * 16);
+    PYFOF_CUDA(cudaMemsetAsync(gsize, 0, sizeof(uint32_t) * na, s));
+    fof_root_kernel<<<grid, BLK, 0, s>>>(st.parent, gsize, na);
+    PYFOF_CUDA(cudaGetLastError());
+    fof_cand_flag_kernel<<<grid, BLK, 0, s>>>(st.parent, gsize, na, (uint32_t)a.np_halo_min, flag);
+    PYFOF_CUDA(cudaGetLastError());
+    PYFOF_TRY(exclusive_scan_u32(flag, crank, na, reinterpret_cast<uint32_t *>(ctx.d_flags + FLAG_COUNT_A), W, s));
+    fof_member_kernel<<<grid, BLK, 0, s>>>(st.parent, gsize, crank, st.pos, na,
+                                           (uint32_t)a.np_halo_min, write_plain ? 1 : 0, pcand,
+                                           a.in_halo, a.halo_id);
+    PYFOF_CUDA(cudaGetLastError());
+    PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t) * FLAG_COUNT,
+                               cudaMemcpyDeviceToHost, s));
+    PYFOF_CUDA(cudaStreamSynchronize(s));
+    if (ctx.h_flags[FLAG_ERR]) {
+      set_error("linking failed (DSU retry cap)");
+      return ctx.h_flags[FLAG_ERR];
+    }
+    st.ncand = (uint32_t)ctx.h_flags[FLAG_COUNT_A];
+  }
+  st.gsize = gsize;
+  st.flag = flag;
+  st.crank = crank;
+  st.pcand = pcand;
+  const int64_t nc = std::max<int64_t>(st.ncand, 1);
+  st.cand_anchor = W.carve<int64_t>(nc);
+  st.cand_region = W.carve<int32_t>(nc);
+  st.cand_np = W.carve<int32_t>(nc);
+  st.cand_root = W.carve<int32_t>(nc);
+  if (!st.cand_anchor || !st.cand_region || !st.cand_np || !st.cand_root) {
+    set_error("workspace exhausted (candidates)");
+    return kAlloc;
+  }
+  if (st.ncand > 0) {
+    const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(na, BLK), (int64_t)kNumSMs * 16);
+    fof_cand_info_kernel<<<grid, BLK, 0, s>>>(flag, crank, st.pos, st.prid, gsize, na,
+                                              st.cand_anchor, st.cand_region, st.cand_np,
+                                              st.cand_root);
+    PYFOF_CUDA(cudaGetLastError());
+  }
+  return kOk;
+}
+
+// ang_mom per input region over all candidates (no unbinding):
+// fof_fortran.f90:224-248.
+int32_t fof_plain_angmom(Context &ctx, const FofArgs &a, FofState &st) {
+  cudaStream_t s = ctx.stream;
+  Arena &W = ctx.work;
+  const int nreg = a.nhalo;
+  std::vector<double> am_host(3 * (size_t)nreg, 0.0);
+  if (st.ncand > 0 && a.vp) {
+    const int64_t na = st.n_active, nc = st.ncand;
+    double *acc = W.carve<double>(7 * (size_t)nc);
+    double *am = W.carve<double>(3 * (size_t)nc);
+    if (!acc || !am) { set_error("workspace exhausted (ang_mom)"); return kAlloc; }
+    PYFOF_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 7 * nc, s));
+    PYFOF_CUDA(cudaMemsetAsync(am, 0, sizeof(double) * 3 * nc, s));
+    Coords xp{a.xp, a.total_np, a.soa}, vp{a.vp, a.total_np, a.soa};
+    const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(na, BLK), (int64_t)kNumSMs * 16);
+    fof_com_kernel<<<grid, BLK, 0, s>>>(xp, vp, a.mp, st.pos, st.pcand, st.cand_anchor, na,
+                                        a.L_Box, 0.5 * a.L_Box, acc);
+    PYFOF_CUDA(cudaGetLastError());
+    fof_angmom_kernel<<<grid, BLK, 0, s>>>(xp, vp, a.mp, st.pos, st.pcand, st.cand_anchor, acc,
+                                           na, a.L_Box, 0.5 * a.L_Box, am);
+    PYFOF_CUDA(cudaGetLastError());
+    std::vector<double> amc(3 * (size_t)nc);
+    std::vector<int32_t> creg(nc);
+    PYFOF_CUDA(cudaMemcpyAsync(amc.data(), am, sizeof(double) * 3 * nc, cudaMemcpyDeviceToHost, s));
+    PYFOF_CUDA(cudaMemcpyAsync(creg.data(), st.cand_region, sizeof(int32_t) * nc,
+                               cudaMemcpyDeviceToHost, s));
+    PYFOF_CUDA(cudaStreamSynchronize(s));
+    for (int64_t c = 0; c < nc; ++c)
+      for (int d = 0; d < 3; ++d) am_host[3 * (size_t)creg[c] + d] += amc[3 * c + d];
+  }
+  memcpy(a.ang_mom, am_host.data(), sizeof(double) * am_host.size());
+  return kOk;
+}
+
+int32_t fof_run(Context &ctx, const FofArgs &a) {
+  FofState st;
+  PYFOF_TRY(fof_link_stage(ctx, a, st));
+  PYFOF_TRY(fof_candidates_stage(ctx, a, st, !a.bound_check));
+  if (!a.bound_check) return fof_plain_angmom(ctx, a, st);
+  return unbind_stage(ctx, a, st);
+}
+
+}  // namespace pyfof

@@ -1,0 +1,36 @@
+// Friends-of-friends pipeline on one device.
+#pragma once
+
+#include "common.cuh"
+
+namespace pyfof {
+
+// Arguments of one fof_fortran-equivalent call (fof_fortran.f90:10-58).
+// All particle arrays are device pointers.
+struct FofArgs {
+  const double *xp = nullptr;  // (3,N): soa ? x[d*N+i] : x[3i+d]
+  const double *vp = nullptr;  // same layout; null means all velocities are zero
+  const double *mp = nullptr;  // (N); null means unit masses
+  int32_t soa = 1;
+  const int32_t *np_halo = nullptr;  // host array (nhalo)
+  int32_t nhalo = 0;
+  int64_t total_np = 0;
+  double L_Box = 512.0, link = 0.2;
+  int32_t np_halo_min = 10, bound_check = 0, verbose = 0;
+  double softening = 0.1, a_val = 1.0, b_val = 0.0, s15 = 15.0 * 0.67 * 512.0 / 300.0;
+  int32_t n_threads = 0;
+  int64_t ng = 256;
+  double ng_global = 512.0;
+  int32_t bound_fp64 = 0;  // 1: plain FP64 unbinding path instead of the FP32 product path
+  // outputs (device): in_halo, halo_id (N int32); ang_mom host (3,nhalo) F-order
+  int32_t *in_halo = nullptr, *halo_id = nullptr;
+  double *ang_mom = nullptr;
+};
+
+struct Context;
+
+// Runs the whole call on ctx's stream; returns a reference ierr code (or
+// kCuda).  Synchronises the stream before returning.
+int32_t fof_run(Context &ctx, const FofArgs &a);
+
+}  // namespace pyfof

@@ -1,0 +1,153 @@
+"""FoF parity: the B200 path (py_fof_b200 -> libpyfof_b200.so) against the
+CPU oracle on seeded inputs.  The partition, in_halo and halo_id (reference
+numbering) must be bit-exact; angular momenta agree to summation-order
+rounding."""
+import numpy as np
+import pytest
+
+import py_fof_b200 as P
+from py_fof_b200 import _native, workloads as W
+from tests.helpers import angmom_close, canonical, oracle_core
+
+pytestmark = pytest.mark.gpu
+
+
+def _both(xp_list, **kw):
+    g = P._fof_core(xp_list, **kw)
+    o = oracle_core(xp_list, **kw)
+    return g, o
+
+
+def _assert_same(g, o, scale=1.0):
+    assert np.array_equal(g[0], o[0]), "in_halo differs"
+    assert np.array_equal(g[1], o[1]), "halo_id differs"
+    assert angmom_close(g[2], o[2], scale), f"ang_mom {g[2]} vs {o[2]}"
+
+
+def test_library_loads_native():
+    L = _native.load()
+    assert L.pyfof_version() == _native.ABI_VERSION
+    assert L.pyfof_init(0) == 0
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_config1_recipe_small(seed):
+    d = W.plummer_box(32 ** 3, 32.0, 8, seed=seed, with_velocities=True)
+    g, o = _both(d["xp"], vp_list=d["vp"], L_Box=32.0, linking_length=0.2, np_halo_min=10,
+                 return_ang_mom=True)
+    assert o[1].max() > 0
+    _assert_same(g, o, scale=np.abs(o[2]).max() + 1.0)
+
+
+def test_config1_full_size():
+    d = W.config1(seed=3)
+    g, o = _both(d["xp"], L_Box=64.0, linking_length=0.2, np_halo_min=10)
+    assert o[1].max() > 10
+    _assert_same(g, o)
+
+
+def test_open_region_clustered():
+    rng = np.random.default_rng(7)
+    xp = np.concatenate([rng.normal(200.0, 3.0, (3, 20000)),
+                         rng.uniform(150.0, 250.0, (3, 5000))], axis=1)
+    vp = rng.normal(0.0, 1.0, xp.shape)
+    g, o = _both(xp, vp_list=vp, L_Box=512.0, linking_length=0.4, np_halo_min=5,
+                 return_ang_mom=True)
+    assert o[1].max() > 0
+    _assert_same(g, o, scale=np.abs(o[2]).max() + 1.0)
+
+
+def test_multi_region_mixed():
+    rng = np.random.default_rng(11)
+    xs, vs = [], []
+    for k, n in enumerate([500, 3, 0, 4000, 12, 2500, 9]):
+        c = rng.uniform(0, 100, (3, 1))
+        xs.append(c + rng.normal(0, 1.5, (3, n)))
+        vs.append(rng.normal(0, 0.3, (3, n)))
+    g, o = _both(xs, vp_list=vs, L_Box=100.0, linking_length=0.35, np_halo_min=10,
+                 return_ang_mom=True)
+    _assert_same(g, o, scale=np.abs(o[2]).max() + 1.0)
+
+
+@pytest.mark.parametrize("L,link", [(0.3, 0.2), (0.5, 0.2), (1.0, 0.3), (2.0, 0.3)])
+def test_small_periodic_boxes(L, link):
+    """Boxes with 1, 2 and 3 cells per axis exercise the neighbour dedup."""
+    rng = np.random.default_rng(int(L * 100))
+    xp = rng.uniform(0, L, (3, 400))
+    g, o = _both(xp, L_Box=L, linking_length=link, np_halo_min=3)
+    _assert_same(g, o)
+
+
+def test_partially_periodic_filament():
+    rng = np.random.default_rng(5)
+    n = 6000
+    xp = np.stack([rng.uniform(0, 50.0, n), 25 + rng.normal(0, 0.4, n),
+                   25 + rng.normal(0, 0.4, n)])
+    g, o = _both(xp, L_Box=50.0, linking_length=0.25, np_halo_min=10)
+    assert o[1].max() > 0
+    _assert_same(g, o)
+
+
+def test_degenerate_positions():
+    xp = np.zeros((3, 50))
+    xp[0, 25:] = 3.0
+    g, o = _both(xp, L_Box=10.0, linking_length=0.2, np_halo_min=10)
+    _assert_same(g, o)
+    assert g[1].max() == 2
+
+
+def test_link_length_boundary():
+    """Pairs placed at the linking length: FP32 rounding decides them."""
+    rng = np.random.default_rng(9)
+    base = rng.uniform(10, 90, (3, 300))
+    d = rng.standard_normal((3, 300))
+    d /= np.linalg.norm(d, axis=0)
+    xp = np.concatenate([base, base + 0.2 * d], axis=1)
+    for L in (100.0, 1e4):
+        g, o = _both(xp, L_Box=L, linking_length=0.2, np_halo_min=2)
+        _assert_same(g, o)
+
+
+@pytest.mark.parametrize("npmin", [1, 2, 1000000])
+def test_np_halo_min_extremes(npmin):
+    rng = np.random.default_rng(2)
+    xp = rng.uniform(0, 20, (3, 3000))
+    g, o = _both(xp, L_Box=20.0, linking_length=0.5, np_halo_min=npmin)
+    _assert_same(g, o)
+
+
+def test_fortran_order_input():
+    d = W.plummer_box(16 ** 3, 16.0, 2, seed=4)
+    xf = np.asfortranarray(d["xp"])
+    a = P._fof_core(xf, L_Box=16.0, linking_length=0.2, np_halo_min=5)
+    b = P._fof_core(d["xp"], L_Box=16.0, linking_length=0.2, np_halo_min=5)
+    assert np.array_equal(a[1], b[1])
+
+
+def test_empty_and_errors():
+    r = P._fof_core(np.zeros((3, 0)))
+    assert r[0].shape == (0,) and r[2].shape == (3, 1)
+    with pytest.raises(ValueError):
+        P.fof(np.array([[np.nan, 0.0], [0.0, 0.0], [0.0, 0.0]]), L_Box=10.0)
+
+
+def test_device_entry_point_matches_host():
+    torch = pytest.importorskip("torch")
+    d = W.plummer_box(24 ** 3, 24.0, 4, seed=8)
+    ref = P._fof_core(d["xp"], L_Box=24.0, linking_length=0.2, np_halo_min=10)
+    x = torch.from_numpy(d["xp"]).cuda()
+    n = d["xp"].shape[1]
+    ih = torch.zeros(n, dtype=torch.int32, device="cuda")
+    hid = torch.zeros(n, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    am, ierr = _native.run_device(x.data_ptr(), 0, 0, _native.LAYOUT_SOA, [n], 1, n, 24.0, 0.2,
+                                  10, 0, 0, 0.1, 1.0, 0.0, 1.0, 0, ih.data_ptr(), hid.data_ptr())
+    assert ierr == 0
+    assert np.array_equal(hid.cpu().numpy(), ref[1])
+    assert np.array_equal(ih.cpu().numpy().astype(bool), ref[0])
+
+
+def test_canonical_partition_matches():
+    d = W.plummer_box(20 ** 3, 20.0, 3, seed=12)
+    g, o = _both(d["xp"], L_Box=20.0, linking_length=0.25, np_halo_min=2)
+    assert np.array_equal(canonical(g[1]), canonical(o[1]))

@@ -1,0 +1,74 @@
+"""CPU-side checks of the native boundary: the C-ABI library loads without a
+GPU and exports every symbol include/pyfof_b200.h declares; the Python
+wrapper validates arguments like the reference."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import py_fof_b200 as P
+from py_fof_b200 import _native
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                      "pyfof_b200.h")
+
+
+def _declared():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(pyfof_\w+)\s*\(", src)))
+
+
+def test_header_matches_binding():
+    assert sorted(_native.EXPORTED) == _declared()
+
+
+def test_library_exports_all_symbols():
+    L = _native.load()
+    for name in _declared():
+        assert hasattr(L, name), name
+    assert L.pyfof_version() == _native.ABI_VERSION
+
+
+def test_validation_errors():
+    xp = np.zeros((3, 5))
+    with pytest.raises(ValueError):
+        P.fof(xp, units="bogus")
+    with pytest.raises(ValueError):
+        P.fof(xp, n_threads=300)
+    with pytest.raises(ValueError):
+        P.fof(np.zeros((2, 5)))
+    with pytest.raises(ValueError):
+        P.fof(xp, bound_check=True)
+    with pytest.raises(ValueError):
+        P.fof(xp, vp_list=[xp, xp])
+    with pytest.raises(ValueError):
+        P.fof(xp, mp_list=-1.0)
+    with pytest.raises(ValueError):
+        P.fof(xp, z=-1.0)
+    with pytest.raises(ValueError):
+        P.fof(xp, vp_list=xp, bound_check=True, units="physical")
+    with pytest.raises(ValueError):
+        P.fof(xp, vp_list=xp, bound_check=True, units="physical", softening=0.1)
+
+
+def test_empty_input_returns_zeros():
+    r = P._fof_core([np.zeros((3, 0)), np.zeros((3, 0))])
+    assert r[0].shape == (0,) and r[1].shape == (0,) and r[2].shape == (3, 2)
+
+
+def test_prepare_units():
+    xp = np.random.default_rng(0).uniform(0, 10, (3, 20))
+    c = P._prepare(xp, units="physical", L_Box=300.0, linking_length=0.1)
+    assert c.L_Box == 512.0
+    assert np.allclose(c.xp, xp / (300.0 / 512.0))
+    c = P._prepare(xp, ng_global=256.0, L_Box=128.0)
+    assert np.isclose(c.s_15_val, 15 * 0.67 * 256.0 / 300.0)
+
+
+def test_catalogue_from_ids():
+    hid = np.array([0, 2, 1, 2, 0, 1, 3], np.int32)
+    res = P.catalogue_from_ids(hid > 0, hid)
+    assert res["nhalo_found"] == 3
+    assert [list(h) for h in res["halo_indices"]] == [[2, 5], [1, 3], [6]]
+    assert list(res["np_per_halo"]) == [2, 2, 1]
