@@ -54,6 +54,17 @@ int32_t pyfof_last_error(char *buf, int64_t len);
  * product path), "timing" (1 = record stage times). */
 int32_t pyfof_set_option(const char *key, int64_t value);
 
+/* Issue all later work of the selected device on `stream` (a cudaStream_t;
+ * NULL restores the library's own stream).  Lets a caller order calls with
+ * its own work and time them with events on that stream. */
+int32_t pyfof_set_stream(void *stream);
+
+/* Counters: "launches" (kernels launched by this process so far), and for
+ * the last call on the selected device "cells" (reference cell grid size),
+ * "active" (particles in linked regions), "candidates" (FoF groups with at
+ * least np_halo_min members). */
+int32_t pyfof_get_stat(const char *key, int64_t *value);
+
 /* Device time of the linking kernel of the last call, when timing is on. */
 int32_t pyfof_last_link_ms(float *ms);
 

@@ -32,7 +32,8 @@ _RUN_ARGS = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, 
 
 # every symbol include/pyfof_b200.h declares
 EXPORTED = ("pyfof_version", "pyfof_init", "pyfof_shutdown", "pyfof_last_error",
-            "pyfof_set_option", "pyfof_last_link_ms", "pyfof_run", "pyfof_run_device")
+            "pyfof_set_option", "pyfof_set_stream", "pyfof_get_stat", "pyfof_last_link_ms", "pyfof_run",
+            "pyfof_run_device")
 
 
 class NativeLibraryError(RuntimeError):
@@ -57,6 +58,10 @@ def load():
         L.pyfof_last_error.argtypes = [ctypes.c_char_p, ctypes.c_int64]
         L.pyfof_set_option.restype = ctypes.c_int32
         L.pyfof_set_option.argtypes = [ctypes.c_char_p, ctypes.c_int64]
+        L.pyfof_set_stream.restype = ctypes.c_int32
+        L.pyfof_set_stream.argtypes = [ctypes.c_void_p]
+        L.pyfof_get_stat.restype = ctypes.c_int32
+        L.pyfof_get_stat.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
         L.pyfof_last_link_ms.restype = ctypes.c_int32
         L.pyfof_last_link_ms.argtypes = [ctypes.POINTER(ctypes.c_float)]
         L.pyfof_run.restype = ctypes.c_int32
@@ -80,6 +85,19 @@ def last_error() -> str:
 def set_option(key: str, value: int) -> None:
     if load().pyfof_set_option(key.encode(), int(value)) != 0:
         raise ValueError(last_error())
+
+
+def set_stream(stream_handle: int) -> None:
+    """Issue library work on the given cudaStream_t (0 = library stream)."""
+    if load().pyfof_set_stream(ctypes.c_void_p(stream_handle) if stream_handle else None) != 0:
+        raise RuntimeError(last_error())
+
+
+def get_stat(key: str) -> int:
+    v = ctypes.c_int64(0)
+    if load().pyfof_get_stat(key.encode(), ctypes.byref(v)) != 0:
+        raise ValueError(last_error())
+    return int(v.value)
 
 
 def last_link_ms() -> float:

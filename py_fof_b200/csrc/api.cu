@@ -10,6 +10,8 @@
 
 namespace pyfof {
 
+std::atomic<int64_t> g_launches{0};
+
 namespace {
 thread_local std::string g_last_error;
 std::mutex g_ctx_mu;
@@ -34,8 +36,9 @@ Context::~Context() {
   if (stream) {
     cudaStreamSynchronize(stream);
     work.release();
-    cudaStreamDestroy(stream);
+    cudaStreamSynchronize(stream);
   }
+  if (own_stream) cudaStreamDestroy(own_stream);
   for (auto &e : ev) if (e) cudaEventDestroy(e);
   if (d_flags) cudaFree(d_flags);
   if (h_flags) cudaFreeHost(h_flags);
@@ -57,7 +60,8 @@ int32_t get_context(int device, Context **out) {
     PYFOF_CUDA(cudaSetDevice(device));
     Context *c = new Context();
     c->device = device;
-    PYFOF_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    PYFOF_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
     PYFOF_CUDA(cudaMalloc(&c->d_flags, sizeof(int32_t) * FLAG_COUNT));
     PYFOF_CUDA(cudaMallocHost(&c->h_flags, sizeof(int32_t) * FLAG_COUNT));
     for (auto &e : c->ev) PYFOF_CUDA(cudaEventCreate(&e));
@@ -159,6 +163,30 @@ int32_t pyfof_set_option(const char *key, int64_t value) {
   if (!std::strcmp(key, "unbind_fp64")) { g_bound_fp64 = value != 0; return kOk; }
   if (!std::strcmp(key, "timing")) { g_timing = value != 0; return kOk; }
   set_error("unknown option %s", key);
+  return kInvalid;
+}
+
+int32_t pyfof_set_stream(void *stream) {
+  Context *c;
+  PYFOF_TRY(get_context(g_default_device, &c));
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaStreamSynchronize(c->stream);
+  if (!c->own_stream) PYFOF_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  c->work.stream = c->stream;
+  return kOk;
+}
+
+int32_t pyfof_get_stat(const char *key, int64_t *value) {
+  if (!key || !value) return kInvalid;
+  if (!std::strcmp(key, "launches")) { *value = g_launches.load(); return kOk; }
+  Context *c;
+  PYFOF_TRY(get_context(g_default_device, &c));
+  if (!std::strcmp(key, "cells")) { *value = c->last_cells; return kOk; }
+  if (!std::strcmp(key, "active")) { *value = c->last_active; return kOk; }
+  if (!std::strcmp(key, "candidates")) { *value = c->last_candidates; return kOk; }
+  if (!std::strcmp(key, "dense_cells")) { *value = c->last_dense; return kOk; }
+  set_error("unknown statistic %s", key);
   return kInvalid;
 }
 

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -33,6 +34,15 @@ std::string last_error();
                          cudaGetErrorString(e_));                               \
       return ::pyfof::kCuda;                                                    \
     }                                                                           \
+  } while (0)
+
+// Counts kernel launches (exposed through pyfof_get_stat("launches")) and
+// checks the launch status.
+extern std::atomic<int64_t> g_launches;
+#define PYFOF_CHECK_LAUNCH()                                                   \
+  do {                                                                         \
+    ::pyfof::g_launches.fetch_add(1, std::memory_order_relaxed);               \
+    PYFOF_CUDA(cudaGetLastError());                                            \
   } while (0)
 
 #define PYFOF_TRY(expr)              \

@@ -13,7 +13,8 @@ struct GreenTable;  // unbinding Green's function cache entry (unbind.cu)
 
 struct Context {
   int device = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // stream all work is issued on
+  cudaStream_t own_stream = nullptr;  // the context's own stream (default)
   Arena work;    // per-call device memory, released at the end of every call
   int32_t *d_flags = nullptr;  // device status words (error codes, counters)
   int32_t *h_flags = nullptr;  // pinned mirror
@@ -23,6 +24,8 @@ struct Context {
   // timing of the last call's stages (ms), filled when timing is enabled
   bool timing = false;
   float stage_ms[16] = {};
+  // statistics of the last call
+  int64_t last_cells = 0, last_active = 0, last_candidates = 0, last_dense = 0;
   ~Context();
 };
 

@@ -210,53 +210,246 @@ __device__ __forceinline__ bool linked_pbc(float4 a, float4 b, const LinkParams 
   return r2 <= P.rp2;
 }
 
-__global__ void __launch_bounds__(BLK) fof_link_kernel(
+// Cells with more than DENSE_T particles carry a sub-cell index (sub[d]
+// slabs per axis, each at least one linking length wide): the particles of
+// the cell are listed by sub-cell in dpos[], sub_tab holds the offsets.  A
+// pair test against such a cell only visits the sub-cells that overlap the
+// cube of half-width `reach` around the particle, which contains every
+// partner the exact distance test can accept.
+constexpr int DENSE_T = 12;
+constexpr int SUB_MAX = 216;
+
+struct DenseIndex {
+  const uint32_t *rank;  // exclusive scan of dense-cell flags, per cell
+  const uint32_t *tab;   // per dense cell: S+1 offsets (relative to cell start)
+  const float4 *dpos;    // dense cells' particles listed by sub-cell; .w = sorted position
+  const uint32_t *order; // work order: dense-cell particles first, then the rest
+  int stride;            // entries per dense cell in tab
+  float reach;           // linking length plus FP32 rounding slack
+};
+
+// Sub-cell of a coordinate inside a cell whose lower corner is lo.  FP32,
+// monotone in x; the same function places particles and bounds queries, and
+// `reach` carries slack for the FP32 rounding of the query endpoints.
+__device__ __forceinline__ int sub_of(float x, float lo, float inv_sub, int s) {
+  float t = floorf(__fmul_rn(__fsub_rn(x, lo), inv_sub));
+  if (!(t >= 0.0f)) t = 0.0f;
+  if (t > (float)(s - 1)) t = (float)(s - 1);
+  return (int)t;
+}
+
+__device__ __forceinline__ float cell_lower(const RegionDev &r, int d, int64_t i) {
+  return __double2float_rn(__dadd_rn(r.origin[d], __dmul_rn((double)i, r.size[d])));
+}
+
+// Union of a linked pair (p, q); rp caches p's root between calls.
+__device__ __forceinline__ void link_pair(int *parent, int p, int q, int &rp, int32_t *flags) {
+  if (rp < 0) rp = dsu_find(parent, p);
+  const int y = __ldcg(parent + q);
+  if (y == rp) return;  // q already hangs directly under p's root
+  const int rq = dsu_find(parent, q);
+  if (rq != rp) {
+    dsu_union(parent, rp, rq, flags);
+    rp = dsu_find(parent, rp);
+  }
+}
+
+__global__ void __launch_bounds__(BLK, 3) fof_link_kernel(
     const float4 *__restrict__ pos, const uint32_t *__restrict__ skey,
     const uint32_t *__restrict__ prid, const RegionDev *__restrict__ R,
     const uint32_t *__restrict__ cell_start, int *parent, int64_t n_active, LinkParams P,
-    int32_t *flags) {
-  for (int64_t p = (int64_t)blockIdx.x * BLK + threadIdx.x; p < n_active;
-       p += (int64_t)gridDim.x * BLK) {
+    DenseIndex D, int32_t *flags) {
+  for (int64_t w = (int64_t)blockIdx.x * BLK + threadIdx.x; w < n_active;
+       w += (int64_t)gridDim.x * BLK) {
+    const int64_t p = D.order[w];
     const float4 me = pos[p];
     const RegionDev &r = R[prid[p]];
     const int64_t local = (int64_t)skey[p] - (int64_t)r.cell_off;
     const int64_t N0 = r.N[0], N1 = r.N[1], N2 = r.N[2];
-    const int64_t ix = local % N0, iy = (local / N0) % N1, iz = local / (N0 * N1);
-    const bool per = r.periodic != 0;
-    int lo[3], hi[3];
+    int64_t ixyz[3];
+    if (r.ncell <= 0xffffffffll) {
+      const uint32_t l32 = (uint32_t)local, n0 = (uint32_t)N0, n1 = (uint32_t)N1;
+      const uint32_t q0 = l32 / n0;
+      ixyz[0] = l32 - q0 * n0;
+      ixyz[1] = q0 % n1;
+      ixyz[2] = q0 / n1;
+    } else {
+      ixyz[0] = local % N0;
+      ixyz[1] = (local / N0) % N1;
+      ixyz[2] = local / (N0 * N1);
+    }
     const int64_t Nd[3] = {N0, N1, N2};
+    const bool per = r.periodic != 0;
+    const float mexyz[3] = {me.x, me.y, me.z};
+    // neighbour offsets per axis: only cells the cube of half-width `reach`
+    // around p can touch (any linked partner lies inside that cube)
+    int lo[3], hi[3];
+#pragma unroll
     for (int d = 0; d < 3; ++d) {
-      if (Nd[d] == 1) { lo[d] = 0; hi[d] = 0; }
-      else if (((r.pdim >> d) & 1) && Nd[d] == 2) { lo[d] = 0; hi[d] = 1; }
-      else { lo[d] = -1; hi[d] = 1; }
+      const bool pd = (r.pdim >> d) & 1;
+      if (Nd[d] == 1) { lo[d] = 0; hi[d] = 0; continue; }
+      const float clo = cell_lower(r, d, ixyz[d]);
+      const float chi = cell_lower(r, d, ixyz[d] + 1);
+      const bool below = __fsub_rn(mexyz[d], D.reach) < clo;
+      const bool above = __fadd_rn(mexyz[d], D.reach) >= chi;
+      if (pd && Nd[d] == 2) { lo[d] = 0; hi[d] = (below || above) ? 1 : 0; }
+      else { lo[d] = below ? -1 : 0; hi[d] = above ? 1 : 0; }
     }
     const int ip = (int)p;
+    int rp = -1;  // cached root of p
     for (int dz = lo[2]; dz <= hi[2]; ++dz) {
-      int64_t jz = iz + dz;
-      if ((r.pdim >> 2) & 1) jz = (jz + N2) % N2;
-      else if (jz < 0 || jz >= N2) continue;
+      int64_t jz = ixyz[2] + dz;
+      double shz = 0.0;
+      if ((r.pdim >> 2) & 1) {
+        if (jz < 0) { jz += N2; shz = P.L; } else if (jz >= N2) { jz -= N2; shz = -P.L; }
+      } else if (jz < 0 || jz >= N2) continue;
       for (int dy = lo[1]; dy <= hi[1]; ++dy) {
-        int64_t jy = iy + dy;
-        if ((r.pdim >> 1) & 1) jy = (jy + N1) % N1;
-        else if (jy < 0 || jy >= N1) continue;
+        int64_t jy = ixyz[1] + dy;
+        double shy = 0.0;
+        if ((r.pdim >> 1) & 1) {
+          if (jy < 0) { jy += N1; shy = P.L; } else if (jy >= N1) { jy -= N1; shy = -P.L; }
+        } else if (jy < 0 || jy >= N1) continue;
         for (int dx = lo[0]; dx <= hi[0]; ++dx) {
-          int64_t jx = ix + dx;
-          if (r.pdim & 1) jx = (jx + N0) % N0;
-          else if (jx < 0 || jx >= N0) continue;
+          int64_t jx = ixyz[0] + dx;
+          double shx = 0.0;
+          if (r.pdim & 1) {
+            if (jx < 0) { jx += N0; shx = P.L; } else if (jx >= N0) { jx -= N0; shx = -P.L; }
+          } else if (jx < 0 || jx >= N0) continue;
           const int64_t jl = jx + N0 * (jy + N1 * jz);
           if (jl < local) continue;
           const uint64_t jc = r.cell_off + (uint64_t)jl;
-          int64_t b = cell_start[jc];
+          const int64_t b = cell_start[jc];
           const int64_t e = cell_start[jc + 1];
-          if (jl == local) b = p + 1;
-          for (int64_t q = b; q < e; ++q) {
-            const float4 o = pos[q];
-            const bool lk = per ? linked_pbc(me, o, P) : linked_open(me, o, P.rp2_open);
-            if (lk) dsu_union(parent, ip, (int)q, flags);
+          const bool own = (jl == local);
+          if (e - b > DENSE_T && r.sub_ok) {
+            const uint32_t *tab = D.tab + (int64_t)D.rank[jc] * D.stride;
+            const int64_t jcoord[3] = {jx, jy, jz};
+            const double sh[3] = {shx, shy, shz};
+            int slo[3], shi[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              const float clo = cell_lower(r, d, jcoord[d]);
+              const float xs = __fadd_rn(mexyz[d], (float)sh[d]);
+              slo[d] = sub_of(__fsub_rn(xs, D.reach), clo, r.inv_sub[d], r.sub[d]);
+              shi[d] = sub_of(__fadd_rn(xs, D.reach), clo, r.inv_sub[d], r.sub[d]);
+            }
+            for (int sz = slo[2]; sz <= shi[2]; ++sz)
+              for (int sy = slo[1]; sy <= shi[1]; ++sy) {
+                const int s0 = slo[0] + r.sub[0] * (sy + r.sub[1] * sz);
+                const int64_t k0 = tab[s0], k1 = tab[s0 + (shi[0] - slo[0]) + 1];
+                for (int64_t k = k0; k < k1; ++k) {
+                  const float4 o = D.dpos[b + k];
+                  const int q = __float_as_int(o.w);
+                  if (own && q <= ip) continue;
+                  const bool lk = per ? linked_pbc(me, o, P) : linked_open(me, o, P.rp2_open);
+                  if (lk) link_pair(parent, ip, q, rp, flags);
+                }
+              }
+          } else {
+            for (int64_t q = own ? p + 1 : b; q < e; ++q) {
+              const float4 o = pos[q];
+              const bool lk = per ? linked_pbc(me, o, P) : linked_open(me, o, P.rp2_open);
+              if (lk) link_pair(parent, ip, (int)q, rp, flags);
+            }
           }
         }
       }
     }
+  }
+}
+
+__global__ void fof_dense_flag_kernel(const uint32_t *__restrict__ cs,
+                                      const uint64_t *__restrict__ cell_off,
+                                      const RegionDev *__restrict__ R, int nreg, int64_t ncell,
+                                      uint32_t *__restrict__ flag) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncell;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t f = 0;
+    if (cs[c + 1] - cs[c] > (uint32_t)DENSE_T) {
+      const int rid = nreg == 1 ? 0 : region_of_key(cell_off, nreg, (uint64_t)c);
+      f = R[rid].sub_ok ? 1u : 0u;
+    }
+    flag[c] = f;
+  }
+}
+
+__global__ void fof_dense_pos_flag_kernel(const uint32_t *__restrict__ skey,
+                                          const uint32_t *__restrict__ cflag, int64_t n,
+                                          uint32_t *__restrict__ pflag) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x)
+    pflag[p] = cflag[skey[p]];
+}
+
+// Dense-cell particles first (they carry most of the pair tests, so they
+// start early), the rest after them; both parts keep the sorted order.
+__global__ void fof_order_kernel(const uint32_t *__restrict__ pflag,
+                                 const uint32_t *__restrict__ prank, int64_t n, int64_t ndense_p,
+                                 uint32_t *__restrict__ order) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = pflag[p] ? (int64_t)prank[p] : ndense_p + (p - (int64_t)prank[p]);
+    order[k] = (uint32_t)p;
+  }
+}
+
+__global__ void fof_dense_list_kernel(const uint32_t *__restrict__ flag,
+                                      const uint32_t *__restrict__ rank, int64_t ncell,
+                                      uint32_t *__restrict__ list) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncell;
+       c += (int64_t)gridDim.x * blockDim.x)
+    if (flag[c]) list[rank[c]] = (uint32_t)c;
+}
+
+// One block per dense cell: counting sort of its particles by sub-cell.
+__global__ void __launch_bounds__(BLK) fof_dense_build_kernel(
+    const uint32_t *__restrict__ list, const uint32_t *__restrict__ cs,
+    const float4 *__restrict__ pos, const RegionDev *__restrict__ R,
+    const uint64_t *__restrict__ cell_off, int nreg, int stride, uint32_t *__restrict__ tab,
+    float4 *__restrict__ dpos) {
+  __shared__ uint32_t hist[SUB_MAX + 1];
+  __shared__ uint32_t cur[SUB_MAX + 1];
+  const uint32_t c = list[blockIdx.x];
+  const int rid = nreg == 1 ? 0 : region_of_key(cell_off, nreg, (uint64_t)c);
+  const RegionDev &r = R[rid];
+  const int64_t local = (int64_t)c - (int64_t)r.cell_off;
+  const int64_t N0 = r.N[0], N1 = r.N[1];
+  const int64_t ic[3] = {local % N0, (local / N0) % N1, local / (N0 * N1)};
+  float clo[3];
+  for (int d = 0; d < 3; ++d) clo[d] = cell_lower(r, d, ic[d]);
+  const int S = r.sub[0] * r.sub[1] * r.sub[2];
+  for (int k = threadIdx.x; k <= SUB_MAX; k += BLK) hist[k] = 0;
+  __syncthreads();
+  const int64_t base = cs[c];
+  const int64_t n = (int64_t)cs[c + 1] - base;
+  for (int64_t k = threadIdx.x; k < n; k += BLK) {
+    const float4 v = pos[base + k];
+    const int sx = sub_of(v.x, clo[0], r.inv_sub[0], r.sub[0]);
+    const int sy = sub_of(v.y, clo[1], r.inv_sub[1], r.sub[1]);
+    const int sz = sub_of(v.z, clo[2], r.inv_sub[2], r.sub[2]);
+    atomicAdd(&hist[sx + r.sub[0] * (sy + r.sub[1] * sz)], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    for (int k = 0; k < S; ++k) {
+      const uint32_t h = hist[k];
+      cur[k] = run;
+      run += h;
+    }
+    cur[S] = run;
+  }
+  __syncthreads();
+  uint32_t *t = tab + (int64_t)blockIdx.x * stride;
+  for (int k = threadIdx.x; k <= S; k += BLK) t[k] = cur[k];
+  __syncthreads();
+  for (int64_t k = threadIdx.x; k < n; k += BLK) {
+    const float4 v = pos[base + k];
+    const int sx = sub_of(v.x, clo[0], r.inv_sub[0], r.sub[0]);
+    const int sy = sub_of(v.y, clo[1], r.inv_sub[1], r.sub[1]);
+    const int sz = sub_of(v.z, clo[2], r.inv_sub[2], r.sub[2]);
+    const uint32_t slot = atomicAdd(&cur[sx + r.sub[0] * (sy + r.sub[1] * sz)], 1u);
+    dpos[base + slot] = make_float4(v.x, v.y, v.z, __int_as_float((int)(base + k)));
   }
 }
 
@@ -266,13 +459,19 @@ __global__ void fof_init_parent(int *parent, int64_t n) {
     parent[p] = (int)p;
 }
 
-__global__ void __launch_bounds__(BLK) fof_root_kernel(int *parent, uint32_t *gsize, int64_t n) {
+// Final labels.  The forest is static after linking; find() may still
+// shorten paths with halving stores (each store points a node at one of its
+// ancestors, so concurrent finds stay correct), but the label of every
+// particle goes to a separate array: a store into parent[] could be
+// overwritten by another thread's halving store with a non-root ancestor.
+__global__ void __launch_bounds__(BLK) fof_root_kernel(int *parent, int *lab, uint32_t *gsize,
+                                                       int64_t n) {
   for (int64_t base = (int64_t)blockIdx.x * BLK; base < n; base += (int64_t)gridDim.x * BLK) {
     const int64_t p = base + threadIdx.x;
     int root = -1;
     if (p < n) {
       root = dsu_find(parent, (int)p);
-      parent[p] = root;
+      lab[p] = root;
     }
     const unsigned peers = __match_any_sync(0xffffffffu, root);
     const int leader = __ffs(peers) - 1;
@@ -280,22 +479,22 @@ __global__ void __launch_bounds__(BLK) fof_root_kernel(int *parent, uint32_t *gs
   }
 }
 
-__global__ void fof_cand_flag_kernel(const int *parent, const uint32_t *gsize, int64_t n,
+__global__ void fof_cand_flag_kernel(const int *lab, const uint32_t *gsize, int64_t n,
                                      uint32_t np_min, uint32_t *flag) {
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
        p += (int64_t)gridDim.x * blockDim.x)
-    flag[p] = (parent[p] == (int)p && gsize[p] >= np_min) ? 1u : 0u;
+    flag[p] = (lab[p] == (int)p && gsize[p] >= np_min) ? 1u : 0u;
 }
 
 // Candidate of every sorted particle (-1 if its group is too small), plus
 // the no-unbinding outputs (fof_fortran.f90:207-222).
-__global__ void fof_member_kernel(const int *parent, const uint32_t *gsize,
+__global__ void fof_member_kernel(const int *lab, const uint32_t *gsize,
                                   const uint32_t *crank, const float4 *pos, int64_t n,
                                   uint32_t np_min, int write_out, int32_t *pcand,
                                   int32_t *in_halo, int32_t *halo_id) {
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
        p += (int64_t)gridDim.x * blockDim.x) {
-    const int r = parent[p];
+    const int r = lab[p];
     int32_t c = -1;
     if (gsize[r] >= np_min) c = (int32_t)crank[r];
     pcand[p] = c;
@@ -442,6 +641,19 @@ void region_geometry(double L, double link, int32_t np, const double *xmin, cons
   r.pdim = pd;
   r.periodic = pd != 0;
   r.ncell = N[0] * N[1] * N[2];
+  // sub-cells for dense cells: slabs at least one linking length wide; none
+  // along periodic axes with fewer than 3 cells (both images are adjacent)
+  int prod = 1;
+  for (int d = 0; d < 3; ++d) {
+    int sd = (int)std::floor(r.size[d] / link);
+    if (sd < 1 || !std::isfinite(r.size[d] / link)) sd = 1;
+    if (sd > 6) sd = 6;
+    if (((pd >> d) & 1) && N[d] < 3) sd = 1;
+    r.sub[d] = sd;
+    prod *= sd;
+  }
+  r.sub_ok = prod > 1 ? 1 : 0;
+  for (int d = 0; d < 3; ++d) r.inv_sub[d] = (float)((double)r.sub[d] / r.size[d]);
 }
 
 int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
@@ -490,7 +702,7 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
   PYFOF_CUDA(cudaMemsetAsync(ctx.d_flags, 0, sizeof(int32_t) * FLAG_COUNT, s));
   if (ntiles) {
     fof_bbox_kernel<<<(unsigned)ntiles, BLK, 0, s>>>(xp, dR, dT, L, half, dbb, ctx.d_flags);
-    PYFOF_CUDA(cudaGetLastError());
+    PYFOF_CHECK_LAUNCH();
   }
   std::vector<unsigned long long> bb(6 * (size_t)nreg);
   PYFOF_CUDA(cudaMemcpyAsync(bb.data(), dbb, sizeof(unsigned long long) * bb.size(),
@@ -529,6 +741,8 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
   }
   st.n_active = n_active;
   st.total_cells = total_cells;
+  ctx.last_cells = (int64_t)total_cells;
+  ctx.last_active = n_active;
   PYFOF_CUDA(cudaMemcpyAsync(dR, reg.data(), sizeof(RegionDev) * nreg, cudaMemcpyHostToDevice, s));
   uint64_t *dcoff = W.carve<uint64_t>(nreg + 1);
   uint32_t *keys = W.carve<uint32_t>(std::max<int64_t>(n, 1));
@@ -547,11 +761,12 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
   const uint32_t sentinel = (uint32_t)total_cells;
   if (ntiles) {
     fof_key_kernel<<<(unsigned)ntiles, BLK, 0, s>>>(xp, dR, dT, L, half, sentinel, keys, cstart);
-    PYFOF_CUDA(cudaGetLastError());
+    PYFOF_CHECK_LAUNCH();
   }
   PYFOF_TRY(exclusive_scan_u32(cstart, cstart, (int64_t)total_cells + 1, nullptr, W, s));
   uint32_t *skey, *sidx;
-  PYFOF_TRY(radix_sort_pairs(keys, nullptr, n, bits_for(total_cells), ka, va, kb, vb, &skey, &sidx,
+  const uint64_t max_key = (n_active < n) ? total_cells : (total_cells ? total_cells - 1 : 0);
+  PYFOF_TRY(radix_sort_pairs(keys, nullptr, n, bits_for(max_key), ka, va, kb, vb, &skey, &sidx,
                              W, s));
   // --- sorted FP32 coordinates, DSU
   float4 *pos = W.carve<float4>(std::max<int64_t>(n_active, 1));
@@ -563,9 +778,9 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
   if (n_active > 0) {
     fof_gather_kernel<<<grid, BLK, 0, s>>>(xp, dR, dcoff, nreg, skey, sidx, n_active, L, half, pos,
                                            prid);
-    PYFOF_CUDA(cudaGetLastError());
+    PYFOF_CHECK_LAUNCH();
     fof_init_parent<<<grid, BLK, 0, s>>>(parent, n_active);
-    PYFOF_CUDA(cudaGetLastError());
+    PYFOF_CHECK_LAUNCH();
     LinkParams P;
     P.L = L;
     P.half = half;
@@ -578,10 +793,60 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
     P.fast_periodic = (P.rp2 > 1e-20 && P.rp2 < 1e20 && L < 1e30) ? 1 : 0;
     P.rp2_lo = (float)(P.rp2 * (1.0 - 4e-6));
     P.rp2_hi = (float)(P.rp2 * (1.0 + 4e-6));
+    DenseIndex D{};
+    // slack: relative 1e-4 for the FP32 distance arithmetic, 8 FP32 ulps of
+    // the box size for the rounding of positions and query endpoints
+    D.reach = (float)(a.link * (1.0 + 1e-4) + 8.0 * 1.1920928955078125e-07 * (std::fabs(L) + 1.0));
+    {
+      int smax = 1;
+      for (int r = 0; r < nreg; ++r)
+        if (reg[r].active) smax = std::max(smax, reg[r].sub[0] * reg[r].sub[1] * reg[r].sub[2]);
+      D.stride = smax + 1;
+      const int64_t nc = (int64_t)total_cells;
+      uint32_t *dflag = W.carve<uint32_t>(nc + 1);
+      uint32_t *drank = W.carve<uint32_t>(nc + 1);
+      float4 *dpos = W.carve<float4>(n_active);
+      uint32_t *order = W.carve<uint32_t>(n_active);
+      uint32_t *pflag = W.carve<uint32_t>(n_active + 1);
+      uint32_t *prank = W.carve<uint32_t>(n_active + 1);
+      if (!dflag || !drank || !dpos || !order || !pflag || !prank) {
+        set_error("workspace exhausted (dense index)");
+        return kAlloc;
+      }
+      const unsigned cgrid = (unsigned)std::min<int64_t>(ceil_div(nc, BLK), (int64_t)kNumSMs * 16);
+      fof_dense_flag_kernel<<<cgrid, BLK, 0, s>>>(cstart, dcoff, dR, nreg, nc, dflag);
+      PYFOF_CHECK_LAUNCH();
+      PYFOF_TRY(exclusive_scan_u32(dflag, drank, nc, reinterpret_cast<uint32_t *>(ctx.d_flags + FLAG_COUNT_B), W, s));
+      fof_dense_pos_flag_kernel<<<grid, BLK, 0, s>>>(skey, dflag, n_active, pflag);
+      PYFOF_CHECK_LAUNCH();
+      PYFOF_TRY(exclusive_scan_u32(pflag, prank, n_active, reinterpret_cast<uint32_t *>(ctx.d_flags + FLAG_COUNT_C), W, s));
+      PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t) * FLAG_COUNT,
+                                 cudaMemcpyDeviceToHost, s));
+      PYFOF_CUDA(cudaStreamSynchronize(s));
+      const int64_t ndense = (uint32_t)ctx.h_flags[FLAG_COUNT_B];
+      const int64_t ndense_p = (uint32_t)ctx.h_flags[FLAG_COUNT_C];
+      fof_order_kernel<<<grid, BLK, 0, s>>>(pflag, prank, n_active, ndense_p, order);
+      PYFOF_CHECK_LAUNCH();
+      uint32_t *tab = W.carve<uint32_t>(std::max<int64_t>(ndense, 1) * D.stride);
+      uint32_t *list = W.carve<uint32_t>(std::max<int64_t>(ndense, 1));
+      if (!tab || !list) { set_error("workspace exhausted (dense tables)"); return kAlloc; }
+      if (ndense > 0) {
+        fof_dense_list_kernel<<<cgrid, BLK, 0, s>>>(dflag, drank, nc, list);
+        PYFOF_CHECK_LAUNCH();
+        fof_dense_build_kernel<<<(unsigned)ndense, BLK, 0, s>>>(list, cstart, pos, dR, dcoff, nreg,
+                                                                D.stride, tab, dpos);
+        PYFOF_CHECK_LAUNCH();
+      }
+      D.rank = drank;
+      D.tab = tab;
+      D.dpos = dpos;
+      D.order = order;
+      ctx.last_dense = ndense;
+    }
     if (ctx.timing) cudaEventRecord(ctx.ev[0], s);
-    fof_link_kernel<<<grid, BLK, 0, s>>>(pos, skey, prid, dR, cstart, parent, n_active, P,
+    fof_link_kernel<<<grid, BLK, 0, s>>>(pos, skey, prid, dR, cstart, parent, n_active, P, D,
                                          ctx.d_flags);
-    PYFOF_CUDA(cudaGetLastError());
+    PYFOF_CHECK_LAUNCH();
     if (ctx.timing) cudaEventRecord(ctx.ev[1], s);
   }
   st.dR = dR;
@@ -609,15 +874,16 @@ int32_t fof_candidates_stage(Context &ctx, const FofArgs &a, FofState &st, bool 
   if (na > 0) {
     const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(na, BLK), (int64_t)kNumSMs * 16);
     PYFOF_CUDA(cudaMemsetAsync(gsize, 0, sizeof(uint32_t) * na, s));
-    fof_root_kernel<<<grid, BLK, 0, s>>>(st.parent, gsize, na);
-    PYFOF_CUDA(cudaGetLastError());
-    fof_cand_flag_kernel<<<grid, BLK, 0, s>>>(st.parent, gsize, na, (uint32_t)a.np_halo_min, flag);
-    PYFOF_CUDA(cudaGetLastError());
+    st.lab = reinterpret_cast<int *>(st.keys_free);  // keys are dead after the sort
+    fof_root_kernel<<<grid, BLK, 0, s>>>(st.parent, st.lab, gsize, na);
+    PYFOF_CHECK_LAUNCH();
+    fof_cand_flag_kernel<<<grid, BLK, 0, s>>>(st.lab, gsize, na, (uint32_t)a.np_halo_min, flag);
+    PYFOF_CHECK_LAUNCH();
     PYFOF_TRY(exclusive_scan_u32(flag, crank, na, reinterpret_cast<uint32_t *>(ctx.d_flags + FLAG_COUNT_A), W, s));
-    fof_member_kernel<<<grid, BLK, 0, s>>>(st.parent, gsize, crank, st.pos, na,
+    fof_member_kernel<<<grid, BLK, 0, s>>>(st.lab, gsize, crank, st.pos, na,
                                            (uint32_t)a.np_halo_min, write_plain ? 1 : 0, pcand,
                                            a.in_halo, a.halo_id);
-    PYFOF_CUDA(cudaGetLastError());
+    PYFOF_CHECK_LAUNCH();
     PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t) * FLAG_COUNT,
                                cudaMemcpyDeviceToHost, s));
     PYFOF_CUDA(cudaStreamSynchronize(s));
@@ -627,6 +893,7 @@ int32_t fof_candidates_stage(Context &ctx, const FofArgs &a, FofState &st, bool 
     }
     st.ncand = (uint32_t)ctx.h_flags[FLAG_COUNT_A];
   }
+  ctx.last_candidates = st.ncand;
   st.gsize = gsize;
   st.flag = flag;
   st.crank = crank;
@@ -645,7 +912,7 @@ int32_t fof_candidates_stage(Context &ctx, const FofArgs &a, FofState &st, bool 
     fof_cand_info_kernel<<<grid, BLK, 0, s>>>(flag, crank, st.pos, st.prid, gsize, na,
                                               st.cand_anchor, st.cand_region, st.cand_np,
                                               st.cand_root);
-    PYFOF_CUDA(cudaGetLastError());
+    PYFOF_CHECK_LAUNCH();
   }
   return kOk;
 }
@@ -668,10 +935,10 @@ int32_t fof_plain_angmom(Context &ctx, const FofArgs &a, FofState &st) {
     const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(na, BLK), (int64_t)kNumSMs * 16);
     fof_com_kernel<<<grid, BLK, 0, s>>>(xp, vp, a.mp, st.pos, st.pcand, st.cand_anchor, na,
                                         a.L_Box, 0.5 * a.L_Box, acc);
-    PYFOF_CUDA(cudaGetLastError());
+    PYFOF_CHECK_LAUNCH();
     fof_angmom_kernel<<<grid, BLK, 0, s>>>(xp, vp, a.mp, st.pos, st.pcand, st.cand_anchor, acc,
                                            na, a.L_Box, 0.5 * a.L_Box, am);
-    PYFOF_CUDA(cudaGetLastError());
+    PYFOF_CHECK_LAUNCH();
     std::vector<double> amc(3 * (size_t)nc);
     std::vector<int32_t> creg(nc);
     PYFOF_CUDA(cudaMemcpyAsync(amc.data(), am, sizeof(double) * 3 * nc, cudaMemcpyDeviceToHost, s));

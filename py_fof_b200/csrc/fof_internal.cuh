@@ -9,7 +9,7 @@
 namespace pyfof {
 
 // Slots of Context::d_flags.
-enum { FLAG_ERR = 0, FLAG_COUNT_A = 1, FLAG_COUNT_B = 2, FLAG_COUNT = 8 };
+enum { FLAG_ERR = 0, FLAG_COUNT_A = 1, FLAG_COUNT_B = 2, FLAG_COUNT_C = 3, FLAG_COUNT = 8 };
 
 // One input region (one element of xp_list) with its reference cell grid.
 struct RegionDev {
@@ -23,7 +23,9 @@ struct RegionDev {
   int32_t pdim;      // bit d set: axis d is periodic
   int32_t periodic;  // any axis periodic: dist2_pbc is used for every pair
   int32_t active;    // np >= np_halo_min
-  int32_t pad;
+  int32_t sub_ok;    // dense cells of this region get a sub-cell index
+  int32_t sub[3];    // sub-cells per axis (each at least one linking length)
+  float inv_sub[3];  // sub-cells per unit length
 };
 
 struct Tile {
@@ -40,7 +42,8 @@ struct FofState {
   RegionDev *dR = nullptr;
   float4 *pos = nullptr;      // sorted FP32 coordinates, .w = original index bits
   uint32_t *prid = nullptr;   // region of each sorted particle
-  int *parent = nullptr;      // DSU over sorted positions; roots after labelling
+  int *parent = nullptr;      // DSU forest over sorted positions
+  int *lab = nullptr;         // root (minimum sorted position) of every particle
   uint32_t *skey = nullptr, *sidx = nullptr, *cell_start = nullptr, *keys_free = nullptr;
   uint32_t *gsize = nullptr, *flag = nullptr, *crank = nullptr;
   int32_t *pcand = nullptr;   // candidate of each sorted particle or -1

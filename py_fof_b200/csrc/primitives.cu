@@ -188,7 +188,7 @@ int32_t exclusive_scan_u32(const uint32_t *in, uint32_t *out, int64_t n, uint32_
   int64_t nb = ceil_div(n, SCAN_TILE);
   if (nb == 1) {
     scan_apply_kernel<<<1, SCAN_THREADS, 0, s>>>(in, out, n, nullptr, total);
-    PYFOF_CUDA(cudaGetLastError());
+    PYFOF_CHECK_LAUNCH();
     return kOk;
   }
   uint32_t *sums = scratch.carve<uint32_t>((size_t)nb);
@@ -198,10 +198,10 @@ int32_t exclusive_scan_u32(const uint32_t *in, uint32_t *out, int64_t n, uint32_
     return kAlloc;
   }
   scan_reduce_kernel<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, n, sums);
-  PYFOF_CUDA(cudaGetLastError());
+  PYFOF_CHECK_LAUNCH();
   PYFOF_TRY(exclusive_scan_u32(sums, offs, nb, nullptr, scratch, s));
   scan_apply_kernel<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, offs, total);
-  PYFOF_CUDA(cudaGetLastError());
+  PYFOF_CHECK_LAUNCH();
   return kOk;
 }
 
@@ -215,7 +215,7 @@ int32_t radix_sort_pairs(const uint32_t *keys_in, const uint32_t *vals_in, int64
   const int passes = bits <= 0 ? 0 : (bits + 7) / 8;
   if (passes == 0) {
     iota_copy_kernel<<<4 * kNumSMs, 256, 0, s>>>(keys_in, vals_in, keys_a, vals_a, n);
-    PYFOF_CUDA(cudaGetLastError());
+    PYFOF_CHECK_LAUNCH();
     return kOk;
   }
   const int64_t ntiles = ceil_div(n, RS_TILE);
@@ -230,10 +230,10 @@ int32_t radix_sort_pairs(const uint32_t *keys_in, const uint32_t *vals_in, int64
   for (int p = 0; p < passes; ++p) {
     const int shift = 8 * p;
     rs_upsweep<<<(unsigned)ntiles, RS_THREADS, 0, s>>>(kin, n, shift, hist, ntiles);
-    PYFOF_CUDA(cudaGetLastError());
+    PYFOF_CHECK_LAUNCH();
     PYFOF_TRY(exclusive_scan_u32(hist, offs, ntiles * RS_BINS, nullptr, scratch, s));
     rs_downsweep<<<(unsigned)ntiles, RS_THREADS, 0, s>>>(kin, vin, ko, vo, n, shift, offs, ntiles);
-    PYFOF_CUDA(cudaGetLastError());
+    PYFOF_CHECK_LAUNCH();
     kin = ko;
     vin = vo;
     *keys_out = ko;

@@ -116,6 +116,32 @@ def test_np_halo_min_extremes(npmin):
     _assert_same(g, o)
 
 
+@pytest.mark.parametrize("L", [30.0, 60.0])
+def test_dense_clumps_across_boundary(L):
+    """Clumps much denser than one particle per cell, some straddling the
+    periodic faces and corners, exercise the sub-cell index of dense cells."""
+    rng = np.random.default_rng(int(L))
+    parts = [rng.uniform(0, L, (3, 20000))]
+    for c in ([0.0, 0.0, 0.0], [L / 2, 0.05, L - 0.05], [L / 3, L / 3, L / 3]):
+        parts.append(np.array(c)[:, None] + rng.normal(0, 0.25, (3, 4000)))
+    xp = np.mod(np.concatenate(parts, axis=1), L)
+    g, o = _both(xp, L_Box=L, linking_length=0.2, np_halo_min=10)
+    assert _native.get_stat("dense_cells") > 0
+    assert o[1].max() >= 3
+    _assert_same(g, o)
+
+
+def test_dense_clumps_open_region():
+    rng = np.random.default_rng(21)
+    parts = [rng.uniform(100, 140, (3, 30000))]
+    for k in range(5):
+        parts.append(rng.uniform(100, 140, (3, 1)) + rng.normal(0, 0.3, (3, 3000)))
+    xp = np.concatenate(parts, axis=1)
+    g, o = _both(xp, L_Box=1000.0, linking_length=0.25, np_halo_min=10)
+    assert _native.get_stat("dense_cells") > 0
+    _assert_same(g, o)
+
+
 def test_fortran_order_input():
     d = W.plummer_box(16 ** 3, 16.0, 2, seed=4)
     xf = np.asfortranarray(d["xp"])
@@ -127,8 +153,11 @@ def test_fortran_order_input():
 def test_empty_and_errors():
     r = P._fof_core(np.zeros((3, 0)))
     assert r[0].shape == (0,) and r[2].shape == (3, 1)
+    bad = np.array([[np.nan, 0.0], [0.0, 0.0], [0.0, 0.0]])
     with pytest.raises(ValueError):
-        P.fof(np.array([[np.nan, 0.0], [0.0, 0.0], [0.0, 0.0]]), L_Box=10.0)
+        P.fof(bad, L_Box=10.0, np_halo_min=1)
+    # a region below np_halo_min is skipped without being read, as in the reference
+    assert not P.fof(bad, L_Box=10.0, np_halo_min=10).any()
 
 
 def test_device_entry_point_matches_host():
