@@ -186,6 +186,9 @@ int32_t pyfof_get_stat(const char *key, int64_t *value) {
   if (!std::strcmp(key, "active")) { *value = c->last_active; return kOk; }
   if (!std::strcmp(key, "candidates")) { *value = c->last_candidates; return kOk; }
   if (!std::strcmp(key, "dense_cells")) { *value = c->last_dense; return kOk; }
+  if (!std::strcmp(key, "direct_halos")) { *value = c->last_direct; return kOk; }
+  if (!std::strcmp(key, "pm_halos")) { *value = c->last_pm; return kOk; }
+  if (!std::strcmp(key, "valid_halos")) { *value = c->last_valid; return kOk; }
   set_error("unknown statistic %s", key);
   return kInvalid;
 }

@@ -50,6 +50,7 @@ struct FofState {
   uint32_t ncand = 0;
   int64_t *cand_anchor = nullptr;  // original index of each candidate's first CRS member
   int32_t *cand_region = nullptr, *cand_np = nullptr, *cand_root = nullptr;
+  float *phi_out = nullptr;   // optional: final potential of every packed member
 };
 
 void region_geometry(double L, double link, int32_t np, const double *xmin, const double *xmax,

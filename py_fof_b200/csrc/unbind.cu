@@ -1,14 +1,756 @@
-// Gravitational unbinding (bound_fortran.f90) -- placeholder until the
-// solver kernels land.
+// Gravitational unbinding of FoF candidates (bound_fortran.f90) on the
+// device: the bound_check=True branch of fof_fortran (fof_fortran.f90:252-360).
+//
+//   1. members of every candidate, ascending global index (the stable-id
+//      order of bound_check_grid, bound_fortran.f90:2504-2528), packed as FP32
+//      positions relative to the candidate anchor, FP32 velocities and masses
+//      (fof_fortran.f90:281-308)
+//   2. per-candidate span and lower corner -> host classification
+//      (bound_classify, :2901-3073): 15 Mpc guard, method/grid/level choice
+//   3. solvers: direct summation (N <= 1000) in one launch with one block
+//      per halo running the whole removal loop; particle-mesh halos in
+//      unbind_pm.cu
+//   4. outputs: kept members of converged halos with >= np_halo_min members,
+//      renumbered in candidate order, and angular momentum per input region
+//      (fof_fortran.f90:313-355)
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
 #include "context.cuh"
+#include "primitives.cuh"
 #include "unbind.cuh"
+#include "unbind_internal.cuh"
 
 namespace pyfof {
 
+namespace {
+
+constexpr int BLK = 256;
+constexpr double kPi = 3.141592653589793238462643383279502884197;
+
+__global__ void ub_mark_kernel(const int32_t *__restrict__ pcand, const float4 *__restrict__ pos,
+                               int64_t n, uint32_t *__restrict__ cand_of) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = pcand[p];
+    if (c >= 0) cand_of[__float_as_int(pos[p].w)] = (uint32_t)c;
+  }
+}
+
+__global__ void ub_fill_kernel(uint32_t *a, int64_t n, uint32_t v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = v;
+}
+
+// xv packing (fof_fortran.f90:297-305): positions unwrapped about the
+// candidate's first CRS member in FP64, then rounded to FP32.
+__global__ void ub_pack_kernel(Coords xp, Coords vp, const double *__restrict__ mp,
+                               const uint32_t *__restrict__ mcand,
+                               const uint32_t *__restrict__ midx,
+                               const int64_t *__restrict__ cand_anchor, int64_t M, double L,
+                               double half, Members m) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t c = mcand[k];
+    const int64_t i = midx[k];
+    const int64_t a = cand_anchor[c];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      m.q[d][k] = __double2float_rn(unwrap(xp.get(i, d), xp.get(a, d), half, L));
+      m.v[d][k] = __double2float_rn(vp.get(i, d));
+    }
+    m.w[k] = mp ? __double2float_rn(mp[i]) : 1.0f;
+    m.pid[k] = (int32_t)i;
+  }
+}
+
+// Span and lower corner of every candidate (bound_classify :2955-2965): the
+// anchor member sits at q = 0; lo and hi start at 0.
+__global__ void __launch_bounds__(BLK) ub_span_kernel(Members m, const int64_t *__restrict__ off,
+                                                      float *__restrict__ lo_out,
+                                                      float *__restrict__ span_out) {
+  const int c = blockIdx.x;
+  const int64_t b = off[c], e = off[c + 1];
+  float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
+  bool bad = false;
+  for (int64_t k = b + threadIdx.x; k < e; k += BLK)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float v = m.q[d][k];
+      bad |= !isfinite(v);
+      lo[d] = fminf(lo[d], v);
+      hi[d] = fmaxf(hi[d], v);
+    }
+  __shared__ float slo[3][BLK / 32], shi[3][BLK / 32];
+  __shared__ int sbad;
+  if (threadIdx.x == 0) sbad = 0;
+  __syncthreads();
+  if (bad) sbad = 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+      hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+    }
+    if (lane == 0) { slo[d][warp] = lo[d]; shi[d][warp] = hi[d]; }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float span = 0.f;
+    for (int d = 0; d < 3; ++d) {
+      float a = slo[d][0], z = shi[d][0];
+      for (int w = 1; w < BLK / 32; ++w) { a = fminf(a, slo[d][w]); z = fmaxf(z, shi[d][w]); }
+      lo_out[3 * c + d] = a;
+      const float s = z - a;
+      span = d == 0 ? s : fmaxf(span, s);
+    }
+    span_out[c] = sbad ? NAN : span;
+  }
+}
+
+// ---------------------------------------------------------------- direct
+
+// bound_depth_continuous (bound_fortran.f90:3080-3102): spline-softened 1/r.
+template <typename T>
+__device__ __forceinline__ T depth_continuous(T r, T h);
+
+template <>
+__device__ __forceinline__ double depth_continuous<double>(double r, double h) {
+  if (r <= 0.0) return __ddiv_rn(208.0, __dmul_rn(70.0, h));
+  if (r >= h) return __ddiv_rn(1.0, r);
+  const double e = __ddiv_rn(__dmul_rn(2.0, r), h);
+  if (e <= 1.0) {
+    double t = __dadd_rn(8.0, __dmul_rn(-3.0, e));
+    t = __dadd_rn(14.0, __dmul_rn(e, t));
+    t = __dadd_rn(-56.0, __dmul_rn(e, t));
+    t = __dadd_rn(112.0, __dmul_rn(__dmul_rn(e, e), t));
+    const double prim = __dmul_rn(__dmul_rn(e, e), t);
+    return __ddiv_rn(__dadd_rn(208.0, -prim), __dmul_rn(70.0, h));
+  }
+  double t = __dadd_rn(-8.0, e);
+  t = __dadd_rn(14.0, __dmul_rn(e, t));
+  t = __dadd_rn(56.0, __dmul_rn(e, t));
+  t = __dadd_rn(-280.0, __dmul_rn(e, t));
+  t = __dadd_rn(448.0, __dmul_rn(e, t));
+  double prim = __dmul_rn(__dmul_rn(e, e), t);
+  prim = __dadd_rn(prim, -__dmul_rn(224.0, e));
+  prim = __dadd_rn(prim, -__ddiv_rn(12.0, e));
+  return __ddiv_rn(__dadd_rn(128.0, -prim), __dmul_rn(70.0, h));
+}
+
+// FP32 product-path kernel: same piecewise polynomial, with the
+// reciprocals precomputed by the caller (inv70h = 1/(70h), inv_h = 1/h).
+__device__ __forceinline__ float depth_f32(float r2, float h, float inv_h, float inv70h) {
+  if (r2 >= h * h) return rsqrtf(r2);
+  const float r = sqrtf(r2);
+  const float e = 2.0f * r * inv_h;
+  if (e <= 1.0f) {
+    const float e2 = e * e;
+    const float prim = e2 * (112.0f + e2 * (-56.0f + e * (14.0f + e * (8.0f - 3.0f * e))));
+    return (208.0f - prim) * inv70h;
+  }
+  const float prim = e * e * (448.0f + e * (-280.0f + e * (56.0f + e * (14.0f + e * (-8.0f + e))))) -
+                     224.0f * e - 12.0f / e;
+  return (128.0f - prim) * inv70h;
+}
+
+// Compensated (Fast2Sum/Kahan) FP32 accumulator.
+struct Kahan {
+  float s = 0.f, c = 0.f;
+  __device__ __forceinline__ void add(float x) {
+    const float y = x - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+};
+
+__device__ __forceinline__ double block_sum_d(double v, double *red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+  return t;
+}
+
+__device__ __forceinline__ int block_sum_i(int v, int *red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  int t = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+  return t;
+}
+
+struct DirectParams {
+  double fac;     // a / (6 pi)
+  double app;     // softening (standard grid units)
+  float b;        // real(b_bound, 4)
+  int nmin;       // np_halo_min
+};
+
+// One block per halo: bound_check_grid for gid 0 (:2611-2864).  FP64=true
+// is the plain FP64 path, bit-exact with the reference arithmetic; FP64=false
+// the FP32 product path with compensated sums.
+template <bool FP64>
+__global__ void __launch_bounds__(BLK) ub_direct_kernel(Members m, const int64_t *__restrict__ off,
+                                                        const int32_t *__restrict__ list,
+                                                        DirectParams P, HaloResult *__restrict__ res,
+                                                        uint8_t *__restrict__ keep_out,
+                                                        float *__restrict__ phi_out,
+                                                        int32_t *flags) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int c = list[blockIdx.x];
+  const int64_t b0 = off[c];
+  const int np = (int)(off[c + 1] - b0);
+  float *qx = reinterpret_cast<float *>(smem);
+  float *qy = qx + kDirectMax, *qz = qy + kDirectMax;
+  float *vx = qz + kDirectMax, *vy = vx + kDirectMax, *vz = vy + kDirectMax;
+  float *w = vz + kDirectMax, *phi = w + kDirectMax, *en = phi + kDirectMax;
+  int *jdel = reinterpret_cast<int *>(en + kDirectMax);
+  int *unb = jdel + kDirectMax;
+  double *phid = reinterpret_cast<double *>(unb + kDirectMax);
+  unsigned char *keep = reinterpret_cast<unsigned char *>(phid + kDirectMax);
+  __shared__ double red_d[BLK / 32];
+  __shared__ int red_i[BLK / 32];
+  __shared__ double s_qc[3], s_vc[3];
+  __shared__ int s_nu, s_err;
+
+  for (int i = threadIdx.x; i < np; i += BLK) {
+    const int64_t k = b0 + i;
+    qx[i] = m.q[0][k]; qy[i] = m.q[1][k]; qz[i] = m.q[2][k];
+    vx[i] = m.v[0][k]; vy[i] = m.v[1][k]; vz[i] = m.v[2][k];
+    w[i] = m.w[k];
+    keep[i] = 1;
+    phid[i] = 0.0;
+  }
+  if (threadIdx.x == 0) s_err = 0;
+  __syncthreads();
+  const float h32 = (float)P.app, inv_h = (float)(1.0 / P.app), inv70h = (float)(1.0 / (70.0 * P.app));
+  const float fac32 = (float)P.fac;
+  int np_bound = np, njd = 0, status = 5;
+
+  for (int pass = 1; pass <= kMaxPasses; ++pass) {
+    int ks = 0;
+    for (int i = threadIdx.x; i < np; i += BLK) ks += keep[i];
+    const int n_source = block_sum_i(ks, red_i);
+    // potential: full sum on the first pass, later passes add back the
+    // sources removed since the previous refresh
+    for (int i = threadIdx.x; i < np; i += BLK) {
+      if (pass == 1) {
+        if (FP64) {
+          double acc = 0.0;
+          for (int j = 0; j < np; ++j) {
+            if (j == i) continue;
+            const double dx = (double)__fsub_rn(qx[j], qx[i]);
+            const double dy = (double)__fsub_rn(qy[j], qy[i]);
+            const double dz = (double)__fsub_rn(qz[j], qz[i]);
+            const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
+                                                  __dmul_rn(dz, dz)));
+            const double dd = __dmul_rn(P.fac, depth_continuous<double>(r, P.app));
+            acc = __dadd_rn(acc, -__dmul_rn((double)w[j], dd));
+          }
+          phid[i] = acc;
+        } else {
+          Kahan acc;
+          const float xi = qx[i], yi = qy[i], zi = qz[i];
+          for (int j = 0; j < np; ++j) {
+            if (j == i) continue;
+            const float dx = qx[j] - xi, dy = qy[j] - yi, dz = qz[j] - zi;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            acc.add(-w[j] * depth_f32(r2, h32, inv_h, inv70h));
+          }
+          phid[i] = (double)(fac32 * acc.s);
+        }
+      } else if (keep[i]) {
+        if (FP64) {
+          double acc = phid[i];
+          for (int k = 0; k < njd; ++k) {
+            const int j = jdel[k];
+            const double dx = (double)__fsub_rn(qx[j], qx[i]);
+            const double dy = (double)__fsub_rn(qy[j], qy[i]);
+            const double dz = (double)__fsub_rn(qz[j], qz[i]);
+            const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
+                                                  __dmul_rn(dz, dz)));
+            acc = __dadd_rn(acc, __dmul_rn(__dmul_rn((double)w[j], P.fac),
+                                           depth_continuous<double>(r, P.app)));
+          }
+          phid[i] = acc;
+        } else {
+          Kahan acc;
+          const float xi = qx[i], yi = qy[i], zi = qz[i];
+          for (int k = 0; k < njd; ++k) {
+            const int j = jdel[k];
+            const float dx = qx[j] - xi, dy = qy[j] - yi, dz = qz[j] - zi;
+            acc.add(w[j] * depth_f32(dx * dx + dy * dy + dz * dz, h32, inv_h, inv70h));
+          }
+          phid[i] += (double)(fac32 * acc.s);
+        }
+      }
+    }
+    njd = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < np; i += BLK) {
+      if (!keep[i]) continue;
+      float v = FP64 ? __double2float_rn(phid[i]) : (float)phid[i];
+      if (np_bound == 1 || n_source == 1) v = 0.0f;
+      if (!isfinite(v)) s_err = kNonFinite;
+      phi[i] = v;
+    }
+    __syncthreads();
+    if (s_err) break;
+    int deleted = 0;
+    for (;;) {
+      // centre of mass and mean velocity of the kept set, FP64
+      if (FP64) {
+        if (threadIdx.x == 0) {
+          double ws = 0, q0 = 0, q1 = 0, q2 = 0, v0 = 0, v1 = 0, v2 = 0;
+          for (int i = 0; i < np; ++i) {
+            if (!keep[i]) continue;
+            const double wi = (double)w[i];
+            ws = __dadd_rn(ws, wi);
+            q0 = __dadd_rn(q0, __dmul_rn(wi, (double)qx[i]));
+            q1 = __dadd_rn(q1, __dmul_rn(wi, (double)qy[i]));
+            q2 = __dadd_rn(q2, __dmul_rn(wi, (double)qz[i]));
+            v0 = __dadd_rn(v0, __dmul_rn(wi, (double)vx[i]));
+            v1 = __dadd_rn(v1, __dmul_rn(wi, (double)vy[i]));
+            v2 = __dadd_rn(v2, __dmul_rn(wi, (double)vz[i]));
+          }
+          s_qc[0] = __ddiv_rn(q0, ws); s_qc[1] = __ddiv_rn(q1, ws); s_qc[2] = __ddiv_rn(q2, ws);
+          s_vc[0] = __ddiv_rn(v0, ws); s_vc[1] = __ddiv_rn(v1, ws); s_vc[2] = __ddiv_rn(v2, ws);
+        }
+      } else {
+        double a[7] = {0, 0, 0, 0, 0, 0, 0};
+        for (int i = threadIdx.x; i < np; i += BLK) {
+          if (!keep[i]) continue;
+          const double wi = (double)w[i];
+          a[0] += wi;
+          a[1] += wi * qx[i]; a[2] += wi * qy[i]; a[3] += wi * qz[i];
+          a[4] += wi * vx[i]; a[5] += wi * vy[i]; a[6] += wi * vz[i];
+        }
+        for (int k = 0; k < 7; ++k) a[k] = block_sum_d(a[k], red_d);
+        if (threadIdx.x == 0) {
+          for (int d = 0; d < 3; ++d) { s_qc[d] = a[1 + d] / a[0]; s_vc[d] = a[4 + d] / a[0]; }
+        }
+      }
+      if (threadIdx.x == 0) s_nu = 0;
+      __syncthreads();
+      const float qc0 = __double2float_rn(s_qc[0]), qc1 = __double2float_rn(s_qc[1]),
+                  qc2 = __double2float_rn(s_qc[2]);
+      const float vc0 = __double2float_rn(s_vc[0]), vc1 = __double2float_rn(s_vc[1]),
+                  vc2 = __double2float_rn(s_vc[2]);
+      // specific energies (bound_fortran.f90:2773-2786), FP32
+      for (int i = threadIdx.x; i < np; i += BLK) {
+        if (!keep[i]) continue;
+        const float d0 = __fadd_rn(__fsub_rn(vx[i], vc0), __fmul_rn(P.b, __fsub_rn(qx[i], qc0)));
+        const float d1 = __fadd_rn(__fsub_rn(vy[i], vc1), __fmul_rn(P.b, __fsub_rn(qy[i], qc1)));
+        const float d2 = __fadd_rn(__fsub_rn(vz[i], vc2), __fmul_rn(P.b, __fsub_rn(qz[i], qc2)));
+        float s = __fmul_rn(d0, d0);
+        s = __fadd_rn(s, __fmul_rn(d1, d1));
+        s = __fadd_rn(s, __fmul_rn(d2, d2));
+        const float e = __fadd_rn(__fdiv_rn(s, 2.0f), phi[i]);
+        if (!isfinite(e)) s_err = kInvalid;
+        en[i] = e;
+        if (e >= 0.0f) unb[atomicAdd(&s_nu, 1)] = i;
+      }
+      __syncthreads();
+      if (s_err) break;
+      const int nu = s_nu;
+      if (nu == 0) {
+        if (deleted == 0) { status = 0; break; }
+        break;
+      }
+      // delete the nb highest energies; ties go to the lower local index
+      // first (bound_fortran.f90:2808-2844)
+      int nb = (int)ceil(0.02 * (double)np_bound);
+      nb = max(1, nb);
+      nb = min(nu, nb);
+      for (int t = threadIdx.x; t < nu; t += BLK) {
+        const int i = unb[t];
+        const float ei = en[i];
+        int rank = 0;
+        for (int u = 0; u < nu; ++u) {
+          const int j = unb[u];
+          const float ej = en[j];
+          rank += (ej > ei) || (ej == ei && j < i);
+        }
+        if (rank < nb) {
+          keep[i] = 0;
+          jdel[njd + rank] = i;
+        }
+      }
+      __syncthreads();
+      njd += nb;
+      np_bound -= nb;
+      deleted += nb;
+      if (np_bound < P.nmin) { status = 1; break; }
+      if ((double)deleted >= 0.2 * (double)np_bound) break;
+    }
+    __syncthreads();
+    if (s_err || status != 5) break;
+    if (pass == kMaxPasses) break;
+  }
+  if (s_err) {
+    if (threadIdx.x == 0) atomicCAS(&flags[FLAG_ERR], 0, s_err);
+    return;
+  }
+  for (int i = threadIdx.x; i < np; i += BLK) {
+    keep_out[b0 + i] = keep[i];
+    if (phi_out) phi_out[b0 + i] = phi[i];
+  }
+  if (threadIdx.x == 0) {
+    res[c].status = status;
+    res[c].np_bound = np_bound;
+  }
+}
+
+// Valid halos (status 0 and np_bound >= np_halo_min) in candidate order.
+__global__ void ub_valid_kernel(const HaloResult *__restrict__ res, int ncand, int nmin,
+                                uint32_t *__restrict__ valid) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncand; c += gridDim.x * blockDim.x)
+    valid[c] = (res[c].status == 0 && res[c].np_bound >= nmin) ? 1u : 0u;
+}
+
+__global__ void ub_write_kernel(const uint32_t *__restrict__ mcand, const Members m,
+                                const uint8_t *__restrict__ keep, const uint32_t *__restrict__ valid,
+                                const uint32_t *__restrict__ vrank, int64_t M,
+                                int32_t *__restrict__ in_halo, int32_t *__restrict__ halo_id) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t c = mcand[k];
+    if (valid[c] && keep[k]) {
+      const int32_t i = m.pid[k];
+      in_halo[i] = 1;
+      halo_id[i] = (int32_t)vrank[c] + 1;
+    }
+  }
+}
+
+// Angular momentum of the kept members of valid halos about their centre
+// (fof_fortran.f90:321-350), accumulated per candidate in two passes.
+__global__ void ub_com_kernel(Coords xp, Coords vp, const double *mp,
+                              const uint32_t *__restrict__ mcand, const Members m,
+                              const uint8_t *__restrict__ keep, const uint32_t *__restrict__ valid,
+                              const int64_t *__restrict__ cand_anchor, int64_t M, double L,
+                              double half, double *acc) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t c = mcand[k];
+    if (!valid[c] || !keep[k]) continue;
+    const int64_t i = m.pid[k], a = cand_anchor[c];
+    const double wi = mp ? mp[i] : 1.0;
+    atomicAdd(&acc[7 * (int64_t)c], wi);
+    for (int d = 0; d < 3; ++d) {
+      atomicAdd(&acc[7 * (int64_t)c + 1 + d], wi * unwrap(xp.get(i, d), xp.get(a, d), half, L));
+      atomicAdd(&acc[7 * (int64_t)c + 4 + d], wi * vp.get(i, d));
+    }
+  }
+}
+
+__global__ void ub_angmom_kernel(Coords xp, Coords vp, const double *mp,
+                                 const uint32_t *__restrict__ mcand, const Members m,
+                                 const uint8_t *__restrict__ keep,
+                                 const uint32_t *__restrict__ valid,
+                                 const int64_t *__restrict__ cand_anchor, const double *acc,
+                                 int64_t M, double L, double half, double *am) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t c = mcand[k];
+    if (!valid[c] || !keep[k]) continue;
+    const double ws = acc[7 * (int64_t)c];
+    if (!(ws > 0.0)) continue;
+    const int64_t i = m.pid[k], a = cand_anchor[c];
+    const double wi = mp ? mp[i] : 1.0;
+    double dx[3], dv[3];
+    for (int d = 0; d < 3; ++d) {
+      dx[d] = unwrap(xp.get(i, d), xp.get(a, d), half, L) - acc[7 * (int64_t)c + 1 + d] / ws;
+      dv[d] = vp.get(i, d) - acc[7 * (int64_t)c + 4 + d] / ws;
+    }
+    atomicAdd(&am[3 * (int64_t)c + 0], wi * (dx[1] * dv[2] - dx[2] * dv[1]));
+    atomicAdd(&am[3 * (int64_t)c + 1], wi * (dx[2] * dv[0] - dx[0] * dv[2]));
+    atomicAdd(&am[3 * (int64_t)c + 2], wi * (dx[0] * dv[1] - dx[1] * dv[0]));
+  }
+}
+
+int bits_for(uint64_t v) {
+  int b = 0;
+  while (b < 64 && (v >> b) != 0) ++b;
+  return b;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ grid rules
+
+// bound_set_context / bound_grid_levels / bound_fgl_init / ladder
+// (bound_fortran.f90:291-330, :1854-1955): the grid classes 48/64/128/256
+// (capped at ng), their spacing levels 1/32, 1/16, ... while the coverage
+// (n/2-3)*spacing stays below s_15, plus spacing_max = s_15/m_max on the
+// largest enabled class.
+void GridRules::init(int64_t ng_in, double s15_in) {
+  static const int cand[4] = {48, 64, 128, 256};
+  ng = ng_in > 0 ? ng_in : 256;
+  const int ngi = (int)ng;
+  ngrid = 1 + (ngi >= 64) + (ngi >= 128) + (ngi >= 256);
+  for (int g = 0; g < 4; ++g) bn[g] = std::min(cand[g], ngi);
+  const int n_max = std::min(256, ngi);
+  const int m_max = n_max / 2 - 3;
+  s15 = s15_in;
+  spacing_max = s15 / (double)m_max;
+  for (int g = 1; g <= 4; ++g) {
+    std::vector<double> &sp = levels[g - 1];
+    sp.clear();
+    if (g > ngrid) continue;
+    const int m = bn[g - 1] / 2 - 3;
+    double s = 1.0 / 32.0;
+    while ((double)m * s < s15 && (int)sp.size() < 32) { sp.push_back(s); s *= 2.0; }
+    if (g == ngrid && (int)sp.size() < 32) sp.push_back(spacing_max);
+  }
+  // global ladder by coverage, selection sort as in bound_build_ladder
+  struct E { int g, l; double sp, cov; };
+  std::vector<E> t;
+  for (int g = 1; g <= ngrid; ++g)
+    for (int l = 0; l < (int)levels[g - 1].size(); ++l)
+      t.push_back(E{g, l, levels[g - 1][l], (double)(bn[g - 1] / 2 - 3) * levels[g - 1][l]});
+  for (size_t j = 0; j + 1 < t.size(); ++j) {
+    size_t k = j;
+    for (size_t i = j + 1; i < t.size(); ++i) if (t[i].cov < t[k].cov) k = i;
+    if (k != j) std::swap(t[j], t[k]);
+  }
+  ladder_g.clear(); ladder_l.clear(); ladder_cov.clear();
+  for (auto &e : t) { ladder_g.push_back(e.g); ladder_l.push_back(e.l); ladder_cov.push_back(e.cov); }
+}
+
+double GridRules::coverage(int g, int l) const {
+  return (double)(bn[g - 1] / 2 - 3) * levels[g - 1][l];
+}
+
+// bound_select_grid_and_level (:1963-2019).  Returns false when no enabled
+// grid class can cover the span.
+bool GridRules::select(int64_t np, double span, int &gid, int &lev, double &sp) const {
+  gid = 0; lev = -1; sp = 0.0;
+  if (np <= 1000) return true;
+  // candidate sequences per size band; spacing < 0 stands for spacing_max
+  static const int nb[3] = {11, 10, 8};
+  static const int cg[3][11] = {{1, 2, 2, 3, 3, 3, 4, 4, 4, 4, 4},
+                                {3, 3, 4, 4, 4, 4, 4, 4, 4, 4, 0},
+                                {4, 4, 4, 4, 4, 4, 4, 4, 0, 0, 0}};
+  static const double cs[3][11] = {
+      {0.125, 0.125, 0.25, 0.125, 0.25, 0.5, 0.0625, 0.125, 0.25, 0.5, -1.0},
+      {0.0625, 0.125, 0.0625, 0.125, 0.25, 0.5, 1.0, 2.0, 4.0, -1.0, 0.0},
+      {0.0625, 0.125, 0.25, 0.5, 1.0, 2.0, 4.0, -1.0, 0.0, 0.0, 0.0}};
+  const int band = np <= 5000 ? 0 : (np <= 20000 ? 1 : 2);
+  for (int s = 0; s < nb[band]; ++s) {
+    const int g = cg[band][s];
+    if (g < 1 || g > ngrid) continue;
+    double want = cs[band][s];
+    if (want == -1.0) want = spacing_max;
+    int l = -1;
+    for (int q = 0; q < (int)levels[g - 1].size(); ++q)
+      if (std::fabs(levels[g - 1][q] - want) <= 1e-12 * std::max(1.0, std::fabs(want))) { l = q; break; }
+    if (l < 0) continue;
+    if (coverage(g, l) < span) continue;
+    gid = g; lev = l; sp = levels[g - 1][l];
+    return true;
+  }
+  if (span <= s15) {
+    for (size_t i = 0; i < ladder_cov.size(); ++i)
+      if (ladder_cov[i] >= span) {
+        const int g = ladder_g[i], l = ladder_l[i];
+        if (g >= 1 && g <= ngrid) { gid = g; lev = l; sp = levels[g - 1][l]; return true; }
+        break;
+      }
+  }
+  return false;
+}
+
+// ------------------------------------------------------------ stage
+
 int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
-  (void)ctx; (void)a; (void)st;
-  set_error("bound_check is not available in this build");
-  return kInvalid;
+  cudaStream_t s = ctx.stream;
+  Arena &W = ctx.work;
+  const int nreg = a.nhalo;
+  std::vector<double> am_host(3 * (size_t)nreg, 0.0);
+  const int ncand = (int)st.ncand;
+  if (ncand == 0) {
+    std::memcpy(a.ang_mom, am_host.data(), sizeof(double) * am_host.size());
+    return kOk;
+  }
+  GridRules rules;
+  rules.init(a.ng, a.s15);
+  if (rules.ngrid != 4) {
+    set_error("bound_check_batch: fixed groups require ng >= 256");
+    return kInvalid;
+  }
+  if (!std::isfinite(a.a_val) || a.a_val <= 0.0 || !std::isfinite(a.b_val)) {
+    set_error("bound_check_batch: invalid physical context");
+    return kInvalid;
+  }
+  const int64_t n = a.total_np;
+  const double L = a.L_Box, half = 0.5 * a.L_Box;
+  Coords xp{a.xp, n, a.soa}, vp{a.vp, n, a.soa};
+
+  // 1. members grouped by candidate, ascending global index
+  uint32_t *cand_of = W.carve<uint32_t>(n);
+  uint32_t *ka = W.carve<uint32_t>(n), *va = W.carve<uint32_t>(n);
+  uint32_t *kb = W.carve<uint32_t>(n), *vb = W.carve<uint32_t>(n);
+  int64_t *off = W.carve<int64_t>(ncand + 1);
+  if (!cand_of || !ka || !va || !kb || !vb || !off) { set_error("workspace exhausted (members)"); return kAlloc; }
+  const unsigned grid_n = (unsigned)std::min<int64_t>(ceil_div(n, BLK), (int64_t)kNumSMs * 16);
+  ub_fill_kernel<<<grid_n, BLK, 0, s>>>(cand_of, n, (uint32_t)ncand);
+  PYFOF_CHECK_LAUNCH();
+  ub_mark_kernel<<<grid_n, BLK, 0, s>>>(st.pcand, st.pos, st.n_active, cand_of);
+  PYFOF_CHECK_LAUNCH();
+  uint32_t *mcand, *midx;
+  PYFOF_TRY(radix_sort_pairs(cand_of, nullptr, n, bits_for((uint64_t)ncand), ka, va, kb, vb, &mcand,
+                             &midx, W, s));
+  std::vector<int32_t> cnp(ncand);
+  PYFOF_CUDA(cudaMemcpyAsync(cnp.data(), st.cand_np, sizeof(int32_t) * ncand, cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaStreamSynchronize(s));
+  std::vector<int64_t> hoff(ncand + 1, 0);
+  for (int c = 0; c < ncand; ++c) hoff[c + 1] = hoff[c] + cnp[c];
+  const int64_t M = hoff[ncand];
+  PYFOF_CUDA(cudaMemcpyAsync(off, hoff.data(), sizeof(int64_t) * (ncand + 1), cudaMemcpyHostToDevice, s));
+  Members m;
+  for (int d = 0; d < 3; ++d) {
+    m.q[d] = W.carve<float>(M);
+    m.v[d] = W.carve<float>(M);
+    if (!m.q[d] || !m.v[d]) { set_error("workspace exhausted (xv)"); return kAlloc; }
+  }
+  m.w = W.carve<float>(M);
+  m.pid = W.carve<int32_t>(M);
+  float *lo = W.carve<float>(3 * (size_t)ncand), *span = W.carve<float>(ncand);
+  HaloResult *res = W.carve<HaloResult>(ncand);
+  uint8_t *keep = W.carve<uint8_t>(M);
+  if (!m.w || !m.pid || !lo || !span || !res || !keep) { set_error("workspace exhausted (xv)"); return kAlloc; }
+  const unsigned grid_m = (unsigned)std::min<int64_t>(ceil_div(M, BLK), (int64_t)kNumSMs * 16);
+  ub_pack_kernel<<<grid_m, BLK, 0, s>>>(xp, vp, a.mp, mcand, midx, st.cand_anchor, M, L, half, m);
+  PYFOF_CHECK_LAUNCH();
+  ub_span_kernel<<<ncand, BLK, 0, s>>>(m, off, lo, span);
+  PYFOF_CHECK_LAUNCH();
+
+  // 2. classification, in candidate order (first error wins)
+  std::vector<float> hlo(3 * (size_t)ncand), hspan(ncand);
+  PYFOF_CUDA(cudaMemcpyAsync(hlo.data(), lo, sizeof(float) * 3 * ncand, cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaMemcpyAsync(hspan.data(), span, sizeof(float) * ncand, cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaStreamSynchronize(s));
+  std::vector<HaloTask> tasks(ncand);
+  std::vector<int32_t> direct, pm;
+  for (int c = 0; c < ncand; ++c) {
+    HaloTask &t = tasks[c];
+    t.off = hoff[c];
+    t.np = cnp[c];
+    const float sp_c = hspan[c];
+    if (!std::isfinite(sp_c)) { set_error("bound_classify: non-finite span"); return kInvalid; }
+    if (t.np > 1000 && sp_c > (float)a.s15) {
+      set_error("candidate %d: span %g exceeds D_max = 15 Mpc (s_15 = %g)", c, (double)sp_c, a.s15);
+      return kSpan;
+    }
+    int g, l;
+    double sp;
+    if (!rules.select(t.np, (double)sp_c, g, l, sp)) {
+      set_error("candidate %d: no enabled grid class can cover span %g", c, (double)sp_c);
+      return kInvalid;
+    }
+    t.gid = g;
+    t.n = g > 0 ? rules.bn[g - 1] : 0;
+    if (g > 0) {
+      const float spf = (float)sp;
+      t.spacing = spf;
+      for (int d = 0; d < 3; ++d) t.origin[d] = hlo[3 * c + d] - spf;
+      if ((double)(rules.bn[g - 1] / 2 - 3) * (double)spf < (double)sp_c) {
+        set_error("candidate %d: single precision spacing does not cover span", c);
+        return kInvalid;
+      }
+      pm.push_back(c);
+    } else {
+      direct.push_back(c);
+    }
+  }
+  ctx.last_direct = (int64_t)direct.size();
+  ctx.last_pm = (int64_t)pm.size();
+
+  // 3. solvers
+  PYFOF_CUDA(cudaMemsetAsync(ctx.d_flags, 0, sizeof(int32_t), s));
+  if (!direct.empty()) {
+    int32_t *dl = W.carve<int32_t>(direct.size());
+    if (!dl) { set_error("workspace exhausted (direct list)"); return kAlloc; }
+    PYFOF_CUDA(cudaMemcpyAsync(dl, direct.data(), sizeof(int32_t) * direct.size(),
+                               cudaMemcpyHostToDevice, s));
+    DirectParams P;
+    P.fac = a.a_val / (6.0 * kPi);
+    P.app = a.softening;
+    P.b = (float)a.b_val;
+    P.nmin = a.np_halo_min;
+    const size_t smem = kDirectSmem;
+    if (a.bound_fp64) {
+      PYFOF_CUDA(cudaFuncSetAttribute(ub_direct_kernel<true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      ub_direct_kernel<true><<<(unsigned)direct.size(), BLK, smem, s>>>(m, off, dl, P, res, keep,
+                                                                         st.phi_out, ctx.d_flags);
+    } else {
+      PYFOF_CUDA(cudaFuncSetAttribute(ub_direct_kernel<false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      ub_direct_kernel<false><<<(unsigned)direct.size(), BLK, smem, s>>>(m, off, dl, P, res, keep,
+                                                                          st.phi_out, ctx.d_flags);
+    }
+    PYFOF_CHECK_LAUNCH();
+  }
+  if (!pm.empty()) PYFOF_TRY(unbind_pm(ctx, a, rules, m, tasks, pm, res, keep, st.phi_out));
+  PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaStreamSynchronize(s));
+  if (ctx.h_flags[FLAG_ERR]) {
+    set_error("unbinding failed (error %d)", ctx.h_flags[FLAG_ERR]);
+    return ctx.h_flags[FLAG_ERR];
+  }
+
+  // 4. outputs
+  uint32_t *valid = W.carve<uint32_t>(ncand + 1), *vrank = W.carve<uint32_t>(ncand + 1);
+  double *acc = W.carve<double>(7 * (size_t)ncand), *am = W.carve<double>(3 * (size_t)ncand);
+  if (!valid || !vrank || !acc || !am) { set_error("workspace exhausted (outputs)"); return kAlloc; }
+  const unsigned grid_c = (unsigned)std::min<int64_t>(ceil_div(ncand, BLK), (int64_t)kNumSMs * 8);
+  ub_valid_kernel<<<grid_c, BLK, 0, s>>>(res, ncand, a.np_halo_min, valid);
+  PYFOF_CHECK_LAUNCH();
+  PYFOF_TRY(exclusive_scan_u32(valid, vrank, ncand, nullptr, W, s));
+  ub_write_kernel<<<grid_m, BLK, 0, s>>>(mcand, m, keep, valid, vrank, M, a.in_halo, a.halo_id);
+  PYFOF_CHECK_LAUNCH();
+  PYFOF_CUDA(cudaMemsetAsync(acc, 0, sizeof(double) * 7 * ncand, s));
+  PYFOF_CUDA(cudaMemsetAsync(am, 0, sizeof(double) * 3 * ncand, s));
+  ub_com_kernel<<<grid_m, BLK, 0, s>>>(xp, vp, a.mp, mcand, m, keep, valid, st.cand_anchor, M, L,
+                                       half, acc);
+  PYFOF_CHECK_LAUNCH();
+  ub_angmom_kernel<<<grid_m, BLK, 0, s>>>(xp, vp, a.mp, mcand, m, keep, valid, st.cand_anchor,
+                                          acc, M, L, half, am);
+  PYFOF_CHECK_LAUNCH();
+  std::vector<double> amc(3 * (size_t)ncand);
+  std::vector<int32_t> creg(ncand);
+  std::vector<HaloResult> hres(ncand);
+  PYFOF_CUDA(cudaMemcpyAsync(amc.data(), am, sizeof(double) * 3 * ncand, cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaMemcpyAsync(creg.data(), st.cand_region, sizeof(int32_t) * ncand,
+                             cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaMemcpyAsync(hres.data(), res, sizeof(HaloResult) * ncand, cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaStreamSynchronize(s));
+  int64_t nvalid = 0, nmax = 0;
+  for (int c = 0; c < ncand; ++c) {
+    for (int d = 0; d < 3; ++d) am_host[3 * (size_t)creg[c] + d] += amc[3 * c + d];
+    nvalid += hres[c].status == 0 && hres[c].np_bound >= a.np_halo_min;
+    nmax += hres[c].status == 5;
+  }
+  ctx.last_valid = nvalid;
+  if (a.verbose >= 1)
+    fprintf(stderr, "[BOUND_STATUS] candidates=%d direct=%zu pm=%zu valid=%lld max_iter=%lld\n",
+            ncand, direct.size(), pm.size(), (long long)nvalid, (long long)nmax);
+  std::memcpy(a.ang_mom, am_host.data(), sizeof(double) * am_host.size());
+  return kOk;
 }
 
 }  // namespace pyfof

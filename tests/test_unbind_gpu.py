@@ -1,0 +1,104 @@
+"""Unbinding parity: the B200 solvers against the CPU oracle.
+
+* plain FP64 path (option unbind_fp64=1): the direct-summation removal loop
+  reproduces the reference arithmetic, so in_halo and halo_id are bit-exact;
+* FP32 product path: potentials carry FP32 rounding (compensated sums), so a
+  particle whose specific energy lies within a relative 1e-5 of zero may be
+  classified differently; everything else must agree.
+"""
+import numpy as np
+import pytest
+
+import py_fof_b200 as P
+from py_fof_b200 import _native
+from tests.helpers import angmom_close, oracle_core
+
+pytestmark = pytest.mark.gpu
+
+G = 1.0 / (6.0 * np.pi)
+
+
+def clumps(seed, n_regions=60, nmin=20, nmax=1000, L=512.0, kick=0.1, masses=False):
+    """Isolated Plummer clumps, one region each, virial velocities plus a
+    kicked fraction, so every candidate takes the direct-summation path."""
+    rng = np.random.default_rng(seed)
+    xs, vs, ms = [], [], []
+    for k in range(n_regions):
+        n = int(rng.integers(nmin, nmax + 1))
+        a = rng.uniform(0.3, 0.8)
+        u = np.clip(rng.random(n), 1e-9, 1 - 1e-9)
+        r = np.minimum(a / np.sqrt(u ** (-2.0 / 3.0) - 1.0), 4 * a)
+        d = rng.standard_normal((3, n))
+        d /= np.linalg.norm(d, axis=0)
+        c = rng.uniform(20, L - 20, (3, 1))
+        xs.append(c + r * d)
+        sig = np.sqrt(G * n / (6.0 * np.sqrt(r * r + a * a)))
+        v = rng.standard_normal((3, n)) * sig
+        nk = int(kick * n)
+        idx = rng.choice(n, nk, replace=False)
+        v[:, idx] *= rng.uniform(2.0, 6.0, nk)
+        vs.append(v + rng.standard_normal((3, 1)))
+        ms.append(rng.lognormal(-0.045, 0.3, n) if masses else None)
+    return xs, vs, (ms if masses else None)
+
+
+@pytest.fixture
+def fp64_path():
+    _native.set_option("unbind_fp64", 1)
+    yield
+    _native.set_option("unbind_fp64", 0)
+
+
+@pytest.mark.parametrize("seed,masses,hubble", [(1, False, False), (2, True, False), (3, True, True)])
+def test_direct_fp64_bit_exact(fp64_path, seed, masses, hubble):
+    xs, vs, ms = clumps(seed, masses=masses)
+    kw = dict(vp_list=vs, L_Box=512.0, linking_length=0.3, np_halo_min=10, bound_check=True,
+              return_ang_mom=True)
+    if ms is not None:
+        kw["mp_list"] = ms
+    if hubble:
+        kw["include_hubble_flow"] = True
+        kw["z"] = 0.5
+    g = P._fof_core(xs, **kw)
+    o = oracle_core(xs, **kw)
+    assert _native.get_stat("direct_halos") > 0
+    assert o[1].max() > 0
+    assert np.array_equal(g[0], o[0])
+    assert np.array_equal(g[1], o[1])
+    assert angmom_close(g[2], o[2], np.abs(o[2]).max() + 1.0)
+
+
+def test_direct_fp32_product_path():
+    xs, vs, ms = clumps(4, n_regions=80, masses=True)
+    kw = dict(vp_list=vs, mp_list=ms, L_Box=512.0, linking_length=0.3, np_halo_min=10,
+              bound_check=True)
+    g = P._fof_core(xs, **kw)
+    o = oracle_core(xs, **kw)
+    n_in = max(1, int(o[0].sum()))
+    mism = int((g[0] != o[0]).sum())
+    # only marginally bound particles may flip
+    assert mism <= max(2, n_in // 2000), (mism, n_in)
+    assert abs(int(g[1].max()) - int(o[1].max())) <= 1
+
+
+def test_direct_many_small_halos_in_box(fp64_path):
+    """Candidates found by FoF in one periodic box, then unbound."""
+    from py_fof_b200 import workloads as W
+    d = W.plummer_box(32 ** 3, 32.0, 8, seed=5, with_velocities=True, lognormal_mass=0.3,
+                      mmax=800)
+    kw = dict(vp_list=d["vp"], mp_list=d["mp"], L_Box=32.0, linking_length=0.2, np_halo_min=10,
+              bound_check=True, return_ang_mom=True)
+    g = P._fof_core(d["xp"], **kw)
+    o = oracle_core(d["xp"], **kw)
+    assert np.array_equal(g[1], o[1])
+    assert angmom_close(g[2], o[2], np.abs(o[2]).max() + 1.0)
+
+
+def test_too_few_and_all_unbound(fp64_path):
+    """Halos that lose too many members end with status TOO_FEW and no output."""
+    xs, vs, _ = clumps(6, n_regions=20, kick=0.0)
+    vs = [v * 50.0 for v in vs]
+    kw = dict(vp_list=vs, L_Box=512.0, linking_length=0.3, np_halo_min=10, bound_check=True)
+    g = P._fof_core(xs, **kw)
+    o = oracle_core(xs, **kw)
+    assert np.array_equal(g[1], o[1])
