@@ -68,6 +68,20 @@ int32_t pyfof_get_stat(const char *key, int64_t *value);
 /* Device time of the linking kernel of the last call, when timing is on. */
 int32_t pyfof_last_link_ms(float *ms);
 
+/* First-pass gravitational potential of one candidate, computed by the
+ * solver the reference rules select for it (bound_select_grid_and_level,
+ * bound_fortran.f90:1963): FP64 direct summation for np <= 1000
+ * (:2613-2647), particle-mesh C1 + C2 otherwise (:2657-2735).  Diagnostic
+ * counterpart of the first pass of bound_check_grid; no removal happens.
+ *   q    (3,np) float32 C order: member positions relative to member 0, in
+ *        stable-id order
+ *   w    (np) float32 masses
+ *   fp64 1 = plain FP64 path, 0 = FP32 product path
+ *   phi  (np) output potential; *method = 0 direct, 1..4 PM grid class. */
+int32_t pyfof_halo_potential(const float *q, const float *w, int32_t np, double softening,
+                             double a_val, double s_15_val, int64_t ng_val, int32_t fp64,
+                             float *phi, int32_t *method);
+
 /* Replaces fof_fortran.fof_fortran (fof_fortran.f90:10-58).
  *   xp, vp    (3,total_np) float64 in `layout`; vp may be NULL (all zero,
  *             the value _fof_core passes when vp_list is None,

@@ -72,29 +72,30 @@ void offt_1d(double complex *x, double complex *work, int n, int sign)
         const cplx *tw = p->tw[s];
         for (int j = 0; j < l; ++j) {
             cplx w[4];
-            for (int q = 0; q < r; ++q) w[q] = sign < 0 ? tw[j * r + q] : conj(tw[j * r + q]);
+            for (int u = 0; u < r; ++u) w[u] = sign < 0 ? tw[j * r + u] : conj(tw[j * r + u]);
             for (int k = 0; k < m; ++k) {
-                cplx v[4];
-                for (int q = 0; q < r; ++q) v[q] = a[(q * l + j) * m + k] * w[q];
-                cplx *o = b + (size_t)(j * r) * m + k;
+                cplx v[4], o[4];
+                for (int q = 0; q < r; ++q) v[q] = a[(q * l + j) * m + k];
                 if (r == 2) {
                     o[0] = v[0] + v[1];
-                    o[m] = v[0] - v[1];
+                    o[1] = v[0] - v[1];
                 } else if (r == 4) {
                     cplx t0 = v[0] + v[2], t1 = v[0] - v[2], t2 = v[1] + v[3];
                     cplx t3 = (v[1] - v[3]) * (sign < 0 ? -I : I);
                     o[0] = t0 + t2;
-                    o[m] = t1 + t3;
-                    o[2 * m] = t0 - t2;
-                    o[3 * m] = t1 - t3;
+                    o[1] = t1 + t3;
+                    o[2] = t0 - t2;
+                    o[3] = t1 - t3;
                 } else { /* r == 3 */
                     cplx t1 = v[1] + v[2];
                     cplx t2 = v[0] - 0.5 * t1;
                     cplx t3 = (sign < 0 ? -I : I) * s3 * (v[1] - v[2]);
                     o[0] = v[0] + t1;
-                    o[m] = t2 + t3;
-                    o[2 * m] = t2 - t3;
+                    o[1] = t2 + t3;
+                    o[2] = t2 - t3;
                 }
+                /* Stockham decimation in frequency: twiddle after the butterfly */
+                for (int u = 0; u < r; ++u) b[(j * r + u) * m + k] = o[u] * w[u];
             }
         }
         m *= r;

@@ -32,8 +32,8 @@ _RUN_ARGS = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, 
 
 # every symbol include/pyfof_b200.h declares
 EXPORTED = ("pyfof_version", "pyfof_init", "pyfof_shutdown", "pyfof_last_error",
-            "pyfof_set_option", "pyfof_set_stream", "pyfof_get_stat", "pyfof_last_link_ms", "pyfof_run",
-            "pyfof_run_device")
+            "pyfof_set_option", "pyfof_set_stream", "pyfof_get_stat", "pyfof_last_link_ms",
+            "pyfof_halo_potential", "pyfof_run", "pyfof_run_device")
 
 
 class NativeLibraryError(RuntimeError):
@@ -64,6 +64,11 @@ def load():
         L.pyfof_get_stat.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
         L.pyfof_last_link_ms.restype = ctypes.c_int32
         L.pyfof_last_link_ms.argtypes = [ctypes.POINTER(ctypes.c_float)]
+        L.pyfof_halo_potential.restype = ctypes.c_int32
+        L.pyfof_halo_potential.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p,
+                                           ctypes.POINTER(ctypes.c_int32)]
         L.pyfof_run.restype = ctypes.c_int32
         L.pyfof_run.argtypes = _RUN_ARGS
         L.pyfof_run_device.restype = ctypes.c_int32
@@ -142,6 +147,22 @@ def run(xp, vp, mp, np_halo, nhalo, L_Box, link, np_halo_min, bound_check, verbo
                        float(ng_global_val), _ptr(in_halo), _ptr(halo_id),
                        ang_mom.ctypes.data_as(_dp))
     return in_halo, halo_id, ang_mom, int(ierr)
+
+
+def halo_potential(q, w, softening=0.1, a_val=1.0, s15=17.152, ng=256, fp64=False):
+    """First-pass potential of one candidate (q: (3,np) positions relative to
+    member 0, stable-id order).  Returns (phi float32, method gid)."""
+    q = np.ascontiguousarray(q, dtype=np.float32)
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    n = w.shape[0]
+    phi = np.zeros(n, np.float32)
+    meth = ctypes.c_int32(-1)
+    ierr = load().pyfof_halo_potential(q.ctypes.data, w.ctypes.data, n, float(softening),
+                                       float(a_val), float(s15), int(ng), int(bool(fp64)),
+                                       phi.ctypes.data, ctypes.byref(meth))
+    if ierr:
+        raise RuntimeError(f"ierr={ierr}: {last_error()}")
+    return phi, int(meth.value)
 
 
 def run_device(xp_ptr, vp_ptr, mp_ptr, layout, np_halo, nhalo, total_np, L_Box, link,

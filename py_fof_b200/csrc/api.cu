@@ -6,6 +6,7 @@
 #include "context.cuh"
 #include "fof.cuh"
 #include "fof_internal.cuh"
+#include "unbind_internal.cuh"
 #include "../../include/pyfof_b200.h"
 
 namespace pyfof {
@@ -198,6 +199,24 @@ int32_t pyfof_last_link_ms(float *ms) {
   if (get_context(g_default_device, &c) != kOk || !ms) return kInvalid;
   *ms = c->stage_ms[0];
   return kOk;
+}
+
+int32_t pyfof_halo_potential(const float *q, const float *w, int32_t np, double softening,
+                             double a_val, double s_15_val, int64_t ng_val, int32_t fp64,
+                             float *phi, int32_t *method) {
+  if (!q || !w || !phi || !method || np <= 0) {
+    set_error("invalid arguments");
+    return kInvalid;
+  }
+  Context *cp;
+  PYFOF_TRY(get_context(g_default_device, &cp));
+  std::lock_guard<std::mutex> lk(cp->mu);
+  PYFOF_CUDA(cudaSetDevice(cp->device));
+  int32_t r = unbind_potential(*cp, q, w, np, softening, a_val, s_15_val, ng_val, fp64, phi, method);
+  cudaStreamSynchronize(cp->stream);
+  cp->work.release();
+  cudaStreamSynchronize(cp->stream);
+  return r;
 }
 
 int32_t pyfof_run(const double *xp, const double *vp, const double *mp, int32_t layout,

@@ -196,6 +196,7 @@ struct DirectParams {
   double app;     // softening (standard grid units)
   float b;        // real(b_bound, 4)
   int nmin;       // np_halo_min
+  int phi_only;   // stop after the first potential
 };
 
 // One block per halo: bound_check_grid for gid 0 (:2611-2864).  FP64=true
@@ -308,6 +309,7 @@ __global__ void __launch_bounds__(BLK) ub_direct_kernel(Members m, const int64_t
     }
     __syncthreads();
     if (s_err) break;
+    if (P.phi_only) { status = 0; break; }
     int deleted = 0;
     for (;;) {
       // centre of mass and mean velocity of the kept set, FP64
@@ -691,6 +693,7 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
     P.app = a.softening;
     P.b = (float)a.b_val;
     P.nmin = a.np_halo_min;
+    P.phi_only = 0;
     const size_t smem = kDirectSmem;
     if (a.bound_fp64) {
       PYFOF_CUDA(cudaFuncSetAttribute(ub_direct_kernel<true>,
@@ -705,7 +708,7 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
     }
     PYFOF_CHECK_LAUNCH();
   }
-  if (!pm.empty()) PYFOF_TRY(unbind_pm(ctx, a, rules, m, tasks, pm, res, keep, st.phi_out));
+  if (!pm.empty()) PYFOF_TRY(unbind_pm(ctx, a, rules, m, tasks, pm, res, keep, st.phi_out, 0));
   PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   PYFOF_CUDA(cudaStreamSynchronize(s));
   if (ctx.h_flags[FLAG_ERR]) {
@@ -750,6 +753,101 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
     fprintf(stderr, "[BOUND_STATUS] candidates=%d direct=%zu pm=%zu valid=%lld max_iter=%lld\n",
             ncand, direct.size(), pm.size(), (long long)nvalid, (long long)nmax);
   std::memcpy(a.ang_mom, am_host.data(), sizeof(double) * am_host.size());
+  return kOk;
+}
+
+int32_t unbind_potential(Context &ctx, const float *q_soa, const float *w, int32_t np,
+                         double softening, double a_val, double s15, int64_t ng, int fp64,
+                         float *phi, int32_t *method) {
+  cudaStream_t s = ctx.stream;
+  Arena &W = ctx.work;
+  GridRules rules;
+  rules.init(ng, s15);
+  if (rules.ngrid != 4 || np <= 0) {
+    set_error("unbind_potential: invalid grid or member count");
+    return kInvalid;
+  }
+  Members m;
+  for (int d = 0; d < 3; ++d) {
+    m.q[d] = W.carve<float>(np);
+    m.v[d] = W.carve<float>(np);
+    if (!m.q[d] || !m.v[d]) { set_error("workspace exhausted"); return kAlloc; }
+    PYFOF_CUDA(cudaMemcpyAsync(m.q[d], q_soa + (size_t)d * np, sizeof(float) * np, cudaMemcpyHostToDevice, s));
+    PYFOF_CUDA(cudaMemsetAsync(m.v[d], 0, sizeof(float) * np, s));
+  }
+  m.w = W.carve<float>(np);
+  m.pid = W.carve<int32_t>(np);
+  int64_t *off = W.carve<int64_t>(2);
+  float *lo = W.carve<float>(3), *span = W.carve<float>(1), *phid = W.carve<float>(np);
+  HaloResult *res = W.carve<HaloResult>(1);
+  uint8_t *keep = W.carve<uint8_t>(np);
+  int32_t *dl = W.carve<int32_t>(1);
+  if (!m.w || !m.pid || !off || !lo || !span || !phid || !res || !keep || !dl) {
+    set_error("workspace exhausted");
+    return kAlloc;
+  }
+  PYFOF_CUDA(cudaMemcpyAsync(m.w, w, sizeof(float) * np, cudaMemcpyHostToDevice, s));
+  const int64_t hoff[2] = {0, np};
+  PYFOF_CUDA(cudaMemcpyAsync(off, hoff, sizeof(hoff), cudaMemcpyHostToDevice, s));
+  ub_span_kernel<<<1, BLK, 0, s>>>(m, off, lo, span);
+  PYFOF_CHECK_LAUNCH();
+  float hlo[3], hspan;
+  PYFOF_CUDA(cudaMemcpyAsync(hlo, lo, sizeof(hlo), cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaMemcpyAsync(&hspan, span, sizeof(float), cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaStreamSynchronize(s));
+  if (!std::isfinite(hspan)) { set_error("non-finite span"); return kInvalid; }
+  if (np > 1000 && hspan > (float)s15) { set_error("span exceeds s_15"); return kSpan; }
+  int g, l;
+  double sp;
+  if (!rules.select(np, (double)hspan, g, l, sp)) { set_error("no grid covers the span"); return kInvalid; }
+  *method = g;
+  std::vector<HaloTask> tasks(1);
+  tasks[0].off = 0;
+  tasks[0].np = np;
+  tasks[0].gid = g;
+  tasks[0].n = g > 0 ? rules.bn[g - 1] : 0;
+  FofArgs a;
+  a.softening = softening;
+  a.a_val = a_val;
+  a.b_val = 0.0;
+  a.s15 = s15;
+  a.ng = ng;
+  a.np_halo_min = 1;
+  a.bound_fp64 = fp64;
+  PYFOF_CUDA(cudaMemsetAsync(ctx.d_flags, 0, sizeof(int32_t), s));
+  if (g == 0) {
+    const int32_t zero = 0;
+    PYFOF_CUDA(cudaMemcpyAsync(dl, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    DirectParams P;
+    P.fac = a_val / (6.0 * kPi);
+    P.app = softening;
+    P.b = 0.0f;
+    P.nmin = 1;
+    P.phi_only = 1;
+    if (fp64) {
+      PYFOF_CUDA(cudaFuncSetAttribute(ub_direct_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kDirectSmem));
+      ub_direct_kernel<true><<<1, BLK, kDirectSmem, s>>>(m, off, dl, P, res, keep, phid, ctx.d_flags);
+    } else {
+      PYFOF_CUDA(cudaFuncSetAttribute(ub_direct_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kDirectSmem));
+      ub_direct_kernel<false><<<1, BLK, kDirectSmem, s>>>(m, off, dl, P, res, keep, phid, ctx.d_flags);
+    }
+    PYFOF_CHECK_LAUNCH();
+  } else {
+    const float spf = (float)sp;
+    tasks[0].spacing = spf;
+    for (int d = 0; d < 3; ++d) tasks[0].origin[d] = hlo[d] - spf;
+    std::vector<int32_t> list(1, 0);
+    PYFOF_TRY(unbind_pm(ctx, a, rules, m, tasks, list, res, keep, phid, 1));
+  }
+  PYFOF_CUDA(cudaMemcpyAsync(phi, phid, sizeof(float) * np, cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaStreamSynchronize(s));
+  if (ctx.h_flags[FLAG_ERR]) {
+    set_error("potential failed (error %d)", ctx.h_flags[FLAG_ERR]);
+    return ctx.h_flags[FLAG_ERR];
+  }
   return kOk;
 }
 

@@ -52,6 +52,12 @@ struct GridRules {
 // Particle-mesh halos (gid >= 1): unbind_pm.cu.
 int32_t unbind_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Members &m,
                   const std::vector<HaloTask> &tasks, const std::vector<int32_t> &list,
-                  HaloResult *res, uint8_t *keep, float *phi_out);
+                  HaloResult *res, uint8_t *keep, float *phi_out, int phi_only);
+
+// First-pass potential of one halo (members in stable-id order, positions
+// relative to the first member), by the solver the reference rules select.
+int32_t unbind_potential(Context &ctx, const float *q_soa, const float *w, int32_t np,
+                         double softening, double a_val, double s15, int64_t ng, int fp64,
+                         float *phi, int32_t *method);
 
 }  // namespace pyfof

@@ -1,16 +1,904 @@
-// Particle-mesh unbinding (bound_fortran.f90:2206-2735, :3125-3552).
+// Particle-mesh unbinding of candidates with more than 1000 members
+// (bound_check_grid for gid >= 1, bound_fortran.f90:2436-2864).
+//
+// Per halo: TSC weights and self-potential of every member (:2558-2602),
+// then up to 20 passes of
+//   C1: TSC deposit of the kept members on the zero-padded n^3 grid, FFT,
+//       multiplication by the optimal Green's function, inverse FFT, TSC
+//       gather, self term and the far-field constant (:2657-2703);
+//   C2: short-range residual between the spline-softened kernel and the C1
+//       split kernel for pairs closer than 3.5 grid cells (:3403-3552),
+//       evaluated over 3.5-cell neighbour lists, recomputed over the kept set
+//       each pass (the reference updates it incrementally; the sum is the
+//       same set of pair terms);
+//   removal: the inner loop of the direct path, with the top-2% selection
+//       done by an in-block radix select (only the deleted set matters here).
+// Halos of one grid class are batched: one launch deposits, transforms and
+// gathers all of them.  R = float is the product path, R = double the plain
+// FP64 path.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
 #include "context.cuh"
+#include "fft.cuh"
+#include "primitives.cuh"
 #include "unbind_internal.cuh"
 
 namespace pyfof {
 
+namespace {
+
+constexpr int BLK = 256;
+constexpr int IBLK = 1024;  // inner-loop block
+constexpr double kPi = 3.141592653589793238462643383279502884197;
+
+// ---------------------------------------------------------------- Green
+
+// bound_fft_wave_number (bound_fortran.f90:3563-3569)
+__device__ __forceinline__ double wave_number(int i0, int n) {
+  const int mode = ((i0 + n / 2) % n) - n / 2;
+  return 2.0 * kPi * (double)mode / (double)n;
+}
+
+// bound_assignment_window_sq with assignment order 2 (:3571-3583)
+__device__ __forceinline__ double window_sq(double k0, double k1, double k2) {
+  double s = 1.0;
+  double x = 0.5 * k0;
+  if (x != 0.0) s = s * sin(x) / x;
+  x = 0.5 * k1;
+  if (x != 0.0) s = s * sin(x) / x;
+  x = 0.5 * k2;
+  if (x != 0.0) s = s * sin(x) / x;
+  const double s2 = s * s, s3 = s2 * s;
+  return s3 * s3;
+}
+
+// Alias-summed optimal Green's function (bound_calc_green_and_self,
+// :2300-2371), one thread per half-spectrum point.
+template <typename R>
+__global__ void green_kernel(R *__restrict__ g, int n, double soft, double range, int truncated,
+                             int32_t *flags) {
+  const int nh = n / 2 + 1;
+  const int64_t total = (int64_t)nh * n * n;
+  const double radius = 0.5 * (double)n;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nh);
+    const int j = (int)((t / nh) % n);
+    const int k = (int)(t / ((int64_t)nh * n));
+    const double kv0 = wave_number(i, n), kv1 = wave_number(j, n), kv2 = wave_number(k, n);
+    double asum = 0.0, bsum = 0.0;
+    for (int ka = -2; ka <= 2; ++ka)
+      for (int ja = -2; ja <= 2; ++ja)
+        for (int ia = -2; ia <= 2; ++ia) {
+          const double k0 = kv0 + 2.0 * kPi * (double)ia;
+          const double k1 = kv1 + 2.0 * kPi * (double)ja;
+          const double k2 = kv2 + 2.0 * kPi * (double)ka;
+          const double kmag = sqrt(k0 * k0 + k1 * k1 + k2 * k2);
+          const double uk2 = window_sq(k0, k1, k2);
+          asum += uk2;
+          double target;
+          if (kmag == 0.0) {
+            if (range == 0.0) target = -4.0 * kPi * radius * radius / 6.0;
+            else if (truncated) target = 0.0;
+            else target = -2.0 * kPi * (range * range - soft * soft) / 15.0;
+          } else {
+            double y = soft * kmag / 2.0;
+            double y2 = y * y;
+            const double ss = 12.0 * (1.0 / (y2 * y2)) * (2.0 - 2.0 * cos(y) - y * sin(y));
+            double sr = 0.0;
+            if (range != 0.0) {
+              y = range * kmag / 2.0;
+              y2 = y * y;
+              sr = 12.0 * (1.0 / (y2 * y2)) * (2.0 - 2.0 * cos(y) - y * sin(y));
+            }
+            double cut = 1.0;
+            if (truncated) {
+              const double kr = kmag * radius;
+              cut = 1.0 - sin(kr) / kr;
+            }
+            target = -4.0 * kPi * (ss * ss - sr * sr) * cut / (kmag * kmag);
+          }
+          bsum += uk2 * target;
+        }
+    if (!(asum > 2.2250738585072014e-308)) {
+      atomicCAS(&flags[FLAG_ERR], 0, kInvalid);
+      continue;
+    }
+    const double v = bsum / (asum * asum);
+    g[t] = (R)v;  // FP32 path: the reference's complex(4) table
+  }
+}
+
+template <typename R>
+__global__ void self_extract_kernel(const R *__restrict__ grid, int n, R *__restrict__ self) {
+  const int t = threadIdx.x;
+  if (t >= 125) return;
+  const int ox = t % 5 - 2, oy = (t / 5) % 5 - 2, oz = t / 25 - 2;
+  const int x = (ox + n) % n, y = (oy + n) % n, z = (oz + n) % n;
+  const R n3 = (R)((double)n * n * n);
+  self[t] = grid[((int64_t)z * n + y) * n + x] / n3;
+}
+
+}  // namespace
+
+struct GreenTable {
+  int n = 0;
+  void *g = nullptr;     // half-spectrum table (R)
+  void *self = nullptr;  // 125 self-kernel values (R), device
+  bool fp64 = false;
+  ~GreenTable() {
+    if (g) cudaFree(g);
+    if (self) cudaFree(self);
+  }
+};
+
+namespace {
+
+// Green table of grid n for (soft, range, truncated), cached per context.
+template <typename R>
+int32_t get_green(Context &ctx, int n, double soft, double range, int truncated,
+                  std::shared_ptr<GreenTable> *out) {
+  const int kind = range == 0.0 ? 0 : (range < 10.0 ? 1 : 2);
+  const int64_t key = ((int64_t)n << 8) | (kind << 1) | (sizeof(R) == 8 ? 1 : 0);
+  auto it = ctx.green.find(key);
+  if (it != ctx.green.end()) { *out = it->second; return kOk; }
+  auto t = std::make_shared<GreenTable>();
+  t->n = n;
+  t->fp64 = sizeof(R) == 8;
+  const int nh = n / 2 + 1;
+  const int64_t cnt = (int64_t)nh * n * n;
+  cudaStream_t s = ctx.stream;
+  PYFOF_CUDA(cudaMalloc(&t->g, sizeof(R) * cnt));
+  PYFOF_CUDA(cudaMalloc(&t->self, sizeof(R) * 125));
+  PYFOF_CUDA(cudaMemsetAsync(ctx.d_flags, 0, sizeof(int32_t), s));
+  green_kernel<R><<<(unsigned)std::min<int64_t>(ceil_div(cnt, 128), 148 * 64), 128, 0, s>>>(
+      (R *)t->g, n, soft, range, truncated, ctx.d_flags);
+  PYFOF_CHECK_LAUNCH();
+  R *grid = nullptr;
+  cplx_t<R> *spec = nullptr;
+  PYFOF_CUDA(cudaMallocAsync(&grid, sizeof(R) * (size_t)n * n * n, s));
+  PYFOF_CUDA(cudaMallocAsync(&spec, sizeof(cplx_t<R>) * cnt, s));
+  int32_t r = c2r_full<R>((const R *)t->g, spec, grid, n, s);
+  if (r == kOk) {
+    self_extract_kernel<R><<<1, 128, 0, s>>>(grid, n, (R *)t->self);
+    PYFOF_CHECK_LAUNCH();
+  }
+  cudaFreeAsync(grid, s);
+  cudaFreeAsync(spec, s);
+  PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaStreamSynchronize(s));
+  if (r != kOk) return r;
+  if (ctx.h_flags[FLAG_ERR]) {
+    set_error("Green's function: zero assignment response");
+    return kInvalid;
+  }
+  ctx.green[key] = t;
+  *out = t;
+  return kOk;
+}
+
+// ---------------------------------------------------------------- setup
+
+struct PmHalo {      // device copy of one PM halo's parameters
+  int64_t off;       // first member
+  int32_t np;
+  int32_t n, sup;    // grid size and support side (n/2+1)
+  float spacing;
+  float origin[3];
+  int64_t cell_off;  // first C2 cell
+  int32_t nc[3];     // C2 cells per axis
+  double u_min[3];   // C2 cell origin (q/spacing units)
+  double mkeep;      // kept mass at the start of the pass (FP64)
+  int32_t np_bound, status, pending, pad;
+};
+
+// TSC weights and self potential (bound_fortran.f90:2562-2602).  FP32
+// weights as in the reference; the self term accumulates in FP64.
+template <typename R>
+__global__ void pm_setup_kernel(const Members m, const PmHalo *__restrict__ H,
+                                const int32_t *__restrict__ mhalo, int64_t M,
+                                const R *const *__restrict__ selfs, int3 *__restrict__ first,
+                                float *__restrict__ wt, R *__restrict__ selfv, int32_t *flags) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int h = mhalo[k];
+    if (h < 0) continue;
+    const PmHalo &p = H[h];
+    float w9[9];
+    int f[3];
+    bool bad = false;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float t = __fdiv_rn(__fsub_rn(m.q[d][k], p.origin[d]), p.spacing);
+      if (!isfinite(t)) bad = true;
+      if (!(t >= 0.0f) || t >= (float)(p.n / 2 - 1)) bad = true;
+      const int nearest = (int)lroundf(t);
+      const float dl = __fsub_rn(t, (float)nearest);
+      const float a = __fsub_rn(0.5f, dl), b = __fadd_rn(0.5f, dl);
+      w9[3 * d + 0] = __fmul_rn(0.5f, __fmul_rn(a, a));
+      w9[3 * d + 1] = __fsub_rn(0.75f, __fmul_rn(dl, dl));
+      w9[3 * d + 2] = __fmul_rn(0.5f, __fmul_rn(b, b));
+      f[d] = nearest;
+    }
+    if (bad) {
+      atomicCAS(&flags[FLAG_ERR], 0, kInvalid);
+      continue;
+    }
+    const R *sp = selfs[h];
+    double acc = 0.0;
+    for (int sz = 0; sz < 3; ++sz)
+      for (int sy = 0; sy < 3; ++sy)
+        for (int sx = 0; sx < 3; ++sx) {
+          const float sw = __fmul_rn(__fmul_rn(w9[sx], w9[3 + sy]), w9[6 + sz]);
+          for (int tz = 0; tz < 3; ++tz)
+            for (int ty = 0; ty < 3; ++ty)
+              for (int tx = 0; tx < 3; ++tx) {
+                const float tw = __fmul_rn(__fmul_rn(w9[tx], w9[3 + ty]), w9[6 + tz]);
+                acc += (double)__fmul_rn(sw, tw) *
+                       (double)sp[((tz - sz + 2) * 5 + (ty - sy + 2)) * 5 + (tx - sx + 2)];
+              }
+        }
+    selfv[k] = (R)acc;
+    first[k] = make_int3(f[0], f[1], f[2]);
+#pragma unroll
+    for (int j = 0; j < 9; ++j) wt[9 * k + j] = w9[j];
+  }
+}
+
+// u = q/spacing extent of every PM halo (bound_build_cells :3134-3138)
+__global__ void __launch_bounds__(BLK) pm_extent_kernel(const Members m, const PmHalo *__restrict__ H,
+                                                        int nh, double *__restrict__ ext) {
+  const int h = blockIdx.x;
+  if (h >= nh) return;
+  const PmHalo &p = H[h];
+  double lo[3] = {1e30, 1e30, 1e30}, hi[3] = {-1e30, -1e30, -1e30};
+  for (int64_t k = p.off + threadIdx.x; k < p.off + p.np; k += BLK)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double u = (double)m.q[d][k] / (double)p.spacing;
+      lo[d] = fmin(lo[d], u);
+      hi[d] = fmax(hi[d], u);
+    }
+  __shared__ double slo[3][BLK / 32], shi[3][BLK / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int d = 0; d < 3; ++d) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+      hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+    }
+    if (lane == 0) { slo[d][warp] = lo[d]; shi[d][warp] = hi[d]; }
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int d = threadIdx.x;
+    double a = slo[d][0], b = shi[d][0];
+    for (int w = 1; w < BLK / 32; ++w) { a = fmin(a, slo[d][w]); b = fmax(b, shi[d][w]); }
+    ext[6 * h + d] = a;
+    ext[6 * h + 3 + d] = b;
+  }
+}
+
+// C2 cell key of every PM member (bound_build_cells :3166-3172)
+__global__ void pm_cellkey_kernel(const Members m, const PmHalo *__restrict__ H,
+                                  const int32_t *__restrict__ mhalo, int64_t M,
+                                  uint32_t *__restrict__ key, uint32_t sentinel) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int h = mhalo[k];
+    if (h < 0) { key[k] = sentinel; continue; }
+    const PmHalo &p = H[h];
+    int64_t c[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double u = (double)m.q[d][k] / (double)p.spacing;
+      double v = floor((u - p.u_min[d]) / 3.5) + 1.0;
+      if (!(v >= 1.0)) v = 1.0;
+      if (v > (double)p.nc[d]) v = (double)p.nc[d];
+      c[d] = (int64_t)v - 1;
+    }
+    key[k] = (uint32_t)(p.cell_off + c[0] + (int64_t)p.nc[0] * (c[1] + (int64_t)p.nc[1] * c[2]));
+  }
+}
+
+__global__ void pm_cellcount_kernel(const uint32_t *__restrict__ key, int64_t M,
+                                    uint32_t sentinel, uint32_t *__restrict__ cnt) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x)
+    if (key[k] != sentinel) atomicAdd(&cnt[key[k]], 1u);
+}
+
+// ---------------------------------------------------------------- passes
+
+template <typename R>
+__global__ void pm_deposit_kernel(const Members m, const PmHalo *__restrict__ H,
+                                  const int32_t *__restrict__ mhalo, const uint8_t *__restrict__ keep,
+                                  const int3 *__restrict__ first, const float *__restrict__ wt,
+                                  const int32_t *__restrict__ slot, int64_t M, R *__restrict__ rho) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int h = mhalo[k];
+    if (h < 0 || !keep[k]) continue;
+    const PmHalo &p = H[h];
+    const int sl = slot[h];
+    if (sl < 0 || !p.pending) continue;
+    const int sup = p.sup;
+    R *g = rho + (int64_t)sl * sup * sup * sup;
+    const int3 f = first[k];
+    const float *w9 = wt + 9 * k;
+    const float wk = m.w[k];
+    for (int sz = 0; sz < 3; ++sz) {
+      const int z = f.z + sz - 1;
+      for (int sy = 0; sy < 3; ++sy) {
+        const int y = f.y + sy - 1;
+        for (int sx = 0; sx < 3; ++sx) {
+          const int x = f.x + sx - 1;
+          const R v = (R)__fmul_rn(__fmul_rn(__fmul_rn(wk, w9[sx]), w9[3 + sy]), w9[6 + sz]);
+          atomicAdd(&g[((int64_t)z * sup + y) * sup + x], v);
+        }
+      }
+    }
+  }
+}
+
+// TSC gather and the C1 potential (bound_fortran.f90:2681-2703)
+template <typename R>
+__global__ void pm_gather_kernel(const Members m, const PmHalo *__restrict__ H,
+                                 const int32_t *__restrict__ mhalo, const uint8_t *__restrict__ keep,
+                                 const int3 *__restrict__ first, const float *__restrict__ wt,
+                                 const R *__restrict__ selfv, const int32_t *__restrict__ slot, int64_t M,
+                                 const R *__restrict__ rho, double a_val, R *__restrict__ phi_c1) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int h = mhalo[k];
+    if (h < 0 || !keep[k]) continue;
+    const PmHalo &p = H[h];
+    const int sl = slot[h];
+    if (sl < 0 || !p.pending) continue;
+    const int sup = p.sup;
+    const R *g = rho + (int64_t)sl * sup * sup * sup;
+    const int3 f = first[k];
+    const float *w9 = wt + 9 * k;
+    R raw = 0;
+    for (int sz = 0; sz < 3; ++sz) {
+      const int z = f.z + sz - 1;
+      for (int sy = 0; sy < 3; ++sy) {
+        const int y = f.y + sy - 1;
+        for (int sx = 0; sx < 3; ++sx) {
+          const int x = f.x + sx - 1;
+          raw += g[((int64_t)z * sup + y) * sup + x] * (R)w9[sx] * (R)w9[3 + sy] * (R)w9[6 + sz];
+        }
+      }
+    }
+    const R wk = (R)m.w[k];
+    const double rest = p.mkeep - (double)m.w[k];
+    const R radius = (R)p.n / (R)2;
+    const R dz0 = (R)(rest > 0.0 ? rest : 0.0) / radius;
+    const R pref = (R)(a_val / (6.0 * kPi * (double)p.spacing));
+    phi_c1[k] = pref * ((raw - wk * selfv[k]) - dz0);
+  }
+}
+
+// bound_depth_continuous / bound_c2_delta_depth (:3080-3117)
+template <typename T>
+__device__ __forceinline__ T depth_c(T r, T h) {
+  if (r <= (T)0) return (T)208 / ((T)70 * h);
+  if (r >= h) return (T)1 / r;
+  const T e = (T)2 * r / h;
+  if (e <= (T)1) {
+    const T prim = e * e * ((T)112 + e * e * ((T)-56 + e * ((T)14 + e * ((T)8 - (T)3 * e))));
+    return ((T)208 - prim) / ((T)70 * h);
+  }
+  const T prim = e * e * ((T)448 + e * ((T)-280 + e * ((T)56 + e * ((T)14 + e * ((T)-8 + e))))) -
+                 (T)224 * e - (T)12 / e;
+  return ((T)128 - prim) / ((T)70 * h);
+}
+
+template <typename T>
+__device__ __forceinline__ T c2_delta(T r, T ht, T hs) {
+  if (r <= (T)0) return ((T)208 / (T)70) * ((T)1 / ht - (T)1 / hs);
+  if (r >= ht && r >= hs) return (T)0;
+  return depth_c<T>(r, ht) - depth_c<T>(r, hs);
+}
+
+// C2 residual of every kept member over the kept members within 3.5 grid
+// cells, from the 27 neighbouring 3.5-cells.
+template <typename R>
+__global__ void pm_c2_kernel(const Members m, const PmHalo *__restrict__ H,
+                             const int32_t *__restrict__ mhalo, const uint8_t *__restrict__ keep,
+                             const uint32_t *__restrict__ ckey, const uint32_t *__restrict__ cstart,
+                             const uint32_t *__restrict__ cmem, int64_t M, double a_val, double app,
+                             R *__restrict__ phi_c2) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int h = mhalo[k];
+    if (h < 0 || !keep[k]) continue;
+    const PmHalo &p = H[h];
+    if (!p.pending) continue;
+    const double sp = (double)p.spacing;
+    const R ht = (R)((double)(float)app / sp);
+    const R hs = (R)3.5;
+    const R r2cut = (R)(12.25 * sp * sp);
+    const R inv_sp = (R)(1.0 / sp);
+    const R pref = (R)(a_val / (6.0 * kPi * sp));
+    const int64_t local = (int64_t)ckey[k] - p.cell_off;
+    const int64_t n0 = p.nc[0], n1 = p.nc[1], n2 = p.nc[2];
+    const int64_t cx = local % n0, cy = (local / n0) % n1, cz = local / (n0 * n1);
+    const float xi = m.q[0][k], yi = m.q[1][k], zi = m.q[2][k];
+    R acc = 0, comp = 0;
+    for (int64_t z = cz - 1; z <= cz + 1; ++z) {
+      if (z < 0 || z >= n2) continue;
+      for (int64_t y = cy - 1; y <= cy + 1; ++y) {
+        if (y < 0 || y >= n1) continue;
+        for (int64_t x = cx - 1; x <= cx + 1; ++x) {
+          if (x < 0 || x >= n0) continue;
+          const int64_t c = p.cell_off + x + n0 * (y + n1 * z);
+          for (uint32_t e = cstart[c]; e < cstart[c + 1]; ++e) {
+            const int64_t j = cmem[e];
+            if (j == k || !keep[j]) continue;
+            const R dx = (R)__fsub_rn(m.q[0][j], xi);
+            const R dy = (R)__fsub_rn(m.q[1][j], yi);
+            const R dz = (R)__fsub_rn(m.q[2][j], zi);
+            const R r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 < r2cut) {
+              const R r = sqrt(r2) * inv_sp;
+              const R dphi = -pref * c2_delta<R>(r, ht, hs);
+              // compensated accumulation
+              const R yv = (R)m.w[j] * dphi - comp;
+              const R t = acc + yv;
+              comp = (t - acc) - yv;
+              acc = t;
+            }
+          }
+        }
+      }
+    }
+    phi_c2[k] = acc;
+  }
+}
+
+// ---------------------------------------------------------------- removal
+
+__device__ __forceinline__ double bsum_d(double v, double *red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+  __syncthreads();
+  return t;
+}
+
+__device__ __forceinline__ int bsum_i(int v, int *red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  int t = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+  __syncthreads();
+  return t;
+}
+
+// One block per pending halo: combine the potential, then the inner
+// removal loop of bound_check_grid (:2739-2855).  Leaves status -1 when the
+// potential must be refreshed (next pass).
+template <typename R>
+__global__ void __launch_bounds__(IBLK) pm_inner_kernel(const Members m, PmHalo *__restrict__ H,
+                                                        const int32_t *__restrict__ list, int nlist,
+                                                        uint8_t *__restrict__ keep,
+                                                        const R *__restrict__ phi_c1,
+                                                        const R *__restrict__ phi_c2,
+                                                        float *__restrict__ phi,
+                                                        float *__restrict__ en, float b_val, int nmin,
+                                                        int phi_only, int32_t *flags) {
+  const int h = list[blockIdx.x];
+  PmHalo &p = H[h];
+  if (!p.pending) return;
+  __shared__ double red_d[IBLK / 32];
+  __shared__ int red_i[IBLK / 32];
+  __shared__ unsigned hist[256];
+  __shared__ int s_err;
+  const int64_t b0 = p.off, np = p.np;
+  if (threadIdx.x == 0) s_err = 0;
+  int np_bound = p.np_bound;
+  const int n_source = np_bound;
+  for (int64_t i = threadIdx.x; i < np; i += IBLK) {
+    const int64_t k = b0 + i;
+    if (!keep[k]) continue;
+    float v = (float)(phi_c1[k] + phi_c2[k]);
+    if (np_bound == 1 || n_source == 1) v = 0.0f;
+    if (!isfinite(v)) s_err = kNonFinite;
+    phi[k] = v;
+  }
+  __syncthreads();
+  if (s_err) {
+    if (threadIdx.x == 0) atomicCAS(&flags[FLAG_ERR], 0, s_err);
+    return;
+  }
+  if (phi_only) {
+    if (threadIdx.x == 0) { p.status = 0; p.pending = 0; }
+    return;
+  }
+  int deleted = 0, status = -1;
+  for (;;) {
+    double a7[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int64_t i = threadIdx.x; i < np; i += IBLK) {
+      const int64_t k = b0 + i;
+      if (!keep[k]) continue;
+      const double wi = (double)m.w[k];
+      a7[0] += wi;
+      for (int d = 0; d < 3; ++d) { a7[1 + d] += wi * (double)m.q[d][k]; a7[4 + d] += wi * (double)m.v[d][k]; }
+    }
+    for (int j = 0; j < 7; ++j) a7[j] = bsum_d(a7[j], red_d);
+    float qc[3], vc[3];
+    for (int d = 0; d < 3; ++d) {
+      qc[d] = __double2float_rn(a7[1 + d] / a7[0]);
+      vc[d] = __double2float_rn(a7[4 + d] / a7[0]);
+    }
+    int nu = 0;
+    for (int64_t i = threadIdx.x; i < np; i += IBLK) {
+      const int64_t k = b0 + i;
+      if (!keep[k]) continue;
+      float s = 0.f;
+      for (int d = 0; d < 3; ++d) {
+        const float dv = __fadd_rn(__fsub_rn(m.v[d][k], vc[d]), __fmul_rn(b_val, __fsub_rn(m.q[d][k], qc[d])));
+        s = d == 0 ? __fmul_rn(dv, dv) : __fadd_rn(s, __fmul_rn(dv, dv));
+      }
+      const float e = __fadd_rn(__fdiv_rn(s, 2.0f), phi[k]);
+      if (!isfinite(e)) s_err = kInvalid;
+      en[k] = e;
+      nu += e >= 0.0f;
+    }
+    nu = bsum_i(nu, red_i);
+    if (s_err) break;
+    if (nu == 0) {
+      if (deleted == 0) status = 0;
+      break;
+    }
+    int nb = max(1, (int)ceil(0.02 * (double)np_bound));
+    nb = min(nu, nb);
+    // radix select of the nb largest energies among the unbound members:
+    // key = bits of (E + 0) (E >= 0, so the bits order like the values)
+    unsigned prefix = 0, mask = 0;
+    int need = nb;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+      for (int t = threadIdx.x; t < 256; t += IBLK) hist[t] = 0;
+      __syncthreads();
+      for (int64_t i = threadIdx.x; i < np; i += IBLK) {
+        const int64_t k = b0 + i;
+        if (!keep[k]) continue;
+        const float e = en[k];
+        if (!(e >= 0.0f)) continue;
+        const unsigned key = __float_as_uint(e + 0.0f);
+        if ((key & mask) != prefix) continue;
+        atomicAdd(&hist[(key >> shift) & 255u], 1u);
+      }
+      __syncthreads();
+      // digit holding the need-th largest key
+      int digit = 255, above = 0;
+      for (; digit >= 0; --digit) {
+        const int c = (int)hist[digit];
+        if (above + c >= need) break;
+        above += c;
+      }
+      __syncthreads();
+      need -= above;
+      prefix |= (unsigned)digit << shift;
+      mask |= 255u << shift;
+    }
+    // delete every key > threshold and the `need` lowest indices among
+    // key == threshold (equal energies: lower index first)
+    const unsigned thr = prefix;
+    int taken_eq = 0;
+    for (int64_t base = 0; base < np; base += IBLK) {
+      const int64_t i = base + threadIdx.x;
+      int64_t k = b0 + i;
+      bool del_gt = false, is_eq = false;
+      if (i < np && keep[k]) {
+        const float e = en[k];
+        if (e >= 0.0f) {
+          const unsigned key = __float_as_uint(e + 0.0f);
+          del_gt = key > thr;
+          is_eq = key == thr;
+        }
+      }
+      // ordered rank of is_eq within this chunk
+      const unsigned bal = __ballot_sync(0xffffffffu, is_eq);
+      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      __syncthreads();
+      if (lane == 0) red_i[warp] = __popc(bal);
+      __syncthreads();
+      int before = taken_eq;
+      for (int w = 0; w < warp; ++w) before += red_i[w];
+      before += __popc(bal & ((1u << lane) - 1u));
+      int chunk_eq = 0;
+      for (int w = 0; w < IBLK / 32; ++w) chunk_eq += red_i[w];
+      if (i < np && (del_gt || (is_eq && before < need))) keep[k] = 0;
+      taken_eq += chunk_eq;
+      __syncthreads();
+    }
+    np_bound -= nb;
+    deleted += nb;
+    if (np_bound < nmin) { status = 1; break; }
+    if ((double)deleted >= 0.2 * (double)np_bound) break;
+  }
+  __syncthreads();
+  if (s_err) {
+    if (threadIdx.x == 0) atomicCAS(&flags[FLAG_ERR], 0, s_err);
+    return;
+  }
+  if (threadIdx.x == 0) {
+    p.np_bound = np_bound;
+    p.status = status;
+    if (status >= 0) p.pending = 0;
+  }
+}
+
+__global__ void pm_mkeep_kernel(const Members m, PmHalo *__restrict__ H, const int32_t *list, int nlist,
+                                const uint8_t *__restrict__ keep) {
+  const int h = list[blockIdx.x];
+  PmHalo &p = H[h];
+  if (!p.pending) return;
+  double s = 0.0;
+  for (int64_t i = threadIdx.x; i < p.np; i += blockDim.x) {
+    const int64_t k = p.off + i;
+    if (keep[k]) s += (double)m.w[k];
+  }
+  __shared__ double red[32];
+  s = bsum_d(s, red);
+  if (threadIdx.x == 0) p.mkeep = s;
+}
+
+__global__ void pm_mark_halo_kernel(const PmHalo *__restrict__ H, int nh, int32_t *__restrict__ mhalo) {
+  const int h = blockIdx.x;
+  if (h >= nh) return;
+  for (int64_t i = threadIdx.x; i < H[h].np; i += blockDim.x) mhalo[H[h].off + i] = h;
+}
+
+__global__ void pm_fill_i32(int32_t *a, int64_t n, int32_t v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = v;
+}
+
+__global__ void pm_fill_u8(uint8_t *a, int64_t n, uint8_t v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = v;
+}
+
+template <typename R>
+__global__ void pm_zero_kernel(R *a, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = (R)0;
+}
+
+// Members per 16-cell region of every 256-grid halo
+// (bound_two_level_setup_ratios, bound_fortran.f90:551-568).
+__global__ void pm_region_count_kernel(const Members m, const PmHalo *__restrict__ H,
+                                       const int32_t *__restrict__ mhalo, int64_t M,
+                                       uint32_t *__restrict__ cnt) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int h = mhalo[k];
+    if (h < 0 || H[h].n != 256) continue;
+    const PmHalo &p = H[h];
+    int b[3];
+    for (int d = 0; d < 3; ++d) {
+      const float t = (float)(((double)m.q[d][k] - (double)p.origin[d]) / (double)p.spacing);
+      const int c = (int)floor((double)t) / 16;
+      b[d] = c < 0 ? 0 : (c > 7 ? 7 : c);
+    }
+    atomicAdd(&cnt[(int64_t)h * 512 + b[0] + 8 * b[1] + 64 * b[2]], 1u);
+  }
+}
+
+int bits_for(uint64_t v) {
+  int b = 0;
+  while (b < 64 && (v >> b) != 0) ++b;
+  return b;
+}
+
+template <typename R>
+int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Members &m,
+               const std::vector<HaloTask> &tasks, const std::vector<int32_t> &list,
+               HaloResult *res, uint8_t *keep, float *phi_out, int phi_only) {
+  (void)rules;
+  cudaStream_t s = ctx.stream;
+  Arena &W = ctx.work;
+  const int nh = (int)list.size();
+  const int64_t M = tasks.back().off + tasks.back().np;  // all packed members
+  // Green tables of the grid classes in use
+  std::shared_ptr<GreenTable> green_of[257];
+  std::vector<PmHalo> H(nh);
+  std::vector<const R *> selfs(nh);
+  for (int h = 0; h < nh; ++h) {
+    const HaloTask &t = tasks[list[h]];
+    PmHalo &p = H[h];
+    std::memset(&p, 0, sizeof(p));
+    p.off = t.off;
+    p.np = t.np;
+    p.n = t.n;
+    p.sup = t.n / 2 + 1;
+    p.spacing = t.spacing;
+    for (int d = 0; d < 3; ++d) p.origin[d] = t.origin[d];
+    p.np_bound = t.np;
+    p.status = -1;
+    p.pending = 1;
+    if (!green_of[t.n]) PYFOF_TRY(get_green<R>(ctx, t.n, 3.5, 0.0, 1, &green_of[t.n]));
+    selfs[h] = (const R *)green_of[t.n]->self;
+  }
+  PmHalo *dH = W.carve<PmHalo>(nh);
+  int32_t *dlist = W.carve<int32_t>(nh);
+  const R **dselfs = W.carve<const R *>(nh);
+  int32_t *mhalo = W.carve<int32_t>(M);
+  int3 *first = W.carve<int3>(M);
+  float *wt = W.carve<float>(9 * (size_t)M);
+  R *selfv = W.carve<R>(M), *c1 = W.carve<R>(M), *c2 = W.carve<R>(M);
+  float *phi = W.carve<float>(M), *en = W.carve<float>(M);
+  double *ext = W.carve<double>(6 * (size_t)nh);
+  if (!dH || !dlist || !dselfs || !mhalo || !first || !wt || !selfv || !c1 || !c2 || !phi || !en || !ext) {
+    set_error("workspace exhausted (PM members)");
+    return kAlloc;
+  }
+  std::vector<int32_t> hl(nh);
+  for (int h = 0; h < nh; ++h) hl[h] = h;
+  PYFOF_CUDA(cudaMemcpyAsync(dH, H.data(), sizeof(PmHalo) * nh, cudaMemcpyHostToDevice, s));
+  PYFOF_CUDA(cudaMemcpyAsync(dlist, hl.data(), sizeof(int32_t) * nh, cudaMemcpyHostToDevice, s));
+  PYFOF_CUDA(cudaMemcpyAsync(dselfs, selfs.data(), sizeof(R *) * nh, cudaMemcpyHostToDevice, s));
+  const unsigned gM = (unsigned)std::min<int64_t>(ceil_div(M, BLK), (int64_t)kNumSMs * 16);
+  pm_fill_i32<<<gM, BLK, 0, s>>>(mhalo, M, -1);
+  PYFOF_CHECK_LAUNCH();
+  pm_mark_halo_kernel<<<nh, BLK, 0, s>>>(dH, nh, mhalo);
+  PYFOF_CHECK_LAUNCH();
+  pm_setup_kernel<R><<<gM, BLK, 0, s>>>(m, dH, mhalo, M, dselfs, first, wt, selfv, ctx.d_flags);
+  PYFOF_CHECK_LAUNCH();
+  // mark PM members kept
+  for (int h = 0; h < nh; ++h) {
+    PYFOF_CUDA(cudaMemsetAsync(keep + H[h].off, 1, (size_t)H[h].np, s));
+  }
+  // dense 16-cell regions of 256-grid halos would switch the reference to
+  // its two-level inner refinement, which this solver does not implement:
+  // refuse such input instead of returning a different answer
+  {
+    uint32_t *rc = W.carve<uint32_t>((size_t)nh * 512);
+    if (!rc) { set_error("workspace exhausted (regions)"); return kAlloc; }
+    PYFOF_CUDA(cudaMemsetAsync(rc, 0, sizeof(uint32_t) * nh * 512, s));
+    pm_region_count_kernel<<<gM, BLK, 0, s>>>(m, dH, mhalo, M, rc);
+    PYFOF_CHECK_LAUNCH();
+    std::vector<uint32_t> hrc((size_t)nh * 512);
+    PYFOF_CUDA(cudaMemcpyAsync(hrc.data(), rc, sizeof(uint32_t) * nh * 512, cudaMemcpyDeviceToHost, s));
+    PYFOF_CUDA(cudaStreamSynchronize(s));
+    for (int h = 0; h < nh; ++h) {
+      if (H[h].n != 256) continue;
+      const bool r2ok = 3.5 * ((double)H[h].spacing / 2.0) >= (double)(float)a.softening;
+      for (int b = 0; b < 512 && r2ok; ++b)
+        if (hrc[(size_t)h * 512 + b] >= 3926u) {
+          set_error("candidate with %d members needs the two-level inner refinement, which is "
+                    "not implemented", H[h].np);
+          return kInvalid;
+        }
+    }
+  }
+  // C2 cells (3.5 grid cells)
+  pm_extent_kernel<<<nh, BLK, 0, s>>>(m, dH, nh, ext);
+  PYFOF_CHECK_LAUNCH();
+  std::vector<double> hext(6 * (size_t)nh);
+  PYFOF_CUDA(cudaMemcpyAsync(hext.data(), ext, sizeof(double) * 6 * nh, cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaStreamSynchronize(s));
+  int64_t ncell = 0;
+  for (int h = 0; h < nh; ++h) {
+    PmHalo &p = H[h];
+    p.cell_off = ncell;
+    int64_t c = 1;
+    for (int d = 0; d < 3; ++d) {
+      p.u_min[d] = hext[6 * h + d];
+      const double span = hext[6 * h + 3 + d] - hext[6 * h + d];
+      p.nc[d] = std::max(1, (int)std::floor(span / 3.5) + 1);
+      c *= p.nc[d];
+    }
+    ncell += c;
+  }
+  if (ncell >= 0xffffffffll) { set_error("too many C2 cells"); return kAlloc; }
+  PYFOF_CUDA(cudaMemcpyAsync(dH, H.data(), sizeof(PmHalo) * nh, cudaMemcpyHostToDevice, s));
+  uint32_t *ckey = W.carve<uint32_t>(M), *cstart = W.carve<uint32_t>(ncell + 2);
+  uint32_t *ka = W.carve<uint32_t>(M), *va = W.carve<uint32_t>(M), *kb = W.carve<uint32_t>(M),
+           *vb = W.carve<uint32_t>(M);
+  if (!ckey || !cstart || !ka || !va || !kb || !vb) { set_error("workspace exhausted (C2 cells)"); return kAlloc; }
+  const uint32_t sentinel = (uint32_t)ncell;
+  pm_cellkey_kernel<<<gM, BLK, 0, s>>>(m, dH, mhalo, M, ckey, sentinel);
+  PYFOF_CHECK_LAUNCH();
+  PYFOF_CUDA(cudaMemsetAsync(cstart, 0, sizeof(uint32_t) * (ncell + 2), s));
+  pm_cellcount_kernel<<<gM, BLK, 0, s>>>(ckey, M, sentinel, cstart);
+  PYFOF_CHECK_LAUNCH();
+  PYFOF_TRY(exclusive_scan_u32(cstart, cstart, ncell + 1, nullptr, W, s));
+  uint32_t *sk, *cmem;
+  PYFOF_TRY(radix_sort_pairs(ckey, nullptr, M, bits_for((uint64_t)ncell), ka, va, kb, vb, &sk, &cmem, W, s));
+  PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaStreamSynchronize(s));
+  if (ctx.h_flags[FLAG_ERR]) {
+    set_error("particle outside the PM source domain or non-finite grid coordinate");
+    return ctx.h_flags[FLAG_ERR];
+  }
+
+  // grid batches per class, bounded by a spectrum budget
+  const size_t budget = (size_t)8 << 30;
+  for (int pass = 1; pass <= kMaxPasses; ++pass) {
+    std::vector<int32_t> pend;
+    for (int h = 0; h < nh; ++h) if (H[h].pending) pend.push_back(h);
+    if (pend.empty()) break;
+    int32_t *dpend = W.carve<int32_t>(pend.size());
+    if (!dpend) { set_error("workspace exhausted (pending)"); return kAlloc; }
+    PYFOF_CUDA(cudaMemcpyAsync(dpend, pend.data(), sizeof(int32_t) * pend.size(), cudaMemcpyHostToDevice, s));
+    pm_mkeep_kernel<<<(unsigned)pend.size(), 256, 0, s>>>(m, dH, dpend, (int)pend.size(), keep);
+    PYFOF_CHECK_LAUNCH();
+    for (int n : {48, 64, 128, 256}) {
+      std::vector<int32_t> grp;
+      for (int h : pend) if (H[h].n == n) grp.push_back(h);
+      if (grp.empty()) continue;
+      const int sup = n / 2 + 1;
+      const size_t spec_bytes = sizeof(cplx_t<R>) * (size_t)(n / 2 + 1) * n * n;
+      const size_t per = spec_bytes + sizeof(R) * (size_t)sup * sup * sup;
+      const int maxb = (int)std::max<size_t>(1, budget / per);
+      for (size_t g0 = 0; g0 < grp.size(); g0 += maxb) {
+        const int nb = (int)std::min<size_t>(maxb, grp.size() - g0);
+        std::vector<int32_t> hslot(nh, -1);
+        for (int j = 0; j < nb; ++j) hslot[grp[g0 + j]] = j;
+        int32_t *dslot = W.carve<int32_t>(nh);
+        if (!dslot) { set_error("workspace exhausted (slots)"); return kAlloc; }
+        PYFOF_CUDA(cudaMemcpyAsync(dslot, hslot.data(), sizeof(int32_t) * nh, cudaMemcpyHostToDevice, s));
+        R *rho = W.carve<R>((size_t)nb * sup * sup * sup);
+        cplx_t<R> *spec = W.carve<cplx_t<R>>((size_t)nb * (n / 2 + 1) * n * n);
+        if (!rho || !spec) { set_error("workspace exhausted (PM grids)"); return kAlloc; }
+        const int64_t ng = (int64_t)nb * sup * sup * sup;
+        pm_zero_kernel<R><<<(unsigned)std::min<int64_t>(ceil_div(ng, BLK), 148 * 16), BLK, 0, s>>>(rho, ng);
+        PYFOF_CHECK_LAUNCH();
+        pm_deposit_kernel<R><<<gM, BLK, 0, s>>>(m, dH, mhalo, keep, first, wt, dslot, M, rho);
+        PYFOF_CHECK_LAUNCH();
+        PYFOF_TRY(pm_convolve_batch<R>(rho, spec, (const R *)green_of[n]->g, n, sup, nb, s));
+        pm_gather_kernel<R><<<gM, BLK, 0, s>>>(m, dH, mhalo, keep, first, wt, selfv, dslot, M, rho, a.a_val,
+                                               c1);
+        PYFOF_CHECK_LAUNCH();
+      }
+    }
+    pm_c2_kernel<R><<<gM, BLK, 0, s>>>(m, dH, mhalo, keep, ckey, cstart, cmem, M, a.a_val, a.softening, c2);
+    PYFOF_CHECK_LAUNCH();
+    pm_inner_kernel<R><<<(unsigned)pend.size(), IBLK, 0, s>>>(m, dH, dpend, (int)pend.size(), keep, c1, c2, phi,
+                                                           en, (float)a.b_val, a.np_halo_min, phi_only,
+                                                           ctx.d_flags);
+    PYFOF_CHECK_LAUNCH();
+    PYFOF_CUDA(cudaMemcpyAsync(H.data(), dH, sizeof(PmHalo) * nh, cudaMemcpyDeviceToHost, s));
+    PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    PYFOF_CUDA(cudaStreamSynchronize(s));
+    if (ctx.h_flags[FLAG_ERR]) {
+      set_error("particle-mesh unbinding failed (error %d)", ctx.h_flags[FLAG_ERR]);
+      return ctx.h_flags[FLAG_ERR];
+    }
+  }
+  std::vector<HaloResult> hr(nh);
+  for (int h = 0; h < nh; ++h) {
+    hr[h].status = H[h].pending ? 5 : H[h].status;
+    hr[h].np_bound = H[h].np_bound;
+  }
+  for (int h = 0; h < nh; ++h)
+    PYFOF_CUDA(cudaMemcpyAsync(res + list[h], &hr[h], sizeof(HaloResult), cudaMemcpyHostToDevice, s));
+  if (phi_out) PYFOF_CUDA(cudaMemcpyAsync(phi_out, phi, sizeof(float) * M, cudaMemcpyDeviceToDevice, s));
+  PYFOF_CUDA(cudaStreamSynchronize(s));
+  return kOk;
+}
+
+}  // namespace
+
 int32_t unbind_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Members &m,
                   const std::vector<HaloTask> &tasks, const std::vector<int32_t> &list,
-                  HaloResult *res, uint8_t *keep, float *phi_out) {
-  (void)ctx; (void)a; (void)rules; (void)m; (void)tasks; (void)list; (void)res; (void)keep;
-  (void)phi_out;
-  set_error("particle-mesh unbinding (candidates above 1000 members) is not available yet");
-  return kInvalid;
+                  HaloResult *res, uint8_t *keep, float *phi_out, int phi_only) {
+  if (a.bound_fp64) return run_pm<double>(ctx, a, rules, m, tasks, list, res, keep, phi_out, phi_only);
+  return run_pm<float>(ctx, a, rules, m, tasks, list, res, keep, phi_out, phi_only);
 }
 
 }  // namespace pyfof
