@@ -190,6 +190,7 @@ int32_t pyfof_get_stat(const char *key, int64_t *value) {
   if (!std::strcmp(key, "direct_halos")) { *value = c->last_direct; return kOk; }
   if (!std::strcmp(key, "pm_halos")) { *value = c->last_pm; return kOk; }
   if (!std::strcmp(key, "valid_halos")) { *value = c->last_valid; return kOk; }
+  if (!std::strcmp(key, "refined_regions")) { *value = c->last_tl_regions; return kOk; }
   set_error("unknown statistic %s", key);
   return kInvalid;
 }

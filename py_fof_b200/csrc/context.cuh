@@ -26,7 +26,7 @@ struct Context {
   float stage_ms[16] = {};
   // statistics of the last call
   int64_t last_cells = 0, last_active = 0, last_candidates = 0, last_dense = 0;
-  int64_t last_direct = 0, last_pm = 0, last_valid = 0;
+  int64_t last_direct = 0, last_pm = 0, last_valid = 0, last_tl_regions = 0;
   ~Context();
 };
 

@@ -192,7 +192,11 @@ struct PmHalo {      // device copy of one PM halo's parameters
   int32_t nc[3];     // C2 cells per axis
   double u_min[3];   // C2 cell origin (q/spacing units)
   double mkeep;      // kept mass at the start of the pass (FP64)
-  int32_t np_bound, status, pending, pad;
+  double cw_u;       // short-range cell width (grid units): 3.5, or 3.5/r_max two-level
+  int32_t np_bound, status, pending;
+  int32_t two_level; // dense regions refined on 128^3 / 216^3 inner grids
+  int32_t r_max;     // largest refinement ratio of the halo's members
+  int32_t pad;
 };
 
 // TSC weights and self potential (bound_fortran.f90:2562-2602).  FP32
@@ -294,7 +298,7 @@ __global__ void pm_cellkey_kernel(const Members m, const PmHalo *__restrict__ H,
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const double u = (double)m.q[d][k] / (double)p.spacing;
-      double v = floor((u - p.u_min[d]) / 3.5) + 1.0;
+      double v = floor((u - p.u_min[d]) / p.cw_u) + 1.0;
       if (!(v >= 1.0)) v = 1.0;
       if (v > (double)p.nc[d]) v = (double)p.nc[d];
       c[d] = (int64_t)v - 1;
@@ -403,14 +407,19 @@ __device__ __forceinline__ T c2_delta(T r, T ht, T hs) {
   return depth_c<T>(r, ht) - depth_c<T>(r, hs);
 }
 
-// C2 residual of every kept member over the kept members within 3.5 grid
-// cells, from the 27 neighbouring 3.5-cells.
+// Short-range residual of every kept member: the spline-softened kernel
+// minus the split kernel its potential already contains, over the kept
+// members within the member's own cutoff a_i = 3.5 spacing / r_i, where
+// r_i = 1 for plain C2 halos (bound_c2_calc_cells, :3403-3483; in grid
+// units there) and the region refinement ratio for two-level halos
+// (bound_two_level_pp_full, :1088-1343).  Both are
+//     phi_i += w_j * -(a/(6 pi)) * (D(d, eps) - D(d, a_i)),  d < a_i.
 template <typename R>
-__global__ void pm_c2_kernel(const Members m, const PmHalo *__restrict__ H,
+__global__ void pm_sr_kernel(const Members m, const PmHalo *__restrict__ H,
                              const int32_t *__restrict__ mhalo, const uint8_t *__restrict__ keep,
-                             const uint32_t *__restrict__ ckey, const uint32_t *__restrict__ cstart,
-                             const uint32_t *__restrict__ cmem, int64_t M, double a_val, double app,
-                             R *__restrict__ phi_c2) {
+                             const uint8_t *__restrict__ pr, const uint32_t *__restrict__ ckey,
+                             const uint32_t *__restrict__ cstart, const uint32_t *__restrict__ cmem,
+                             int64_t M, double a_val, double app, R *__restrict__ phi_sr) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
        k += (int64_t)gridDim.x * blockDim.x) {
     const int h = mhalo[k];
@@ -418,34 +427,39 @@ __global__ void pm_c2_kernel(const Members m, const PmHalo *__restrict__ H,
     const PmHalo &p = H[h];
     if (!p.pending) continue;
     const double sp = (double)p.spacing;
-    const R ht = (R)((double)(float)app / sp);
-    const R hs = (R)3.5;
-    const R r2cut = (R)(12.25 * sp * sp);
-    const R inv_sp = (R)(1.0 / sp);
-    const R pref = (R)(a_val / (6.0 * kPi * sp));
+    const int ri = pr[k];
+    const R ai = (R)(3.5 * sp / (double)ri);
+    const R a2 = ai * ai;
+    const R eps = (R)(double)(float)app;
+    const R fac = (R)(a_val / (6.0 * kPi));
+    int kk = (int)ceil((3.5 / (double)ri) / p.cw_u - 1e-9);
+    kk = kk < 1 ? 1 : (kk > 4 ? 4 : kk);
     const int64_t local = (int64_t)ckey[k] - p.cell_off;
     const int64_t n0 = p.nc[0], n1 = p.nc[1], n2 = p.nc[2];
     const int64_t cx = local % n0, cy = (local / n0) % n1, cz = local / (n0 * n1);
     const float xi = m.q[0][k], yi = m.q[1][k], zi = m.q[2][k];
     R acc = 0, comp = 0;
-    for (int64_t z = cz - 1; z <= cz + 1; ++z) {
+    for (int64_t z = cz - kk; z <= cz + kk; ++z) {
       if (z < 0 || z >= n2) continue;
-      for (int64_t y = cy - 1; y <= cy + 1; ++y) {
+      for (int64_t y = cy - kk; y <= cy + kk; ++y) {
         if (y < 0 || y >= n1) continue;
-        for (int64_t x = cx - 1; x <= cx + 1; ++x) {
+        for (int64_t x = cx - kk; x <= cx + kk; ++x) {
           if (x < 0 || x >= n0) continue;
           const int64_t c = p.cell_off + x + n0 * (y + n1 * z);
           for (uint32_t e = cstart[c]; e < cstart[c + 1]; ++e) {
             const int64_t j = cmem[e];
             if (j == k || !keep[j]) continue;
-            const R dx = (R)__fsub_rn(m.q[0][j], xi);
-            const R dy = (R)__fsub_rn(m.q[1][j], yi);
-            const R dz = (R)__fsub_rn(m.q[2][j], zi);
+            R dx, dy, dz;
+            if (p.two_level) {
+              dx = (R)m.q[0][j] - (R)xi; dy = (R)m.q[1][j] - (R)yi; dz = (R)m.q[2][j] - (R)zi;
+            } else {
+              dx = (R)__fsub_rn(m.q[0][j], xi); dy = (R)__fsub_rn(m.q[1][j], yi);
+              dz = (R)__fsub_rn(m.q[2][j], zi);
+            }
             const R r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 < r2cut) {
-              const R r = sqrt(r2) * inv_sp;
-              const R dphi = -pref * c2_delta<R>(r, ht, hs);
-              // compensated accumulation
+            if (r2 < a2) {
+              const R d = sqrt(r2);
+              const R dphi = -(fac * (depth_c<R>(d, eps) - depth_c<R>(d, ai)));
               const R yv = (R)m.w[j] * dphi - comp;
               const R t = acc + yv;
               comp = (t - acc) - yv;
@@ -455,7 +469,217 @@ __global__ void pm_c2_kernel(const Members m, const PmHalo *__restrict__ H,
         }
       }
     }
-    phi_c2[k] = acc;
+    phi_sr[k] = acc;
+  }
+}
+
+// ---------------------------------------------------------------- two-level
+
+// One refined region: halo h, region b (8x8x8 regions of 16 grid cells),
+// ratio r, inner grid n_in (bound_two_level_build_halo, :614-823).
+struct TlRegion {
+  int32_t h, b, r, n_in;
+  float lo[3], hi[3];  // region bounds (grid units)
+  float bo;            // source margin 3.5 + 3/r
+  float u0[3];         // inner grid origin
+};
+
+__device__ __forceinline__ void tl_t(const Members &m, const PmHalo &p, int64_t k, float *t) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    t[d] = (float)(((double)m.q[d][k] - (double)p.origin[d]) / (double)p.spacing);
+}
+
+__device__ __forceinline__ int tl_region(const float *t, int *bxyz) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int c = (int)floor((double)t[d]) / 16;
+    bxyz[d] = c < 0 ? 0 : (c > 7 ? 7 : c);
+  }
+  return bxyz[0] + 8 * bxyz[1] + 64 * bxyz[2];
+}
+
+// fine-grid TSC of a coordinate relative to region R; false if the nodes
+// leave the first half of the inner grid
+__device__ __forceinline__ bool tl_tsc(const TlRegion &R, const float *t, int *f, float *w9) {
+  bool ok = true;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float tf = __fmul_rn(__fsub_rn(t[d], R.u0[d]), (float)R.r);
+    const int nearest = (int)lroundf(tf);
+    const float dl = __fsub_rn(tf, (float)nearest);
+    const float a = __fsub_rn(0.5f, dl), b = __fadd_rn(0.5f, dl);
+    w9[3 * d + 0] = __fmul_rn(0.5f, __fmul_rn(a, a));
+    w9[3 * d + 1] = __fsub_rn(0.75f, __fmul_rn(dl, dl));
+    w9[3 * d + 2] = __fmul_rn(0.5f, __fmul_rn(b, b));
+    f[d] = nearest;
+    if (nearest < 1 || nearest + 2 > R.n_in / 2) ok = false;
+  }
+  return ok;
+}
+
+__global__ void tl_particle_kernel(const Members m, const PmHalo *__restrict__ H,
+                                   const int32_t *__restrict__ mhalo, int64_t M,
+                                   const uint8_t *__restrict__ region_r,
+                                   const int32_t *__restrict__ act_of, uint8_t *__restrict__ pr,
+                                   int32_t *__restrict__ preg) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int h = mhalo[k];
+    if (h < 0) continue;
+    const PmHalo &p = H[h];
+    if (!p.two_level) { pr[k] = 1; preg[k] = -1; continue; }
+    float t[3];
+    int bx[3];
+    tl_t(m, p, k, t);
+    const int b = tl_region(t, bx);
+    pr[k] = region_r[(int64_t)h * 512 + b];
+    preg[k] = act_of[(int64_t)h * 512 + b];
+  }
+}
+
+// Sources of every refined region: members inside the region box widened
+// by 3.5 + 3/r grid cells (:685-745).  pass 0 counts, pass 1 fills.
+__global__ void tl_source_kernel(const Members m, const PmHalo *__restrict__ H,
+                                 const int32_t *__restrict__ mhalo, int64_t M,
+                                 const int32_t *__restrict__ act_of, const TlRegion *__restrict__ A,
+                                 uint32_t *__restrict__ cnt, uint32_t *__restrict__ src, int fill) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int h = mhalo[k];
+    if (h < 0 || !H[h].two_level) continue;
+    float t[3];
+    int bx[3];
+    tl_t(m, H[h], k, t);
+    tl_region(t, bx);
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int x = bx[0] + dx, y = bx[1] + dy, z = bx[2] + dz;
+          if (x < 0 || x > 7 || y < 0 || y > 7 || z < 0 || z > 7) continue;
+          const int a = act_of[(int64_t)h * 512 + x + 8 * y + 64 * z];
+          if (a < 0) continue;
+          const TlRegion &R = A[a];
+          bool in = true;
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            in = in && t[d] >= __fsub_rn(R.lo[d], R.bo) && t[d] <= __fadd_rn(R.hi[d], R.bo);
+          if (!in) continue;
+          const uint32_t pos = atomicAdd(&cnt[a], 1u);
+          if (fill) src[pos] = (uint32_t)k;
+        }
+  }
+}
+
+// Targets of every refined region: its own members (pass 0 counts, 1 fills)
+__global__ void tl_target_kernel(const int32_t *__restrict__ preg, int64_t M,
+                                 uint32_t *__restrict__ cnt, uint32_t *__restrict__ tgt, int fill) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int a = preg[k];
+    if (a < 0) continue;
+    const uint32_t pos = atomicAdd(&cnt[a], 1u);
+    if (fill) tgt[pos] = (uint32_t)k;
+  }
+}
+
+// Node range checks of sources and targets, and the inner self term of
+// every target (:729-800).
+template <typename R>
+__global__ void tl_setup_kernel(const Members m, const PmHalo *__restrict__ H,
+                                const TlRegion *__restrict__ A, int na,
+                                const uint32_t *__restrict__ src_start, const uint32_t *__restrict__ src,
+                                const uint32_t *__restrict__ tgt_start, const uint32_t *__restrict__ tgt,
+                                const R *__restrict__ self2, const R *__restrict__ self4,
+                                R *__restrict__ self_in, int32_t *flags) {
+  const int a = blockIdx.x;
+  if (a >= na) return;
+  const TlRegion &Rg = A[a];
+  const PmHalo &p = H[Rg.h];
+  for (uint32_t e = src_start[a] + threadIdx.x; e < src_start[a + 1]; e += blockDim.x) {
+    float t[3], w9[9];
+    int f[3];
+    tl_t(m, p, src[e], t);
+    if (!tl_tsc(Rg, t, f, w9)) atomicCAS(&flags[FLAG_ERR], 0, kInvalid);
+  }
+  const R *sp = Rg.r == 2 ? self2 : self4;
+  for (uint32_t e = tgt_start[a] + threadIdx.x; e < tgt_start[a + 1]; e += blockDim.x) {
+    const int64_t k = tgt[e];
+    float t[3], w9[9];
+    int f[3];
+    tl_t(m, p, k, t);
+    if (!tl_tsc(Rg, t, f, w9)) { atomicCAS(&flags[FLAG_ERR], 0, kInvalid); continue; }
+    double acc = 0.0;
+    for (int sz = 0; sz < 3; ++sz)
+      for (int sy = 0; sy < 3; ++sy)
+        for (int sx = 0; sx < 3; ++sx) {
+          const float sw = __fmul_rn(__fmul_rn(w9[sx], w9[3 + sy]), w9[6 + sz]);
+          for (int tz = 0; tz < 3; ++tz)
+            for (int ty = 0; ty < 3; ++ty)
+              for (int tx = 0; tx < 3; ++tx) {
+                const float tw = __fmul_rn(__fmul_rn(w9[tx], w9[3 + ty]), w9[6 + tz]);
+                acc += (double)__fmul_rn(sw, tw) *
+                       (double)sp[((tz - sz + 2) * 5 + (ty - sy + 2)) * 5 + (tx - sx + 2)];
+              }
+        }
+    self_in[k] = (R)acc;
+  }
+}
+
+// Inner PM of a batch of refined regions of one inner grid size
+// (bound_two_level_run_pm, :825-942): deposit of the kept sources ...
+template <typename R>
+__global__ void tl_deposit_kernel(const Members m, const PmHalo *__restrict__ H,
+                                  const TlRegion *__restrict__ A, const int32_t *__restrict__ batch,
+                                  const uint32_t *__restrict__ src_start, const uint32_t *__restrict__ src,
+                                  const uint8_t *__restrict__ keep, int sup, R *__restrict__ rho) {
+  const int a = batch[blockIdx.x];
+  const TlRegion &Rg = A[a];
+  const PmHalo &p = H[Rg.h];
+  R *g = rho + (int64_t)blockIdx.x * sup * sup * sup;
+  for (uint32_t e = src_start[a] + threadIdx.x; e < src_start[a + 1]; e += blockDim.x) {
+    const int64_t k = src[e];
+    if (!keep[k]) continue;
+    float t[3], w9[9];
+    int f[3];
+    tl_t(m, p, k, t);
+    tl_tsc(Rg, t, f, w9);
+    const float wk = m.w[k];
+    for (int sz = 0; sz < 3; ++sz)
+      for (int sy = 0; sy < 3; ++sy)
+        for (int sx = 0; sx < 3; ++sx) {
+          const R v = (R)__fmul_rn(__fmul_rn(__fmul_rn(wk, w9[sx]), w9[3 + sy]), w9[6 + sz]);
+          atomicAdd(&g[((int64_t)(f[2] + sz - 1) * sup + (f[1] + sy - 1)) * sup + (f[0] + sx - 1)], v);
+        }
+  }
+}
+
+// ... and gather at the kept targets: phi_in = a r/(6 pi sp) (raw - w self_in)
+template <typename R>
+__global__ void tl_gather_kernel(const Members m, const PmHalo *__restrict__ H,
+                                 const TlRegion *__restrict__ A, const int32_t *__restrict__ batch,
+                                 const uint32_t *__restrict__ tgt_start, const uint32_t *__restrict__ tgt,
+                                 const uint8_t *__restrict__ keep, const R *__restrict__ self_in, int sup,
+                                 const R *__restrict__ rho, double a_val, R *__restrict__ phi_in) {
+  const int a = batch[blockIdx.x];
+  const TlRegion &Rg = A[a];
+  const PmHalo &p = H[Rg.h];
+  const R *g = rho + (int64_t)blockIdx.x * sup * sup * sup;
+  const R pref = (R)(a_val * (double)Rg.r / (6.0 * kPi * (double)p.spacing));
+  for (uint32_t e = tgt_start[a] + threadIdx.x; e < tgt_start[a + 1]; e += blockDim.x) {
+    const int64_t k = tgt[e];
+    if (!keep[k]) continue;
+    float t[3], w9[9];
+    int f[3];
+    tl_t(m, p, k, t);
+    tl_tsc(Rg, t, f, w9);
+    R raw = 0;
+    for (int sz = 0; sz < 3; ++sz)
+      for (int sy = 0; sy < 3; ++sy)
+        for (int sx = 0; sx < 3; ++sx)
+          raw += g[((int64_t)(f[2] + sz - 1) * sup + (f[1] + sy - 1)) * sup + (f[0] + sx - 1)] *
+                 (R)w9[sx] * (R)w9[3 + sy] * (R)w9[6 + sz];
+    phi_in[k] = pref * (raw - (R)m.w[k] * self_in[k]);
   }
 }
 
@@ -491,6 +715,7 @@ __global__ void __launch_bounds__(IBLK) pm_inner_kernel(const Members m, PmHalo 
                                                         const int32_t *__restrict__ list, int nlist,
                                                         uint8_t *__restrict__ keep,
                                                         const R *__restrict__ phi_c1,
+                                                        const R *__restrict__ phi_in,
                                                         const R *__restrict__ phi_c2,
                                                         float *__restrict__ phi,
                                                         float *__restrict__ en, float b_val, int nmin,
@@ -509,7 +734,7 @@ __global__ void __launch_bounds__(IBLK) pm_inner_kernel(const Members m, PmHalo 
   for (int64_t i = threadIdx.x; i < np; i += IBLK) {
     const int64_t k = b0 + i;
     if (!keep[k]) continue;
-    float v = (float)(phi_c1[k] + phi_c2[k]);
+    float v = (float)((phi_c1[k] + phi_in[k]) + phi_c2[k]);
     if (np_bound == 1 || n_source == 1) v = 0.0f;
     if (!isfinite(v)) s_err = kNonFinite;
     phi[k] = v;
@@ -741,6 +966,7 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
   float *wt = W.carve<float>(9 * (size_t)M);
   R *selfv = W.carve<R>(M), *c1 = W.carve<R>(M), *c2 = W.carve<R>(M);
   float *phi = W.carve<float>(M), *en = W.carve<float>(M);
+  R *tl_self_in = nullptr;
   double *ext = W.carve<double>(6 * (size_t)nh);
   if (!dH || !dlist || !dselfs || !mhalo || !first || !wt || !selfv || !c1 || !c2 || !phi || !en || !ext) {
     set_error("workspace exhausted (PM members)");
@@ -762,9 +988,11 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
   for (int h = 0; h < nh; ++h) {
     PYFOF_CUDA(cudaMemsetAsync(keep + H[h].off, 1, (size_t)H[h].np, s));
   }
-  // dense 16-cell regions of 256-grid halos would switch the reference to
-  // its two-level inner refinement, which this solver does not implement:
-  // refuse such input instead of returning a different answer
+  // two-level refinement of dense 16-cell regions of 256-grid halos
+  // (bound_two_level_setup_ratios / build_halo, bound_fortran.f90:551-823)
+  std::vector<TlRegion> act;
+  std::vector<int32_t> act_of((size_t)nh * 512, -1);
+  std::vector<uint8_t> region_r((size_t)nh * 512, 1);
   {
     uint32_t *rc = W.carve<uint32_t>((size_t)nh * 512);
     if (!rc) { set_error("workspace exhausted (regions)"); return kAlloc; }
@@ -774,16 +1002,43 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
     std::vector<uint32_t> hrc((size_t)nh * 512);
     PYFOF_CUDA(cudaMemcpyAsync(hrc.data(), rc, sizeof(uint32_t) * nh * 512, cudaMemcpyDeviceToHost, s));
     PYFOF_CUDA(cudaStreamSynchronize(s));
+    const double app_f = (double)(float)a.softening;
     for (int h = 0; h < nh; ++h) {
       if (H[h].n != 256) continue;
-      const bool r2ok = 3.5 * ((double)H[h].spacing / 2.0) >= (double)(float)a.softening;
-      for (int b = 0; b < 512 && r2ok; ++b)
-        if (hrc[(size_t)h * 512 + b] >= 3926u) {
-          set_error("candidate with %d members needs the two-level inner refinement, which is "
-                    "not implemented", H[h].np);
-          return kInvalid;
+      const double sp = (double)H[h].spacing;
+      int rmax = 1;
+      for (int b = 0; b < 512; ++b) {
+        const uint32_t c = hrc[(size_t)h * 512 + b];
+        int r = c < 3926u ? 1 : (c < 14688u ? 2 : 4);
+        if (r == 4 && 3.5 * (sp / 4.0) < app_f) r = 2;
+        if (r == 2 && 3.5 * (sp / 2.0) < app_f) r = 1;
+        region_r[(size_t)h * 512 + b] = (uint8_t)r;
+        if (c > 0 && r > rmax) rmax = r;
+      }
+      if (rmax == 1) continue;
+      H[h].two_level = 1;
+      H[h].r_max = rmax;
+      for (int b = 0; b < 512; ++b) {
+        const uint32_t c = hrc[(size_t)h * 512 + b];
+        const int r = region_r[(size_t)h * 512 + b];
+        if (c == 0 || r == 1) continue;
+        TlRegion Rg;
+        Rg.h = h;
+        Rg.b = b;
+        Rg.r = r;
+        Rg.n_in = r == 2 ? 128 : 216;
+        const int bb[3] = {b % 8, (b / 8) % 8, b / 64};
+        Rg.bo = 3.5f + 3.0f / (float)r;
+        for (int d = 0; d < 3; ++d) {
+          Rg.lo[d] = (float)(bb[d] * 16);
+          Rg.hi[d] = std::min(Rg.lo[d] + 16.0f, 127.0f);
+          Rg.u0[d] = ((Rg.lo[d] - Rg.bo) - (1.0f / (float)r)) + (0.0f / (float)r);
         }
+        act_of[(size_t)h * 512 + b] = (int32_t)act.size();
+        act.push_back(Rg);
+      }
     }
+    ctx.last_tl_regions = (int64_t)act.size();
   }
   // C2 cells (3.5 grid cells)
   pm_extent_kernel<<<nh, BLK, 0, s>>>(m, dH, nh, ext);
@@ -795,11 +1050,12 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
   for (int h = 0; h < nh; ++h) {
     PmHalo &p = H[h];
     p.cell_off = ncell;
+    p.cw_u = p.two_level ? 3.5 / (double)p.r_max : 3.5;
     int64_t c = 1;
     for (int d = 0; d < 3; ++d) {
       p.u_min[d] = hext[6 * h + d];
       const double span = hext[6 * h + 3 + d] - hext[6 * h + d];
-      p.nc[d] = std::max(1, (int)std::floor(span / 3.5) + 1);
+      p.nc[d] = std::max(1, (int)std::floor(span / p.cw_u) + 1);
       c *= p.nc[d];
     }
     ncell += c;
@@ -819,6 +1075,74 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
   PYFOF_TRY(exclusive_scan_u32(cstart, cstart, ncell + 1, nullptr, W, s));
   uint32_t *sk, *cmem;
   PYFOF_TRY(radix_sort_pairs(ckey, nullptr, M, bits_for((uint64_t)ncell), ka, va, kb, vb, &sk, &cmem, W, s));
+  // per-member refinement ratio, refined-region sources and targets
+  const int na = (int)act.size();
+  uint8_t *pr = W.carve<uint8_t>(M);
+  int32_t *preg = W.carve<int32_t>(M);
+  R *phi_in = W.carve<R>(M);
+  if (!pr || !preg || !phi_in) { set_error("workspace exhausted (two-level)"); return kAlloc; }
+  PYFOF_CUDA(cudaMemsetAsync(phi_in, 0, sizeof(R) * M, s));
+  PYFOF_CUDA(cudaMemsetAsync(pr, 1, M, s));
+  PYFOF_CUDA(cudaMemsetAsync(preg, 0xff, sizeof(int32_t) * M, s));  // -1: no refined region
+  TlRegion *dA = nullptr;
+  uint32_t *src_start = nullptr, *src = nullptr, *tgt_start = nullptr, *tgt = nullptr;
+  std::vector<uint32_t> hsrc, htgt;
+  std::shared_ptr<GreenTable> g_r2, g_r4;
+  {
+    uint8_t *dregr = W.carve<uint8_t>((size_t)nh * 512);
+    int32_t *dact_of = W.carve<int32_t>((size_t)nh * 512);
+    if (!dregr || !dact_of) { set_error("workspace exhausted (two-level)"); return kAlloc; }
+    PYFOF_CUDA(cudaMemcpyAsync(dregr, region_r.data(), (size_t)nh * 512, cudaMemcpyHostToDevice, s));
+    PYFOF_CUDA(cudaMemcpyAsync(dact_of, act_of.data(), sizeof(int32_t) * nh * 512, cudaMemcpyHostToDevice, s));
+    tl_particle_kernel<<<gM, BLK, 0, s>>>(m, dH, mhalo, M, dregr, dact_of, pr, preg);
+    PYFOF_CHECK_LAUNCH();
+    if (na > 0) {
+      dA = W.carve<TlRegion>(na);
+      uint32_t *cnt = W.carve<uint32_t>(na + 1);
+      src_start = W.carve<uint32_t>(na + 1);
+      tgt_start = W.carve<uint32_t>(na + 1);
+      if (!dA || !cnt || !src_start || !tgt_start) { set_error("workspace exhausted (two-level)"); return kAlloc; }
+      PYFOF_CUDA(cudaMemcpyAsync(dA, act.data(), sizeof(TlRegion) * na, cudaMemcpyHostToDevice, s));
+      // sources
+      PYFOF_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (na + 1), s));
+      tl_source_kernel<<<gM, BLK, 0, s>>>(m, dH, mhalo, M, dact_of, dA, cnt, nullptr, 0);
+      PYFOF_CHECK_LAUNCH();
+      PYFOF_TRY(exclusive_scan_u32(cnt, src_start, na + 1, nullptr, W, s));
+      hsrc.resize(na + 1);
+      PYFOF_CUDA(cudaMemcpyAsync(hsrc.data(), src_start, sizeof(uint32_t) * (na + 1), cudaMemcpyDeviceToHost, s));
+      PYFOF_CUDA(cudaStreamSynchronize(s));
+      src = W.carve<uint32_t>(std::max<uint32_t>(hsrc[na], 1));
+      if (!src) { set_error("workspace exhausted (two-level sources)"); return kAlloc; }
+      PYFOF_CUDA(cudaMemcpyAsync(cnt, src_start, sizeof(uint32_t) * (na + 1), cudaMemcpyDeviceToDevice, s));
+      tl_source_kernel<<<gM, BLK, 0, s>>>(m, dH, mhalo, M, dact_of, dA, cnt, src, 1);
+      PYFOF_CHECK_LAUNCH();
+      // targets
+      PYFOF_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (na + 1), s));
+      tl_target_kernel<<<gM, BLK, 0, s>>>(preg, M, cnt, nullptr, 0);
+      PYFOF_CHECK_LAUNCH();
+      PYFOF_TRY(exclusive_scan_u32(cnt, tgt_start, na + 1, nullptr, W, s));
+      htgt.resize(na + 1);
+      PYFOF_CUDA(cudaMemcpyAsync(htgt.data(), tgt_start, sizeof(uint32_t) * (na + 1), cudaMemcpyDeviceToHost, s));
+      PYFOF_CUDA(cudaStreamSynchronize(s));
+      tgt = W.carve<uint32_t>(std::max<uint32_t>(htgt[na], 1));
+      if (!tgt) { set_error("workspace exhausted (two-level targets)"); return kAlloc; }
+      PYFOF_CUDA(cudaMemcpyAsync(cnt, tgt_start, sizeof(uint32_t) * (na + 1), cudaMemcpyDeviceToDevice, s));
+      tl_target_kernel<<<gM, BLK, 0, s>>>(preg, M, cnt, tgt, 1);
+      PYFOF_CHECK_LAUNCH();
+      bool need2 = false, need4 = false;
+      for (auto &Rg : act) { need2 |= Rg.r == 2; need4 |= Rg.r == 4; }
+      if (need2) PYFOF_TRY(get_green<R>(ctx, 128, 3.5, 7.0, 0, &g_r2));
+      if (need4) PYFOF_TRY(get_green<R>(ctx, 216, 3.5, 14.0, 0, &g_r4));
+      R *self_in = c1;  // reuse: c1 is rewritten every pass, self_in must persist -> own array
+      self_in = W.carve<R>(M);
+      if (!self_in) { set_error("workspace exhausted (two-level self)"); return kAlloc; }
+      tl_setup_kernel<R><<<na, BLK, 0, s>>>(m, dH, dA, na, src_start, src, tgt_start, tgt,
+                                            g_r2 ? (const R *)g_r2->self : nullptr,
+                                            g_r4 ? (const R *)g_r4->self : nullptr, self_in, ctx.d_flags);
+      PYFOF_CHECK_LAUNCH();
+      tl_self_in = self_in;
+    }
+  }
   PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   PYFOF_CUDA(cudaStreamSynchronize(s));
   if (ctx.h_flags[FLAG_ERR]) {
@@ -866,9 +1190,38 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
         PYFOF_CHECK_LAUNCH();
       }
     }
-    pm_c2_kernel<R><<<gM, BLK, 0, s>>>(m, dH, mhalo, keep, ckey, cstart, cmem, M, a.a_val, a.softening, c2);
+    // refined regions of pending halos, batched per inner grid size
+    for (int r : {2, 4}) {
+      std::vector<int32_t> regs;
+      for (int ia = 0; ia < na; ++ia)
+        if (act[ia].r == r && H[act[ia].h].pending) regs.push_back(ia);
+      if (regs.empty()) continue;
+      const int nin = r == 2 ? 128 : 216;
+      const int sup = nin / 2 + 1;
+      const size_t per = sizeof(cplx_t<R>) * (size_t)(nin / 2 + 1) * nin * nin + sizeof(R) * (size_t)sup * sup * sup;
+      const int maxb = (int)std::max<size_t>(1, budget / per);
+      const R *gin = (const R *)(r == 2 ? g_r2 : g_r4)->g;
+      for (size_t g0 = 0; g0 < regs.size(); g0 += maxb) {
+        const int nb = (int)std::min<size_t>(maxb, regs.size() - g0);
+        int32_t *dbatch = W.carve<int32_t>(nb);
+        R *rho = W.carve<R>((size_t)nb * sup * sup * sup);
+        cplx_t<R> *spec = W.carve<cplx_t<R>>((size_t)nb * (nin / 2 + 1) * nin * nin);
+        if (!dbatch || !rho || !spec) { set_error("workspace exhausted (inner grids)"); return kAlloc; }
+        PYFOF_CUDA(cudaMemcpyAsync(dbatch, regs.data() + g0, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s));
+        const int64_t ng = (int64_t)nb * sup * sup * sup;
+        pm_zero_kernel<R><<<(unsigned)std::min<int64_t>(ceil_div(ng, BLK), 148 * 16), BLK, 0, s>>>(rho, ng);
+        PYFOF_CHECK_LAUNCH();
+        tl_deposit_kernel<R><<<nb, BLK, 0, s>>>(m, dH, dA, dbatch, src_start, src, keep, sup, rho);
+        PYFOF_CHECK_LAUNCH();
+        PYFOF_TRY(pm_convolve_batch<R>(rho, spec, gin, nin, sup, nb, s));
+        tl_gather_kernel<R><<<nb, BLK, 0, s>>>(m, dH, dA, dbatch, tgt_start, tgt, keep, tl_self_in, sup, rho,
+                                               a.a_val, phi_in);
+        PYFOF_CHECK_LAUNCH();
+      }
+    }
+    pm_sr_kernel<R><<<gM, BLK, 0, s>>>(m, dH, mhalo, keep, pr, ckey, cstart, cmem, M, a.a_val, a.softening, c2);
     PYFOF_CHECK_LAUNCH();
-    pm_inner_kernel<R><<<(unsigned)pend.size(), IBLK, 0, s>>>(m, dH, dpend, (int)pend.size(), keep, c1, c2, phi,
+    pm_inner_kernel<R><<<(unsigned)pend.size(), IBLK, 0, s>>>(m, dH, dpend, (int)pend.size(), keep, c1, phi_in, c2, phi,
                                                            en, (float)a.b_val, a.np_halo_min, phi_only,
                                                            ctx.d_flags);
     PYFOF_CHECK_LAUNCH();

@@ -62,6 +62,8 @@ def test_first_pass_potential(n, a, rmax, expect_gid):
     phi64, g64 = _native.halo_potential(q, w, fp64=True, s15=S15)
     phi32, g32 = _native.halo_potential(q, w, fp64=False, s15=S15)
     assert g_o == g64 == g32 == expect_gid
+    if n == 30000:
+        assert _native.get_stat("refined_regions") > 0
     scale = np.abs(phi_o).max()
     err64 = np.abs(phi64 - phi_o).max() / scale
     err32 = np.abs(phi32 - phi64).max() / scale
@@ -101,7 +103,7 @@ def test_pm_unbinding_end_to_end(fp64):
     finally:
         _native.set_option("unbind_fp64", 0)
     o = oracle_core(xs, **kw)
-    assert _native.get_stat("pm_halos") >= 4
+    assert _native.get_stat("pm_halos") >= 3
     n_in = int(o[0].sum())
     mism = int((g[0] != o[0]).sum())
     assert n_in > 1000
