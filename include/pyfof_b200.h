@@ -82,6 +82,21 @@ int32_t pyfof_halo_potential(const float *q, const float *w, int32_t np, double 
                              double a_val, double s_15_val, int64_t ng_val, int32_t fp64,
                              float *phi, int32_t *method);
 
+/* Allocation-free variant of pyfof_halo_potential for direct-summation
+ * candidates (np <= 1000).  No counterpart in the reference: it exists for
+ * callers that must not allocate device memory while running, e.g. a host
+ * framework whose caching allocator already owns the device memory, or a
+ * latency-bound loop that cannot afford an allocation failing mid-step.
+ * All device scratch lives in a static array of the library (about 42 KiB
+ * per GPU, held until exit); inputs q (3,np), w (np) and the output phi (np)
+ * are host arrays as in pyfof_halo_potential; `stream` is a cudaStream_t
+ * (NULL = legacy default stream).  Returns 1 for np > 1000.  The first call
+ * on a device looks up the array's address (make it before any stream
+ * capture); calls share the array, so calls that overlap on the GPU race. */
+int32_t pyfof_halo_potential_direct_static(const float *q, const float *w, int32_t np,
+                                           double softening, double a_val, int32_t fp64,
+                                           float *phi, void *stream);
+
 /* Replaces fof_fortran.fof_fortran (fof_fortran.f90:10-58).
  *   xp, vp    (3,total_np) float64 in `layout`; vp may be NULL (all zero,
  *             the value _fof_core passes when vp_list is None,

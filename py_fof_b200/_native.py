@@ -33,7 +33,8 @@ _RUN_ARGS = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, 
 # every symbol include/pyfof_b200.h declares
 EXPORTED = ("pyfof_version", "pyfof_init", "pyfof_shutdown", "pyfof_last_error",
             "pyfof_set_option", "pyfof_set_stream", "pyfof_get_stat", "pyfof_last_link_ms",
-            "pyfof_halo_potential", "pyfof_run", "pyfof_run_device")
+            "pyfof_halo_potential", "pyfof_halo_potential_direct_static", "pyfof_run",
+            "pyfof_run_device")
 
 
 class NativeLibraryError(RuntimeError):
@@ -69,6 +70,10 @@ def load():
                                            ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                            ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p,
                                            ctypes.POINTER(ctypes.c_int32)]
+        L.pyfof_halo_potential_direct_static.restype = ctypes.c_int32
+        L.pyfof_halo_potential_direct_static.argtypes = [
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+            ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]
         L.pyfof_run.restype = ctypes.c_int32
         L.pyfof_run.argtypes = _RUN_ARGS
         L.pyfof_run_device.restype = ctypes.c_int32
@@ -163,6 +168,20 @@ def halo_potential(q, w, softening=0.1, a_val=1.0, s15=17.152, ng=256, fp64=Fals
     if ierr:
         raise RuntimeError(f"ierr={ierr}: {last_error()}")
     return phi, int(meth.value)
+
+
+def halo_potential_direct_static(q, w, softening=0.1, a_val=1.0, fp64=False, stream=0):
+    """Direct-summation potential (np <= 1000) computed without any device
+    allocation: scratch lives in the library's static device array.
+    Returns (phi float32, ierr)."""
+    q = np.ascontiguousarray(q, dtype=np.float32)
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    n = w.shape[0]
+    phi = np.zeros(n, np.float32)
+    ierr = load().pyfof_halo_potential_direct_static(
+        q.ctypes.data, w.ctypes.data, n, float(softening), float(a_val), int(bool(fp64)),
+        phi.ctypes.data, ctypes.c_void_p(stream) if stream else None)
+    return phi, int(ierr)
 
 
 def run_device(xp_ptr, vp_ptr, mp_ptr, layout, np_halo, nhalo, total_np, L_Box, link,

@@ -21,6 +21,7 @@
 #include "context.cuh"
 #include "primitives.cuh"
 #include "unbind.cuh"
+#include "unbind_direct.cuh"
 #include "unbind_internal.cuh"
 
 namespace pyfof {
@@ -113,307 +114,6 @@ __global__ void __launch_bounds__(BLK) ub_span_kernel(Members m, const int64_t *
 }
 
 // ---------------------------------------------------------------- direct
-
-// bound_depth_continuous (bound_fortran.f90:3080-3102): spline-softened 1/r.
-template <typename T>
-__device__ __forceinline__ T depth_continuous(T r, T h);
-
-template <>
-__device__ __forceinline__ double depth_continuous<double>(double r, double h) {
-  if (r <= 0.0) return __ddiv_rn(208.0, __dmul_rn(70.0, h));
-  if (r >= h) return __ddiv_rn(1.0, r);
-  const double e = __ddiv_rn(__dmul_rn(2.0, r), h);
-  if (e <= 1.0) {
-    double t = __dadd_rn(8.0, __dmul_rn(-3.0, e));
-    t = __dadd_rn(14.0, __dmul_rn(e, t));
-    t = __dadd_rn(-56.0, __dmul_rn(e, t));
-    t = __dadd_rn(112.0, __dmul_rn(__dmul_rn(e, e), t));
-    const double prim = __dmul_rn(__dmul_rn(e, e), t);
-    return __ddiv_rn(__dadd_rn(208.0, -prim), __dmul_rn(70.0, h));
-  }
-  double t = __dadd_rn(-8.0, e);
-  t = __dadd_rn(14.0, __dmul_rn(e, t));
-  t = __dadd_rn(56.0, __dmul_rn(e, t));
-  t = __dadd_rn(-280.0, __dmul_rn(e, t));
-  t = __dadd_rn(448.0, __dmul_rn(e, t));
-  double prim = __dmul_rn(__dmul_rn(e, e), t);
-  prim = __dadd_rn(prim, -__dmul_rn(224.0, e));
-  prim = __dadd_rn(prim, -__ddiv_rn(12.0, e));
-  return __ddiv_rn(__dadd_rn(128.0, -prim), __dmul_rn(70.0, h));
-}
-
-// FP32 product-path kernel: same piecewise polynomial, with the
-// reciprocals precomputed by the caller (inv70h = 1/(70h), inv_h = 1/h).
-__device__ __forceinline__ float depth_f32(float r2, float h, float inv_h, float inv70h) {
-  if (r2 >= h * h) return rsqrtf(r2);
-  const float r = sqrtf(r2);
-  const float e = 2.0f * r * inv_h;
-  if (e <= 1.0f) {
-    const float e2 = e * e;
-    const float prim = e2 * (112.0f + e2 * (-56.0f + e * (14.0f + e * (8.0f - 3.0f * e))));
-    return (208.0f - prim) * inv70h;
-  }
-  const float prim = e * e * (448.0f + e * (-280.0f + e * (56.0f + e * (14.0f + e * (-8.0f + e))))) -
-                     224.0f * e - 12.0f / e;
-  return (128.0f - prim) * inv70h;
-}
-
-// Compensated (Fast2Sum/Kahan) FP32 accumulator.
-struct Kahan {
-  float s = 0.f, c = 0.f;
-  __device__ __forceinline__ void add(float x) {
-    const float y = x - c;
-    const float t = s + y;
-    c = (t - s) - y;
-    s = t;
-  }
-};
-
-__device__ __forceinline__ double block_sum_d(double v, double *red) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  __syncthreads();
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  double t = 0.0;
-  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-  return t;
-}
-
-__device__ __forceinline__ int block_sum_i(int v, int *red) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  __syncthreads();
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  int t = 0;
-  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-  return t;
-}
-
-struct DirectParams {
-  double fac;     // a / (6 pi)
-  double app;     // softening (standard grid units)
-  float b;        // real(b_bound, 4)
-  int nmin;       // np_halo_min
-  int phi_only;   // stop after the first potential
-};
-
-// One block per halo: bound_check_grid for gid 0 (:2611-2864).  FP64=true
-// is the plain FP64 path, bit-exact with the reference arithmetic; FP64=false
-// the FP32 product path with compensated sums.
-template <bool FP64>
-__global__ void __launch_bounds__(BLK) ub_direct_kernel(Members m, const int64_t *__restrict__ off,
-                                                        const int32_t *__restrict__ list,
-                                                        DirectParams P, HaloResult *__restrict__ res,
-                                                        uint8_t *__restrict__ keep_out,
-                                                        float *__restrict__ phi_out,
-                                                        int32_t *flags) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int c = list[blockIdx.x];
-  const int64_t b0 = off[c];
-  const int np = (int)(off[c + 1] - b0);
-  float *qx = reinterpret_cast<float *>(smem);
-  float *qy = qx + kDirectMax, *qz = qy + kDirectMax;
-  float *vx = qz + kDirectMax, *vy = vx + kDirectMax, *vz = vy + kDirectMax;
-  float *w = vz + kDirectMax, *phi = w + kDirectMax, *en = phi + kDirectMax;
-  int *jdel = reinterpret_cast<int *>(en + kDirectMax);
-  int *unb = jdel + kDirectMax;
-  double *phid = reinterpret_cast<double *>(unb + kDirectMax);
-  unsigned char *keep = reinterpret_cast<unsigned char *>(phid + kDirectMax);
-  __shared__ double red_d[BLK / 32];
-  __shared__ int red_i[BLK / 32];
-  __shared__ double s_qc[3], s_vc[3];
-  __shared__ int s_nu, s_err;
-
-  for (int i = threadIdx.x; i < np; i += BLK) {
-    const int64_t k = b0 + i;
-    qx[i] = m.q[0][k]; qy[i] = m.q[1][k]; qz[i] = m.q[2][k];
-    vx[i] = m.v[0][k]; vy[i] = m.v[1][k]; vz[i] = m.v[2][k];
-    w[i] = m.w[k];
-    keep[i] = 1;
-    phid[i] = 0.0;
-  }
-  if (threadIdx.x == 0) s_err = 0;
-  __syncthreads();
-  const float h32 = (float)P.app, inv_h = (float)(1.0 / P.app), inv70h = (float)(1.0 / (70.0 * P.app));
-  const float fac32 = (float)P.fac;
-  int np_bound = np, njd = 0, status = 5;
-
-  for (int pass = 1; pass <= kMaxPasses; ++pass) {
-    int ks = 0;
-    for (int i = threadIdx.x; i < np; i += BLK) ks += keep[i];
-    const int n_source = block_sum_i(ks, red_i);
-    // potential: full sum on the first pass, later passes add back the
-    // sources removed since the previous refresh
-    for (int i = threadIdx.x; i < np; i += BLK) {
-      if (pass == 1) {
-        if (FP64) {
-          double acc = 0.0;
-          for (int j = 0; j < np; ++j) {
-            if (j == i) continue;
-            const double dx = (double)__fsub_rn(qx[j], qx[i]);
-            const double dy = (double)__fsub_rn(qy[j], qy[i]);
-            const double dz = (double)__fsub_rn(qz[j], qz[i]);
-            const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
-                                                  __dmul_rn(dz, dz)));
-            const double dd = __dmul_rn(P.fac, depth_continuous<double>(r, P.app));
-            acc = __dadd_rn(acc, -__dmul_rn((double)w[j], dd));
-          }
-          phid[i] = acc;
-        } else {
-          Kahan acc;
-          const float xi = qx[i], yi = qy[i], zi = qz[i];
-          for (int j = 0; j < np; ++j) {
-            if (j == i) continue;
-            const float dx = qx[j] - xi, dy = qy[j] - yi, dz = qz[j] - zi;
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            acc.add(-w[j] * depth_f32(r2, h32, inv_h, inv70h));
-          }
-          phid[i] = (double)(fac32 * acc.s);
-        }
-      } else if (keep[i]) {
-        if (FP64) {
-          double acc = phid[i];
-          for (int k = 0; k < njd; ++k) {
-            const int j = jdel[k];
-            const double dx = (double)__fsub_rn(qx[j], qx[i]);
-            const double dy = (double)__fsub_rn(qy[j], qy[i]);
-            const double dz = (double)__fsub_rn(qz[j], qz[i]);
-            const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
-                                                  __dmul_rn(dz, dz)));
-            acc = __dadd_rn(acc, __dmul_rn(__dmul_rn((double)w[j], P.fac),
-                                           depth_continuous<double>(r, P.app)));
-          }
-          phid[i] = acc;
-        } else {
-          Kahan acc;
-          const float xi = qx[i], yi = qy[i], zi = qz[i];
-          for (int k = 0; k < njd; ++k) {
-            const int j = jdel[k];
-            const float dx = qx[j] - xi, dy = qy[j] - yi, dz = qz[j] - zi;
-            acc.add(w[j] * depth_f32(dx * dx + dy * dy + dz * dz, h32, inv_h, inv70h));
-          }
-          phid[i] += (double)(fac32 * acc.s);
-        }
-      }
-    }
-    njd = 0;
-    __syncthreads();
-    for (int i = threadIdx.x; i < np; i += BLK) {
-      if (!keep[i]) continue;
-      float v = FP64 ? __double2float_rn(phid[i]) : (float)phid[i];
-      if (np_bound == 1 || n_source == 1) v = 0.0f;
-      if (!isfinite(v)) s_err = kNonFinite;
-      phi[i] = v;
-    }
-    __syncthreads();
-    if (s_err) break;
-    if (P.phi_only) { status = 0; break; }
-    int deleted = 0;
-    for (;;) {
-      // centre of mass and mean velocity of the kept set, FP64
-      if (FP64) {
-        if (threadIdx.x == 0) {
-          double ws = 0, q0 = 0, q1 = 0, q2 = 0, v0 = 0, v1 = 0, v2 = 0;
-          for (int i = 0; i < np; ++i) {
-            if (!keep[i]) continue;
-            const double wi = (double)w[i];
-            ws = __dadd_rn(ws, wi);
-            q0 = __dadd_rn(q0, __dmul_rn(wi, (double)qx[i]));
-            q1 = __dadd_rn(q1, __dmul_rn(wi, (double)qy[i]));
-            q2 = __dadd_rn(q2, __dmul_rn(wi, (double)qz[i]));
-            v0 = __dadd_rn(v0, __dmul_rn(wi, (double)vx[i]));
-            v1 = __dadd_rn(v1, __dmul_rn(wi, (double)vy[i]));
-            v2 = __dadd_rn(v2, __dmul_rn(wi, (double)vz[i]));
-          }
-          s_qc[0] = __ddiv_rn(q0, ws); s_qc[1] = __ddiv_rn(q1, ws); s_qc[2] = __ddiv_rn(q2, ws);
-          s_vc[0] = __ddiv_rn(v0, ws); s_vc[1] = __ddiv_rn(v1, ws); s_vc[2] = __ddiv_rn(v2, ws);
-        }
-      } else {
-        double a[7] = {0, 0, 0, 0, 0, 0, 0};
-        for (int i = threadIdx.x; i < np; i += BLK) {
-          if (!keep[i]) continue;
-          const double wi = (double)w[i];
-          a[0] += wi;
-          a[1] += wi * qx[i]; a[2] += wi * qy[i]; a[3] += wi * qz[i];
-          a[4] += wi * vx[i]; a[5] += wi * vy[i]; a[6] += wi * vz[i];
-        }
-        for (int k = 0; k < 7; ++k) a[k] = block_sum_d(a[k], red_d);
-        if (threadIdx.x == 0) {
-          for (int d = 0; d < 3; ++d) { s_qc[d] = a[1 + d] / a[0]; s_vc[d] = a[4 + d] / a[0]; }
-        }
-      }
-      if (threadIdx.x == 0) s_nu = 0;
-      __syncthreads();
-      const float qc0 = __double2float_rn(s_qc[0]), qc1 = __double2float_rn(s_qc[1]),
-                  qc2 = __double2float_rn(s_qc[2]);
-      const float vc0 = __double2float_rn(s_vc[0]), vc1 = __double2float_rn(s_vc[1]),
-                  vc2 = __double2float_rn(s_vc[2]);
-      // specific energies (bound_fortran.f90:2773-2786), FP32
-      for (int i = threadIdx.x; i < np; i += BLK) {
-        if (!keep[i]) continue;
-        const float d0 = __fadd_rn(__fsub_rn(vx[i], vc0), __fmul_rn(P.b, __fsub_rn(qx[i], qc0)));
-        const float d1 = __fadd_rn(__fsub_rn(vy[i], vc1), __fmul_rn(P.b, __fsub_rn(qy[i], qc1)));
-        const float d2 = __fadd_rn(__fsub_rn(vz[i], vc2), __fmul_rn(P.b, __fsub_rn(qz[i], qc2)));
-        float s = __fmul_rn(d0, d0);
-        s = __fadd_rn(s, __fmul_rn(d1, d1));
-        s = __fadd_rn(s, __fmul_rn(d2, d2));
-        const float e = __fadd_rn(__fdiv_rn(s, 2.0f), phi[i]);
-        if (!isfinite(e)) s_err = kInvalid;
-        en[i] = e;
-        if (e >= 0.0f) unb[atomicAdd(&s_nu, 1)] = i;
-      }
-      __syncthreads();
-      if (s_err) break;
-      const int nu = s_nu;
-      if (nu == 0) {
-        if (deleted == 0) { status = 0; break; }
-        break;
-      }
-      // delete the nb highest energies; ties go to the lower local index
-      // first (bound_fortran.f90:2808-2844)
-      int nb = (int)ceil(0.02 * (double)np_bound);
-      nb = max(1, nb);
-      nb = min(nu, nb);
-      for (int t = threadIdx.x; t < nu; t += BLK) {
-        const int i = unb[t];
-        const float ei = en[i];
-        int rank = 0;
-        for (int u = 0; u < nu; ++u) {
-          const int j = unb[u];
-          const float ej = en[j];
-          rank += (ej > ei) || (ej == ei && j < i);
-        }
-        if (rank < nb) {
-          keep[i] = 0;
-          jdel[njd + rank] = i;
-        }
-      }
-      __syncthreads();
-      njd += nb;
-      np_bound -= nb;
-      deleted += nb;
-      if (np_bound < P.nmin) { status = 1; break; }
-      if ((double)deleted >= 0.2 * (double)np_bound) break;
-    }
-    __syncthreads();
-    if (s_err || status != 5) break;
-    if (pass == kMaxPasses) break;
-  }
-  if (s_err) {
-    if (threadIdx.x == 0) atomicCAS(&flags[FLAG_ERR], 0, s_err);
-    return;
-  }
-  for (int i = threadIdx.x; i < np; i += BLK) {
-    keep_out[b0 + i] = keep[i];
-    if (phi_out) phi_out[b0 + i] = phi[i];
-  }
-  if (threadIdx.x == 0) {
-    res[c].status = status;
-    res[c].np_bound = np_bound;
-  }
-}
 
 // Valid halos (status 0 and np_bound >= np_halo_min) in candidate order.
 __global__ void ub_valid_kernel(const HaloResult *__restrict__ res, int ncand, int nmin,
@@ -688,7 +388,7 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
     if (!dl) { set_error("workspace exhausted (direct list)"); return kAlloc; }
     PYFOF_CUDA(cudaMemcpyAsync(dl, direct.data(), sizeof(int32_t) * direct.size(),
                                cudaMemcpyHostToDevice, s));
-    DirectParams P;
+    direct::DirectParams P;
     P.fac = a.a_val / (6.0 * kPi);
     P.app = a.softening;
     P.b = (float)a.b_val;
@@ -696,14 +396,14 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
     P.phi_only = 0;
     const size_t smem = kDirectSmem;
     if (a.bound_fp64) {
-      PYFOF_CUDA(cudaFuncSetAttribute(ub_direct_kernel<true>,
+      PYFOF_CUDA(cudaFuncSetAttribute(direct::ub_direct_kernel<true>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      ub_direct_kernel<true><<<(unsigned)direct.size(), BLK, smem, s>>>(m, off, dl, P, res, keep,
+      direct::ub_direct_kernel<true><<<(unsigned)direct.size(), BLK, smem, s>>>(m, off, dl, P, res, keep,
                                                                          st.phi_out, ctx.d_flags);
     } else {
-      PYFOF_CUDA(cudaFuncSetAttribute(ub_direct_kernel<false>,
+      PYFOF_CUDA(cudaFuncSetAttribute(direct::ub_direct_kernel<false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      ub_direct_kernel<false><<<(unsigned)direct.size(), BLK, smem, s>>>(m, off, dl, P, res, keep,
+      direct::ub_direct_kernel<false><<<(unsigned)direct.size(), BLK, smem, s>>>(m, off, dl, P, res, keep,
                                                                           st.phi_out, ctx.d_flags);
     }
     PYFOF_CHECK_LAUNCH();
@@ -818,20 +518,20 @@ int32_t unbind_potential(Context &ctx, const float *q_soa, const float *w, int32
   if (g == 0) {
     const int32_t zero = 0;
     PYFOF_CUDA(cudaMemcpyAsync(dl, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, s));
-    DirectParams P;
+    direct::DirectParams P;
     P.fac = a_val / (6.0 * kPi);
     P.app = softening;
     P.b = 0.0f;
     P.nmin = 1;
     P.phi_only = 1;
     if (fp64) {
-      PYFOF_CUDA(cudaFuncSetAttribute(ub_direct_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      PYFOF_CUDA(cudaFuncSetAttribute(direct::ub_direct_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kDirectSmem));
-      ub_direct_kernel<true><<<1, BLK, kDirectSmem, s>>>(m, off, dl, P, res, keep, phid, ctx.d_flags);
+      direct::ub_direct_kernel<true><<<1, BLK, kDirectSmem, s>>>(m, off, dl, P, res, keep, phid, ctx.d_flags);
     } else {
-      PYFOF_CUDA(cudaFuncSetAttribute(ub_direct_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      PYFOF_CUDA(cudaFuncSetAttribute(direct::ub_direct_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kDirectSmem));
-      ub_direct_kernel<false><<<1, BLK, kDirectSmem, s>>>(m, off, dl, P, res, keep, phid, ctx.d_flags);
+      direct::ub_direct_kernel<false><<<1, BLK, kDirectSmem, s>>>(m, off, dl, P, res, keep, phid, ctx.d_flags);
     }
     PYFOF_CHECK_LAUNCH();
   } else {
