@@ -50,8 +50,9 @@ int32_t pyfof_shutdown(void);
  * truncated to len) and returns its full length. */
 int32_t pyfof_last_error(char *buf, int64_t len);
 
-/* Library options: "unbind_fp64" (1 = plain FP64 unbinding path, 0 = FP32
- * product path), "timing" (1 = record stage times). */
+/* Library options: "unbind_fp64" (1 = FP64 unbinding, batched; 0 = FP32
+ * product path), "unbind_per_halo" (1 = the plain FP64 baseline: one halo per
+ * launch sequence), "timing" (1 = record stage times). */
 int32_t pyfof_set_option(const char *key, int64_t value);
 
 /* Issue all later work of the selected device on `stream` (a cudaStream_t;

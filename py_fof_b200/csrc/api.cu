@@ -19,6 +19,7 @@ std::mutex g_ctx_mu;
 Context *g_ctx[64] = {};
 int g_default_device = 0;
 int g_bound_fp64 = 0;
+int g_bound_per_halo = 0;
 int g_timing = 0;
 }  // namespace
 
@@ -120,6 +121,7 @@ static int32_t validate(int32_t nhalo, int64_t total_np, const int32_t *np_halo,
 static int32_t run_common(Context &ctx, FofArgs &a) {
   ctx.timing = g_timing != 0;
   a.bound_fp64 = g_bound_fp64;
+  a.bound_per_halo = g_bound_per_halo;
   int32_t r = fof_run(ctx, a);
   cudaError_t e = cudaStreamSynchronize(ctx.stream);
   if (r == kOk && e != cudaSuccess) {
@@ -162,6 +164,7 @@ int32_t pyfof_last_error(char *buf, int64_t len) {
 int32_t pyfof_set_option(const char *key, int64_t value) {
   if (!key) return kInvalid;
   if (!std::strcmp(key, "unbind_fp64")) { g_bound_fp64 = value != 0; return kOk; }
+  if (!std::strcmp(key, "unbind_per_halo")) { g_bound_per_halo = value != 0; return kOk; }
   if (!std::strcmp(key, "timing")) { g_timing = value != 0; return kOk; }
   set_error("unknown option %s", key);
   return kInvalid;
@@ -285,6 +288,7 @@ int32_t pyfof_run(const double *xp, const double *vp, const double *mp, int32_t 
   a.ang_mom = ang_mom;
   ctx.timing = g_timing != 0;
   a.bound_fp64 = g_bound_fp64;
+  a.bound_per_halo = g_bound_per_halo;
   r = fof_run(ctx, a);
   if (r == kOk) {
     cudaMemcpyAsync(in_halo, a.in_halo, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);

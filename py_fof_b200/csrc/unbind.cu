@@ -395,7 +395,17 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
     P.nmin = a.np_halo_min;
     P.phi_only = 0;
     const size_t smem = kDirectSmem;
-    if (a.bound_fp64) {
+    if (a.bound_per_halo) {
+      // plain baseline: one halo per launch, waited for before the next
+      PYFOF_CUDA(cudaFuncSetAttribute(direct::ub_direct_kernel<true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      for (size_t i = 0; i < direct.size(); ++i) {
+        direct::ub_direct_kernel<true><<<1, BLK, smem, s>>>(m, off, dl + i, P, res, keep, st.phi_out,
+                                                            ctx.d_flags);
+        PYFOF_CHECK_LAUNCH();
+        PYFOF_CUDA(cudaStreamSynchronize(s));
+      }
+    } else if (a.bound_fp64) {
       PYFOF_CUDA(cudaFuncSetAttribute(direct::ub_direct_kernel<true>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       direct::ub_direct_kernel<true><<<(unsigned)direct.size(), BLK, smem, s>>>(m, off, dl, P, res, keep,
@@ -408,7 +418,16 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
     }
     PYFOF_CHECK_LAUNCH();
   }
-  if (!pm.empty()) PYFOF_TRY(unbind_pm(ctx, a, rules, m, tasks, pm, res, keep, st.phi_out, 0));
+  if (!pm.empty()) {
+    if (a.bound_per_halo) {
+      for (int32_t c : pm) {
+        const std::vector<int32_t> one(1, c);
+        PYFOF_TRY(unbind_pm(ctx, a, rules, m, tasks, one, res, keep, st.phi_out, 0));
+      }
+    } else {
+      PYFOF_TRY(unbind_pm(ctx, a, rules, m, tasks, pm, res, keep, st.phi_out, 0));
+    }
+  }
   PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   PYFOF_CUDA(cudaStreamSynchronize(s));
   if (ctx.h_flags[FLAG_ERR]) {

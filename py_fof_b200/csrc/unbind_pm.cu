@@ -473,6 +473,66 @@ __global__ void pm_sr_kernel(const Members m, const PmHalo *__restrict__ H,
   }
 }
 
+// Incremental short-range update after a refresh (bound_c2_update_
+// incremental_cells :3490-3552, bound_two_level_pp_update :1345-1498): every
+// member removed since the previous pass takes its pair terms back out of the
+// kept members within their cutoff.  jd[k] marks such members and is cleared.
+template <typename R>
+__global__ void pm_sr_update_kernel(const Members m, const PmHalo *__restrict__ H,
+                                    const int32_t *__restrict__ mhalo, const uint8_t *__restrict__ keep,
+                                    uint8_t *__restrict__ jd, const uint8_t *__restrict__ pr,
+                                    const uint32_t *__restrict__ ckey, const uint32_t *__restrict__ cstart,
+                                    const uint32_t *__restrict__ cmem, int64_t M, double a_val, double app,
+                                    R *__restrict__ phi_sr) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    if (!jd[k]) continue;
+    jd[k] = 0;
+    const int h = mhalo[k];
+    if (h < 0) continue;
+    const PmHalo &p = H[h];
+    if (!p.pending) continue;
+    const double sp = (double)p.spacing;
+    const R eps = (R)(double)(float)app;
+    const R fac = (R)(a_val / (6.0 * kPi));
+    int kk = p.two_level ? (int)ceil(3.5 / p.cw_u - 1e-9) : 1;
+    kk = kk < 1 ? 1 : (kk > 4 ? 4 : kk);
+    const int64_t local = (int64_t)ckey[k] - p.cell_off;
+    const int64_t n0 = p.nc[0], n1 = p.nc[1], n2 = p.nc[2];
+    const int64_t cx = local % n0, cy = (local / n0) % n1, cz = local / (n0 * n1);
+    const float xj = m.q[0][k], yj = m.q[1][k], zj = m.q[2][k];
+    const R wj = (R)m.w[k];
+    for (int64_t z = cz - kk; z <= cz + kk; ++z) {
+      if (z < 0 || z >= n2) continue;
+      for (int64_t y = cy - kk; y <= cy + kk; ++y) {
+        if (y < 0 || y >= n1) continue;
+        for (int64_t x = cx - kk; x <= cx + kk; ++x) {
+          if (x < 0 || x >= n0) continue;
+          const int64_t c = p.cell_off + x + n0 * (y + n1 * z);
+          for (uint32_t e = cstart[c]; e < cstart[c + 1]; ++e) {
+            const int64_t i = cmem[e];
+            if (i == k || !keep[i]) continue;
+            const R ai = (R)(3.5 * sp / (double)pr[i]);
+            R dx, dy, dz;
+            if (p.two_level) {
+              dx = (R)m.q[0][i] - (R)xj; dy = (R)m.q[1][i] - (R)yj; dz = (R)m.q[2][i] - (R)zj;
+            } else {
+              dx = (R)__fsub_rn(m.q[0][i], xj); dy = (R)__fsub_rn(m.q[1][i], yj);
+              dz = (R)__fsub_rn(m.q[2][i], zj);
+            }
+            const R r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 < ai * ai) {
+              const R d = sqrt(r2);
+              const R dphi = -(fac * (depth_c<R>(d, eps) - depth_c<R>(d, ai)));
+              atomicAdd(&phi_sr[i], -wj * dphi);
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------- two-level
 
 // One refined region: halo h, region b (8x8x8 regions of 16 grid cells),
@@ -714,6 +774,7 @@ template <typename R>
 __global__ void __launch_bounds__(IBLK) pm_inner_kernel(const Members m, PmHalo *__restrict__ H,
                                                         const int32_t *__restrict__ list, int nlist,
                                                         uint8_t *__restrict__ keep,
+                                                        uint8_t *__restrict__ jd,
                                                         const R *__restrict__ phi_c1,
                                                         const R *__restrict__ phi_in,
                                                         const R *__restrict__ phi_c2,
@@ -842,7 +903,10 @@ __global__ void __launch_bounds__(IBLK) pm_inner_kernel(const Members m, PmHalo 
       before += __popc(bal & ((1u << lane) - 1u));
       int chunk_eq = 0;
       for (int w = 0; w < IBLK / 32; ++w) chunk_eq += red_i[w];
-      if (i < np && (del_gt || (is_eq && before < need))) keep[k] = 0;
+      if (i < np && (del_gt || (is_eq && before < need))) {
+        keep[k] = 0;
+        jd[k] = 1;
+      }
       taken_eq += chunk_eq;
       __syncthreads();
     }
@@ -967,6 +1031,9 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
   R *selfv = W.carve<R>(M), *c1 = W.carve<R>(M), *c2 = W.carve<R>(M);
   float *phi = W.carve<float>(M), *en = W.carve<float>(M);
   R *tl_self_in = nullptr;
+  uint8_t *jd = W.carve<uint8_t>(M);  // removed since the previous pass
+  if (!jd) { set_error("workspace exhausted (removal marks)"); return kAlloc; }
+  PYFOF_CUDA(cudaMemsetAsync(jd, 0, M, s));
   double *ext = W.carve<double>(6 * (size_t)nh);
   if (!dH || !dlist || !dselfs || !mhalo || !first || !wt || !selfv || !c1 || !c2 || !phi || !en || !ext) {
     set_error("workspace exhausted (PM members)");
@@ -1219,9 +1286,13 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
         PYFOF_CHECK_LAUNCH();
       }
     }
-    pm_sr_kernel<R><<<gM, BLK, 0, s>>>(m, dH, mhalo, keep, pr, ckey, cstart, cmem, M, a.a_val, a.softening, c2);
+    if (pass == 1)
+      pm_sr_kernel<R><<<gM, BLK, 0, s>>>(m, dH, mhalo, keep, pr, ckey, cstart, cmem, M, a.a_val, a.softening, c2);
+    else
+      pm_sr_update_kernel<R><<<gM, BLK, 0, s>>>(m, dH, mhalo, keep, jd, pr, ckey, cstart, cmem, M, a.a_val,
+                                                a.softening, c2);
     PYFOF_CHECK_LAUNCH();
-    pm_inner_kernel<R><<<(unsigned)pend.size(), IBLK, 0, s>>>(m, dH, dpend, (int)pend.size(), keep, c1, phi_in, c2, phi,
+    pm_inner_kernel<R><<<(unsigned)pend.size(), IBLK, 0, s>>>(m, dH, dpend, (int)pend.size(), keep, jd, c1, phi_in, c2, phi,
                                                            en, (float)a.b_val, a.np_halo_min, phi_only,
                                                            ctx.d_flags);
     PYFOF_CHECK_LAUNCH();
@@ -1250,7 +1321,7 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
 int32_t unbind_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Members &m,
                   const std::vector<HaloTask> &tasks, const std::vector<int32_t> &list,
                   HaloResult *res, uint8_t *keep, float *phi_out, int phi_only) {
-  if (a.bound_fp64) return run_pm<double>(ctx, a, rules, m, tasks, list, res, keep, phi_out, phi_only);
+  if (a.bound_fp64 || a.bound_per_halo) return run_pm<double>(ctx, a, rules, m, tasks, list, res, keep, phi_out, phi_only);
   return run_pm<float>(ctx, a, rules, m, tasks, list, res, keep, phi_out, phi_only);
 }
 

@@ -102,3 +102,28 @@ def test_too_few_and_all_unbound(fp64_path):
     g = P._fof_core(xs, **kw)
     o = oracle_core(xs, **kw)
     assert np.array_equal(g[1], o[1])
+
+
+def test_per_halo_baseline_matches_batched():
+    """The plain per-halo FP64 baseline (one halo per launch sequence) and the
+    batched FP64 path compute each halo independently.  Direct summation is
+    deterministic; the mesh deposit adds with atomics, whose order may move a
+    potential in its last bits, so a marginally bound PM member may flip."""
+    from tests.test_pm_gpu import _pm_halos
+    xs, vs, ms = clumps(8, n_regions=30, masses=True)
+    xp, vp, mp = _pm_halos(11, [1300, 2200])
+    xs, vs, ms = xs + xp, vs + vp, ms + mp
+    kw = dict(vp_list=vs, mp_list=ms, L_Box=512.0, linking_length=0.3, np_halo_min=10,
+              bound_check=True, return_ang_mom=True)
+    _native.set_option("unbind_fp64", 1)
+    try:
+        a = P._fof_core(xs, **kw)
+        _native.set_option("unbind_per_halo", 1)
+        b = P._fof_core(xs, **kw)
+        assert _native.get_stat("pm_halos") >= 1
+    finally:
+        _native.set_option("unbind_per_halo", 0)
+        _native.set_option("unbind_fp64", 0)
+    assert int((a[0] != b[0]).sum()) <= 2
+    assert int(a[1].max()) == int(b[1].max())
+    assert angmom_close(a[2], b[2], np.abs(a[2]).max() + 1.0)
