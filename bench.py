@@ -2,24 +2,34 @@
 """Benchmark of the py_fof B200 hot path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload fof256|fof64|unbind256]
+                    [--workload fof_unbind_256|fof_256|fof_128|fof_64]
 
-One step = one full ``fof()`` call (binning, linking, labelling, candidate
-statistics; with --workload unbind256 also the unbinding of every candidate)
-over one synthetic particle set.  Default workload: 256^3 = 16,777,216
-particles in a periodic box of side 256 with 4096 Plummer halos (70% uniform
-background), link 0.2, np_halo_min 10.
+One step = one full ``fof()`` call over one synthetic particle set.  The
+default workload is FoF + unbinding (bound_check=True, cube units,
+softening 0.1) on 256^3 = 16,777,216 particles in a periodic box of side 256:
+70% uniform background, 30% in 4096 Plummer spheres (a = 1.5, member counts
+dN/dM ~ M^-1.9 over 20..5000), lognormal masses (sigma_ln 0.3, mean 1),
+virial velocities + bulk sigma 3 with 10% of members kicked by 3 sigma,
+background sigma 1; link 0.2, np_halo_min 10, s_15 = 15 * 0.67 * 256 / 300.
 
-* value: particles per second (Mpart/s) with the inputs resident in HBM,
-  device-timed with CUDA events on the stream the library launches on; all
-  ranks run their own replica (the periodic box is one region, which this
-  path does not split), value = N * particles / max-over-ranks time.
+* value: particles per second (Mpart/s) of the whole call (binning, linking,
+  labelling, candidate packing, unbinding of every candidate, outputs) with
+  the inputs resident in HBM, on the library's default FP32 unbinding path,
+  device-timed with CUDA events on the stream the library launches on.
+  All ranks run their own replica (one periodic box is one region, which
+  this path does not split): value = N * particles / max-over-ranks time.
+* unbind: candidates unbound per second of unbinding stage time for the
+  batched FP32 path, the batched FP64 path and the plain per-halo FP64 path
+  (one halo per launch sequence), each on the same input.
 * e2e: the same metric through the public API ``py_fof_b200.fof`` with
-  host (pinned) input arrays, host<->device copies inside the timed region.
-* roofline: the linking kernel's algorithmic bytes per launch over its
-  event-timed duration, against the measured HBM copy bandwidth.
-* cpu_baseline: the CPU restatement of the reference (oracle/, OpenMP) timed
-  on this host on the same workload.
+  pinned host inputs, host<->device copies inside the timed region.
+* roofline: the dominant kernel group.  With unbinding: the particle-mesh
+  convolutions (the FFT kernels), algorithmic bytes 16 (n+2) n^2 per solve
+  on an n^3 grid over their event-timed device time.  Plain FoF: the linking
+  kernel, 20 B per particle + 4 B per cell.
+* cpu_baseline: the CPU restatement of the reference (oracle/, OpenMP) on
+  this host, on a bounded sample of the workload (a sub-volume with the same
+  recipe and density).
 Under torchrun (N > 1) rank 0 prints the single JSON line.
 """
 from __future__ import annotations
@@ -38,15 +48,26 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# name: (n_side, bound_check); box side = n_side, halos = 4096 (n_side/256)^3
 WORKLOADS = {
-    # name: (n_side, L, halos, bound_check)
-    "fof256": (256, 256.0, 4096, False),
-    "fof64": (64, 64.0, 64, False),
-    "fof128": (128, 128.0, 512, False),
-    "unbind256": (256, 256.0, 4096, True),
+    "fof_unbind_256": (256, True),
+    "fof_unbind_128": (128, True),
+    "fof_256": (256, False),
+    "fof_128": (128, False),
+    "fof_64": (64, False),
+}
+# CPU sample of each workload: a sub-volume with the same recipe and density
+CPU_SAMPLE = {
+    "fof_unbind_256": "fof_unbind_128",
+    "fof_unbind_128": "fof_unbind_128",
+    "fof_256": "fof_64",
+    "fof_128": "fof_64",
+    "fof_64": "fof_64",
 }
 LINK = 0.2
 NP_MIN = 10
+SOFTENING = 0.1
+S15 = 15.0 * 0.67 * 256.0 / 300.0  # the 256-box value, kept for its sub-volumes
 # algorithmic bytes of the linking kernel: 12 B position read, 4 B parent
 # read, 4 B parent write per particle plus a 4 B cell offset per cell
 LINK_BYTES_PER_PARTICLE = 20
@@ -59,6 +80,18 @@ def _peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def _traffic(workload, kernel):
+    """DRAM bytes per algorithmic byte of `kernel`, from a committed ncu
+    summary (profiles/roofline_traffic.json), or None."""
+    tp = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if not os.path.exists(tp):
+        return None
+    d = json.load(open(tp)).get(kernel)
+    if not d:
+        return None
+    return float(d["dram_bytes_per_algorithmic_byte"])
 
 
 class ClockSampler:
@@ -119,10 +152,11 @@ class ClockSampler:
 
 def make_workload(name, seed=0):
     from py_fof_b200 import workloads as W
-    n_side, L, halos, bound = WORKLOADS[name]
-    d = W.plummer_box(n_side ** 3, L, halos, seed=seed, with_velocities=bound,
+    side, bound = WORKLOADS[name]
+    halos = max(1, int(round(4096 * (side / 256.0) ** 3)))
+    d = W.plummer_box(side ** 3, float(side), halos, seed=seed, with_velocities=bound,
                       lognormal_mass=0.3 if bound else None)
-    return d, L, bound
+    return d, float(side), bound
 
 
 def cpu_port_run(d, L, bound, threads):
@@ -134,26 +168,47 @@ def cpu_port_run(d, L, bound, threads):
     mp = d["mp"] if d["mp"] is not None else np.ones(n)
     t0 = time.perf_counter()
     _, hid, _, ierr = O.fof_fortran(xp, vp, mp, np.array([n], np.int32), 1, L, LINK, NP_MIN,
-                                    int(bound), 0, 0.1, 1.0, 0.0, 15 * 0.67 * L / 300.0,
-                                    threads, n)
+                                    int(bound), 0, SOFTENING, 1.0, 0.0, S15, threads, n)
     dt = time.perf_counter() - t0
     if ierr:
         raise RuntimeError(f"oracle ierr={ierr}")
     return dt, int(hid.max()), O.last_threads()
 
 
+def cpu_baseline(workload, seed, budget_s=15.0):
+    """The oracle on a bounded sample of `workload`, repeated for ~budget_s."""
+    name = CPU_SAMPLE[workload]
+    d, L, bound = make_workload(name, seed)
+    threads = os.cpu_count() or 1
+    cpu_port_run(d, L, bound, threads)  # first call builds the Green's function tables
+    dts = []
+    deadline = time.perf_counter() + budget_s
+    used = threads
+    while time.perf_counter() < deadline or not dts:
+        dt, _, used = cpu_port_run(d, L, bound, threads)
+        dts.append(dt)
+    n = d["xp"].shape[1]
+    return {"value": n / (sum(dts) / len(dts)) / 1e6, "unit": "Mpart/s", "cores": used,
+            "kind": "port",
+            "sample": f"{name}: {n} particles, same recipe and density as {workload} "
+                      f"(a sub-volume), {len(dts)} calls after one untimed call, "
+                      "reference thread policy"}
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU algorithm (restated in oracle/,
-    no reference build is possible here) on all host cores."""
+    the reference itself cannot be built here) on all host cores, each step a
+    bounded sample of the workload."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    d, L, bound = make_workload(args.workload, args.seed)
+    name = CPU_SAMPLE[args.workload]
+    d, L, bound = make_workload(name, args.seed)
     n = d["xp"].shape[1]
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
         cpu_port_run(d, L, bound, threads)
-    times = []
+    times, used = [], threads
     for _ in range(args.steps):
         dt, _, used = cpu_port_run(d, L, bound, threads)
         times.append(dt)
@@ -165,10 +220,10 @@ def run_reference(args):
         "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "particles": n, "L_Box": L, "link": LINK,
-                   "np_halo_min": NP_MIN, "bound_check": bound},
+                   "np_halo_min": NP_MIN, "bound_check": bound, "softening": SOFTENING},
         "cpu_baseline": {"value": v, "unit": "Mpart/s", "cores": used, "kind": "port",
-                         "sample": f"full workload ({n} particles) per step, reference "
-                                   "thread policy (one region: 2 linking threads)"},
+                         "sample": f"{name}: {n} particles per step, same recipe and density "
+                                   f"as {args.workload} (a sub-volume), reference thread policy"},
         "e2e": {"value": v, "unit": "Mpart/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -205,17 +260,31 @@ def run_b200(args):
     stream = torch.cuda.current_stream(dev)
     _native.set_stream(stream.cuda_stream)
     _native.set_option("timing", 1)
-    s15 = 15.0 * 0.67 * Lbox / 300.0
 
     def step():
-        am, ierr = _native.run_device(
+        _, ierr = _native.run_device(
             xp.data_ptr(), vp.data_ptr() if vp is not None else 0,
             mp.data_ptr() if mp is not None else 0, _native.LAYOUT_SOA, [n], 1, n, Lbox, LINK,
-            NP_MIN, int(bound), 0, 0.1, 1.0, 0.0, s15, 0, ih.data_ptr(), hid.data_ptr())
+            NP_MIN, int(bound), 0, SOFTENING, 1.0, 0.0, S15, 0, ih.data_ptr(), hid.data_ptr())
         if ierr:
             raise RuntimeError(f"ierr={ierr}: {_native.last_error()}")
-        return _native.last_link_ms()
+        return {k: _native.last_stage_ms(k) for k in ("link", "fof", "unbind", "call", "pm_fft")} | {
+            "pm_fft_bytes": _native.get_stat("pm_fft_bytes")}
 
+    def timed(steps):
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = [step() for _ in range(steps)]
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / steps, st
+
+    def mean(st, k):
+        return sum(s[k] for s in st) / len(st)
+
+    # the product path: batched FP32 unbinding (library default)
     for _ in range(max(args.warmup, 0)):
         step()
     torch.cuda.synchronize(dev)
@@ -224,83 +293,99 @@ def run_b200(args):
         dist.barrier()
     sampler = ClockSampler(local)
     sampler.start()
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize(dev)
-    t_start.record(stream)
-    link_ms = []
-    for _ in range(args.steps):
-        link_ms.append(step())
-    t_end.record(stream)
-    torch.cuda.synchronize(dev)
+    ms, st = timed(args.steps)
     clocks = sampler.stop()
     launches = _native.get_stat("launches") - launches0
     if world > 1:
         dist.barrier()
-    ms = t_start.elapsed_time(t_end) / args.steps
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
     value = world * n / (ms_max * 1e-3) / 1e6
     ngroups = int(hid.max().item())
+    counts = {k: _native.get_stat(k) for k in ("candidates", "direct_halos", "pm_halos",
+                                               "valid_halos", "pm_solves")}
+
+    if args.profile_run:
+        # only the warm-up and timed product steps (for a profiler's launch list)
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"profile_run": args.workload, "ms_per_step": ms_max,
+                              "gpu_launches": launches}), flush=True)
+        return 0
+
+    unbind = None
+    if bound:
+        ncand = counts["candidates"]
+
+        def leg(ms_call, st_):
+            u = mean(st_, "unbind")
+            return {"halos_per_s": ncand / (u * 1e-3) if u > 0 else None, "unbind_ms": u,
+                    "call_ms": ms_call}
+
+        legs = {"fp32_batched": leg(ms, st)}
+        _native.set_option("unbind_fp64", 1)
+        step()
+        legs["fp64_batched"] = leg(*timed(max(1, args.steps // 3)))
+        _native.set_option("unbind_per_halo", 1)
+        legs["fp64_per_halo"] = leg(*timed(1))
+        _native.set_option("unbind_per_halo", 0)
+        _native.set_option("unbind_fp64", 0)
+        base = legs["fp64_per_halo"]["halos_per_s"]
+        unbind = {"halos": ncand, "direct": counts["direct_halos"], "pm": counts["pm_halos"],
+                  "valid": counts["valid_halos"], "pm_solves": counts["pm_solves"], **legs,
+                  "fp32_vs_fp64_per_halo": (legs["fp32_batched"]["halos_per_s"] / base)
+                  if base else None}
 
     # end to end through the public API with pinned host buffers
-    xp_pin = torch.empty((3, n), dtype=torch.float64, pin_memory=True)
-    xp_pin.copy_(torch.from_numpy(d["xp"]))
-    xp_h = xp_pin.numpy()
-    vp_h = None
-    if d["vp"] is not None:
-        vp_pin = torch.empty((3, n), dtype=torch.float64, pin_memory=True)
-        vp_pin.copy_(torch.from_numpy(d["vp"]))
-        vp_h = vp_pin.numpy()
+    def pinned(a):
+        if a is None:
+            return None
+        p = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        p.copy_(torch.from_numpy(a))
+        return p.numpy()
+
+    xp_h, vp_h, mp_h = pinned(d["xp"]), pinned(d["vp"]), pinned(d["mp"])
     _native.set_stream(0)
-    kw = dict(vp_list=vp_h, L_Box=Lbox, linking_length=LINK, np_halo_min=NP_MIN,
-              bound_check=bound, mp_list=d["mp"])
-    for _ in range(max(1, args.warmup)):
+    kw = dict(vp_list=vp_h, mp_list=mp_h, L_Box=Lbox, linking_length=LINK, np_halo_min=NP_MIN,
+              bound_check=bound, softening=SOFTENING, ng_global=256.0)
+    for _ in range(max(1, min(args.warmup, 2))):
         P.fof(xp_h, **kw)
     e2e_t = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
         P.fof(xp_h, **kw)
         e2e_t.append(time.perf_counter() - t0)
-    e2e_s = sum(e2e_t) / len(e2e_t)
-    e2e_t_all = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    e2e_s = torch.tensor([sum(e2e_t) / len(e2e_t)], dtype=torch.float64, device=dev)
     if world > 1:
-        dist.all_reduce(e2e_t_all, op=dist.ReduceOp.MAX)
-    e2e_value = world * n / float(e2e_t_all.item()) / 1e6
-    h2d = 24 * n + (24 * n if vp_h is not None else 0) + (8 * n if d["mp"] is not None else 0)
+        dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
+    e2e_value = world * n / float(e2e_s.item()) / 1e6
+    h2d = 24 * n + (24 * n if vp_h is not None else 0) + (8 * n if mp_h is not None else 0)
     d2h = 8 * n + 24
 
-    # roofline of the linking kernel
     peak, peak_kind = _peaks()
-    link_ms_avg = sum(link_ms) / len(link_ms)
-    ncell = _native.get_stat("cells")
-    link_bytes = LINK_BYTES_PER_PARTICLE * n + LINK_BYTES_PER_CELL * ncell
-    achieved = link_bytes / (link_ms_avg * 1e-3) / 1e9 if link_ms_avg > 0 else None
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "link_traffic.json")
-    if os.path.exists(tp):
-        tj = json.load(open(tp))
-        if tj.get("workload") == args.workload:
-            traffic = tj.get("dram_bytes_per_launch")
+    if bound:
+        kname = "pm_convolve"
+        k_ms = mean(st, "pm_fft")
+        k_bytes = mean(st, "pm_fft_bytes")
+        roof_extra = {"kernels": "k_fft_x_r2c, k_fft_yz (3 launches), k_fft_x_c2r per batch",
+                      "algorithmic_bytes": "16 (n+2) n^2 per solve (a read and a write of the "
+                                           "padded grid per transform, two transforms)",
+                      "solves_per_call": counts["pm_solves"]}
+    else:
+        kname = "fof_link_kernel"
+        k_ms = mean(st, "link")
+        k_bytes = LINK_BYTES_PER_PARTICLE * n + LINK_BYTES_PER_CELL * _native.get_stat("cells")
+        roof_extra = {"algorithmic_bytes": "20 B per particle + 4 B per cell"}
+    achieved = k_bytes / (k_ms * 1e-3) / 1e9 if k_ms > 0 else None
+    ratio = _traffic(args.workload, kname)
+    traffic = ratio * k_bytes if ratio is not None else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        sample_name = "fof64" if args.workload != "fof64" else "fof64"
-        ds, Ls, bs = make_workload(sample_name, args.seed)
-        threads = os.cpu_count() or 1
-        cpu_port_run(ds, Ls, bs, threads)
-        dts = []
-        deadline = time.perf_counter() + 15.0
-        while time.perf_counter() < deadline or not dts:
-            dt, _, used = cpu_port_run(ds, Ls, bs, threads)
-            dts.append(dt)
-        ns = ds["xp"].shape[1]
-        cpu = {"value": ns / (sum(dts) / len(dts)) / 1e6, "unit": "Mpart/s", "cores": used,
-               "kind": "port",
-               "sample": f"{sample_name}: {ns} particles, same recipe and density, "
-                         f"{len(dts)} calls in ~15 s, reference thread policy"}
+        cpu = cpu_baseline(args.workload, args.seed)
 
     if world > 1:
         dist.barrier()
@@ -310,19 +395,25 @@ def run_b200(args):
     line = {
         "metric": "fof_mpart_per_s", "value": value, "unit": "Mpart/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 linking; f32 unbinding" if bound else "f64",
         "data": "synthetic",
         "config": {"workload": args.workload, "particles": n, "L_Box": Lbox, "link": LINK,
-                   "np_halo_min": NP_MIN, "bound_check": bound, "groups": ngroups,
+                   "np_halo_min": NP_MIN, "bound_check": bound, "softening": SOFTENING,
+                   "s_15": S15, "groups": ngroups, "unbinding": "fp32 batched" if bound else None,
                    "l2": "inputs larger than L2 (402 MB positions)" if n >= 2 ** 24 else
                          "inputs smaller than L2",
                    "parallelism": f"replicas x{world}"},
+        "stages_ms": {"fof": mean(st, "fof"), "link_kernel": mean(st, "link"),
+                      "unbind": mean(st, "unbind"), "pm_fft": mean(st, "pm_fft")},
+        "unbind": unbind,
         "e2e": {"value": e2e_value, "unit": "Mpart/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": "fof_link_kernel", "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": link_bytes, "kernel_ms": link_ms_avg},
+                     "kernel": kname, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_call": k_bytes, "kernel_ms_per_call": k_ms,
+                     **roof_extra},
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,
@@ -337,9 +428,11 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="fof256", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="fof_unbind_256", choices=sorted(WORKLOADS))
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="run only the warm-up and timed steps of the default path")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

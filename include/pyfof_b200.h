@@ -63,11 +63,23 @@ int32_t pyfof_set_stream(void *stream);
 /* Counters: "launches" (kernels launched by this process so far), and for
  * the last call on the selected device "cells" (reference cell grid size),
  * "active" (particles in linked regions), "candidates" (FoF groups with at
- * least np_halo_min members). */
+ * least np_halo_min members), "dense_cells" (cells given a sub-cell index),
+ * "direct_halos" / "pm_halos" (candidates unbound by direct summation / the
+ * particle mesh), "valid_halos" (halos written to the output),
+ * "refined_regions" (two-level inner regions), "pm_solves" (halo-grid
+ * convolutions over all passes), "pm_fft_bytes" (their algorithmic bytes:
+ * 16 (n+2) n^2 per solve on an n^3 grid). */
 int32_t pyfof_get_stat(const char *key, int64_t *value);
 
 /* Device time of the linking kernel of the last call, when timing is on. */
 int32_t pyfof_last_link_ms(float *ms);
+
+/* Device time (ms) of one stage of the last call, when timing is on:
+ * "link" (the linking kernel), "fof" (binning, linking and labelling up to
+ * the candidate list), "unbind" (unbinding and outputs with bound_check, the
+ * ang_mom pass without), "call" (all of it), "pm_fft" (the particle-mesh
+ * convolutions, summed over all solves). */
+int32_t pyfof_last_stage_ms(const char *stage, float *ms);
 
 /* First-pass gravitational potential of one candidate, computed by the
  * solver the reference rules select for it (bound_select_grid_and_level,

@@ -32,7 +32,7 @@ _RUN_ARGS = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, 
 
 # every symbol include/pyfof_b200.h declares
 EXPORTED = ("pyfof_version", "pyfof_init", "pyfof_shutdown", "pyfof_last_error",
-            "pyfof_set_option", "pyfof_set_stream", "pyfof_get_stat", "pyfof_last_link_ms",
+            "pyfof_set_option", "pyfof_set_stream", "pyfof_get_stat", "pyfof_last_link_ms", "pyfof_last_stage_ms",
             "pyfof_halo_potential", "pyfof_halo_potential_direct_static", "pyfof_run",
             "pyfof_run_device")
 
@@ -65,6 +65,8 @@ def load():
         L.pyfof_get_stat.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
         L.pyfof_last_link_ms.restype = ctypes.c_int32
         L.pyfof_last_link_ms.argtypes = [ctypes.POINTER(ctypes.c_float)]
+        L.pyfof_last_stage_ms.restype = ctypes.c_int32
+        L.pyfof_last_stage_ms.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_float)]
         L.pyfof_halo_potential.restype = ctypes.c_int32
         L.pyfof_halo_potential.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                            ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -113,6 +115,15 @@ def get_stat(key: str) -> int:
 def last_link_ms() -> float:
     v = ctypes.c_float(0.0)
     load().pyfof_last_link_ms(ctypes.byref(v))
+    return float(v.value)
+
+
+def last_stage_ms(stage: str) -> float:
+    """Device time of one stage of the last call ("link", "fof", "unbind",
+    "call"); needs set_option("timing", 1)."""
+    v = ctypes.c_float(0.0)
+    if load().pyfof_last_stage_ms(stage.encode(), ctypes.byref(v)) != 0:
+        raise ValueError(last_error())
     return float(v.value)
 
 

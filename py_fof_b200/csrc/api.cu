@@ -118,6 +118,18 @@ static int32_t validate(int32_t nhalo, int64_t total_np, const int32_t *np_halo,
   return kOk;
 }
 
+// stage_ms: [0] linking kernel, [1] binning to candidates, [2] unbinding (or
+// the plain ang_mom pass), [3] the whole call on the device
+static void record_stage_times(Context &ctx) {
+  for (float &t : ctx.stage_ms) t = 0.0f;
+  cudaEventElapsedTime(&ctx.stage_ms[0], ctx.ev[0], ctx.ev[1]);
+  cudaEventElapsedTime(&ctx.stage_ms[1], ctx.ev[2], ctx.ev[3]);
+  cudaEventElapsedTime(&ctx.stage_ms[2], ctx.ev[3], ctx.ev[4]);
+  cudaEventElapsedTime(&ctx.stage_ms[3], ctx.ev[2], ctx.ev[4]);
+  ctx.stage_ms[4] = (float)ctx.conv_timer.ms;
+  cudaGetLastError();  // a region without linking leaves the link events unrecorded
+}
+
 static int32_t run_common(Context &ctx, FofArgs &a) {
   ctx.timing = g_timing != 0;
   a.bound_fp64 = g_bound_fp64;
@@ -128,7 +140,7 @@ static int32_t run_common(Context &ctx, FofArgs &a) {
     set_error("CUDA failure: %s", cudaGetErrorString(e));
     r = kCuda;
   }
-  if (ctx.timing && r == kOk) cudaEventElapsedTime(&ctx.stage_ms[0], ctx.ev[0], ctx.ev[1]);
+  if (ctx.timing && r == kOk) record_stage_times(ctx);
   ctx.work.release();
   cudaStreamSynchronize(ctx.stream);
   return r;
@@ -194,6 +206,8 @@ int32_t pyfof_get_stat(const char *key, int64_t *value) {
   if (!std::strcmp(key, "pm_halos")) { *value = c->last_pm; return kOk; }
   if (!std::strcmp(key, "valid_halos")) { *value = c->last_valid; return kOk; }
   if (!std::strcmp(key, "refined_regions")) { *value = c->last_tl_regions; return kOk; }
+  if (!std::strcmp(key, "pm_solves")) { *value = c->last_pm_solves; return kOk; }
+  if (!std::strcmp(key, "pm_fft_bytes")) { *value = (int64_t)c->last_pm_fft_bytes; return kOk; }
   set_error("unknown statistic %s", key);
   return kInvalid;
 }
@@ -203,6 +217,23 @@ int32_t pyfof_last_link_ms(float *ms) {
   if (get_context(g_default_device, &c) != kOk || !ms) return kInvalid;
   *ms = c->stage_ms[0];
   return kOk;
+}
+
+int32_t pyfof_last_stage_ms(const char *stage, float *ms) {
+  Context *c;
+  if (!stage || !ms) {
+    set_error("pyfof_last_stage_ms: null argument");
+    return kInvalid;
+  }
+  if (get_context(g_default_device, &c) != kOk) return kInvalid;
+  static const char *names[5] = {"link", "fof", "unbind", "call", "pm_fft"};
+  for (int i = 0; i < 5; ++i)
+    if (!std::strcmp(stage, names[i])) {
+      *ms = c->stage_ms[i];
+      return kOk;
+    }
+  set_error("unknown stage %s", stage);
+  return kInvalid;
 }
 
 int32_t pyfof_halo_potential(const float *q, const float *w, int32_t np, double softening,
@@ -299,7 +330,7 @@ int32_t pyfof_run(const double *xp, const double *vp, const double *mp, int32_t 
     set_error("CUDA failure: %s", cudaGetErrorString(e));
     r = kCuda;
   }
-  if (ctx.timing && r == kOk) cudaEventElapsedTime(&ctx.stage_ms[0], ctx.ev[0], ctx.ev[1]);
+  if (ctx.timing && r == kOk) record_stage_times(ctx);
   ctx.work.release();
   cudaStreamSynchronize(s);
   if (r != kOk) {

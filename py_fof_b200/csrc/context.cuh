@@ -4,12 +4,43 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <vector>
 
 #include "common.cuh"
 
 namespace pyfof {
 
 struct GreenTable;  // unbinding Green's function cache entry (unbind.cu)
+
+// Device time of a launch group that repeats many times within one call
+// (bracketed by begin/end on the stream); collect() adds up the completed
+// pairs after a stream synchronisation.
+struct GroupTimer {
+  std::vector<cudaEvent_t> ev;
+  size_t used = 0;
+  double ms = 0.0;
+  void begin(cudaStream_t s) { record(s); }
+  void end(cudaStream_t s) { record(s); }
+  void collect() {
+    for (size_t i = 0; i + 1 < used; i += 2) {
+      float t = 0.0f;
+      if (cudaEventElapsedTime(&t, ev[i], ev[i + 1]) == cudaSuccess) ms += t;
+    }
+    used = 0;
+  }
+  void reset() { used = 0; ms = 0.0; }
+  ~GroupTimer() { for (auto e : ev) cudaEventDestroy(e); }
+
+ private:
+  void record(cudaStream_t s) {
+    if (used == ev.size()) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return;
+      ev.push_back(e);
+    }
+    cudaEventRecord(ev[used++], s);
+  }
+};
 
 struct Context {
   int device = 0;
@@ -24,6 +55,12 @@ struct Context {
   // timing of the last call's stages (ms), filled when timing is enabled
   bool timing = false;
   float stage_ms[16] = {};
+  GroupTimer conv_timer;  // PM convolutions (the FFT kernels) of the last call
+  // statistics of the last call: PM solves and their algorithmic FFT bytes
+  // (one read and one write of the padded (n+2) n^2 grid per transform, two
+  // transforms per solve)
+  int64_t last_pm_solves = 0;
+  double last_pm_fft_bytes = 0.0;
   // statistics of the last call
   int64_t last_cells = 0, last_active = 0, last_candidates = 0, last_dense = 0;
   int64_t last_direct = 0, last_pm = 0, last_valid = 0, last_tl_regions = 0;

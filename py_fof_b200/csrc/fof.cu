@@ -954,10 +954,17 @@ int32_t fof_plain_angmom(Context &ctx, const FofArgs &a, FofState &st) {
 
 int32_t fof_run(Context &ctx, const FofArgs &a) {
   FofState st;
+  ctx.conv_timer.reset();
+  ctx.last_pm_solves = 0;
+  ctx.last_pm_fft_bytes = 0.0;
+  if (ctx.timing) cudaEventRecord(ctx.ev[2], ctx.stream);
   PYFOF_TRY(fof_link_stage(ctx, a, st));
   PYFOF_TRY(fof_candidates_stage(ctx, a, st, !a.bound_check));
-  if (!a.bound_check) return fof_plain_angmom(ctx, a, st);
-  return unbind_stage(ctx, a, st);
+  if (ctx.timing) cudaEventRecord(ctx.ev[3], ctx.stream);
+  if (!a.bound_check) PYFOF_TRY(fof_plain_angmom(ctx, a, st));
+  else PYFOF_TRY(unbind_stage(ctx, a, st));
+  if (ctx.timing) cudaEventRecord(ctx.ev[4], ctx.stream);
+  return kOk;
 }
 
 }  // namespace pyfof

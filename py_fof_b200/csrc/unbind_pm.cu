@@ -1251,7 +1251,11 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
         PYFOF_CHECK_LAUNCH();
         pm_deposit_kernel<R><<<gM, BLK, 0, s>>>(m, dH, mhalo, keep, first, wt, dslot, M, rho);
         PYFOF_CHECK_LAUNCH();
+        if (ctx.timing) ctx.conv_timer.begin(s);
         PYFOF_TRY(pm_convolve_batch<R>(rho, spec, (const R *)green_of[n]->g, n, sup, nb, s));
+        if (ctx.timing) ctx.conv_timer.end(s);
+        ctx.last_pm_solves += nb;
+        ctx.last_pm_fft_bytes += 16.0 * nb * (n + 2.0) * n * n;
         pm_gather_kernel<R><<<gM, BLK, 0, s>>>(m, dH, mhalo, keep, first, wt, selfv, dslot, M, rho, a.a_val,
                                                c1);
         PYFOF_CHECK_LAUNCH();
@@ -1280,7 +1284,11 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
         PYFOF_CHECK_LAUNCH();
         tl_deposit_kernel<R><<<nb, BLK, 0, s>>>(m, dH, dA, dbatch, src_start, src, keep, sup, rho);
         PYFOF_CHECK_LAUNCH();
+        if (ctx.timing) ctx.conv_timer.begin(s);
         PYFOF_TRY(pm_convolve_batch<R>(rho, spec, gin, nin, sup, nb, s));
+        if (ctx.timing) ctx.conv_timer.end(s);
+        ctx.last_pm_solves += nb;
+        ctx.last_pm_fft_bytes += 16.0 * nb * (nin + 2.0) * nin * nin;
         tl_gather_kernel<R><<<nb, BLK, 0, s>>>(m, dH, dA, dbatch, tgt_start, tgt, keep, tl_self_in, sup, rho,
                                                a.a_val, phi_in);
         PYFOF_CHECK_LAUNCH();
@@ -1299,6 +1307,7 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
     PYFOF_CUDA(cudaMemcpyAsync(H.data(), dH, sizeof(PmHalo) * nh, cudaMemcpyDeviceToHost, s));
     PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     PYFOF_CUDA(cudaStreamSynchronize(s));
+    if (ctx.timing) ctx.conv_timer.collect();
     if (ctx.h_flags[FLAG_ERR]) {
       set_error("particle-mesh unbinding failed (error %d)", ctx.h_flags[FLAG_ERR]);
       return ctx.h_flags[FLAG_ERR];
