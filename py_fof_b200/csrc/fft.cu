@@ -1,278 +1,591 @@
 // Batched zero-padded 3-D FFT convolution for the particle-mesh solver.
-// See fft.cuh for layouts.  Each kernel transforms whole lines held in
-// shared memory with a Stockham autosort FFT (radices 4, 2, 3).
+// See fft.cuh for layouts.
+//
+// Every line transform of length N = N1 * N2 runs as two register-resident
+// DFTs with one shared-memory exchange between them (Cooley-Tukey with the
+// input index e = s + N2 q and the output index k = k1 + N1 k2):
+//   stage A  thread (line, s):  Y[s][k1] = sum_q x[s + N2 q] W_N1^(q k1),
+//            times the twiddle W_N^(s k1), written to shared memory;
+//   stage B  thread (line, k1): X[k1 + N1 k2] = sum_s Y[s][k1] W_N2^(s k2).
+// The register DFTs are mixed-radix (4, 2, 3) decompositions unrolled at
+// compile time with constant twiddles.  A block works on a tile of W lines
+// that are adjacent in memory (consecutive kx), so every global access of a
+// warp covers whole 128-byte segments.  The z pass does forward transform,
+// Green multiplication and inverse transform in one kernel (stage B holds a
+// full frequency line per thread; the inverse walks the same stages back),
+// and loops over the halos of a batch with the Green values held in
+// registers, so the table is read once per block.
+#include <utility>
+
 #include "fft.cuh"
 
 namespace pyfof {
 
 namespace {
 
-constexpr int FT = 256;  // threads per block
+// ------------------------------------------------------------ compile time
 
-template <typename R>
-__device__ __forceinline__ void sincospi_t(R x, R *s, R *c);
-template <>
-__device__ __forceinline__ void sincospi_t<float>(float x, float *s, float *c) { sincospif(x, s, c); }
-template <>
-__device__ __forceinline__ void sincospi_t<double>(double x, double *s, double *c) { sincospi(x, s, c); }
-
-template <typename C>
-__device__ __forceinline__ C cmul(C a, C b) {
-  C r;
-  r.x = a.x * b.x - a.y * b.y;
-  r.y = a.x * b.y + a.y * b.x;
-  return r;
+template <class F, int... I>
+__device__ __forceinline__ void sfor_impl(F &&f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, I>{}), ...);
 }
-template <typename C>
-__device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
-template <typename C>
-__device__ __forceinline__ C csub(C a, C b) { C r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+template <int N, class F>
+__device__ __forceinline__ void sfor(F &&f) {
+  sfor_impl(static_cast<F &&>(f), std::make_integer_sequence<int, N>{});
+}
 
-struct Radices {
-  int nf;
-  int f[12];
+constexpr double kQuarterPi = 0.785398163397448309615660845819875721;
+
+__host__ __device__ constexpr double taylor_sin(double x) {
+  double x2 = x * x, term = x, sum = x;
+  for (int k = 1; k < 12; ++k) {
+    term *= -x2 / (double)((2 * k) * (2 * k + 1));
+    sum += term;
+  }
+  return sum;
+}
+__host__ __device__ constexpr double taylor_cos(double x) {
+  double x2 = x * x, term = 1.0, sum = 1.0;
+  for (int k = 1; k < 12; ++k) {
+    term *= -x2 / (double)((2 * k - 1) * (2 * k));
+    sum += term;
+  }
+  return sum;
+}
+
+struct CosSin {
+  double c, s;
 };
 
-Radices factor(int n) {
-  Radices r{};
-  while (n % 4 == 0) { r.f[r.nf++] = 4; n /= 4; }
-  while (n % 2 == 0) { r.f[r.nf++] = 2; n /= 2; }
-  while (n % 3 == 0) { r.f[r.nf++] = 3; n /= 3; }
-  if (n != 1) r.nf = -1;
-  return r;
-}
-
-// tw[k] = exp(-2 pi i k / n)
-template <typename R>
-__device__ __forceinline__ void make_twiddles(cplx_t<R> *tw, int n) {
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    R s, c;
-    sincospi_t<R>((R)(2 * k) / (R)n, &s, &c);
-    tw[k].x = c;
-    tw[k].y = -s;
+// cos and sin of the angle 2 pi num / den: exact octant reduction of the
+// rational angle, then Taylor series on [0, pi/4].
+__host__ __device__ constexpr CosSin turn(int num, int den) {
+  num %= den;
+  if (num < 0) num += den;
+  const long long e = 8LL * num;
+  const int o = (int)(e / den);
+  const long long r = e - (long long)o * den;
+  const double th = kQuarterPi * (double)r / (double)den;          // [0, pi/4)
+  const double ph = kQuarterPi * (double)(den - r) / (double)den;  // pi/4 - th
+  switch (o) {
+    case 0: return {taylor_cos(th), taylor_sin(th)};
+    case 1: return {taylor_sin(ph), taylor_cos(ph)};
+    case 2: return {-taylor_sin(th), taylor_cos(th)};
+    case 3: return {-taylor_cos(ph), taylor_sin(ph)};
+    case 4: return {-taylor_cos(th), -taylor_sin(th)};
+    case 5: return {-taylor_sin(ph), -taylor_cos(ph)};
+    case 6: return {taylor_sin(th), -taylor_cos(th)};
+    default: return {taylor_cos(ph), -taylor_sin(ph)};
   }
 }
 
-// Stockham FFT of `lines` lines of length n held in A (A[l*n+e]); B is
-// scratch.  sign = -1 forward, +1 inverse (unnormalised).  Returns the
-// buffer that holds the result.
+// ---------------------------------------------------------------- complex
+
+template <typename C>
+__device__ __forceinline__ C mk(decltype(C{}.x) x, decltype(C{}.x) y) {
+  C r;
+  r.x = x;
+  r.y = y;
+  return r;
+}
+template <typename C>
+__device__ __forceinline__ C cadd(C a, C b) { return mk<C>(a.x + b.x, a.y + b.y); }
+template <typename C>
+__device__ __forceinline__ C csub(C a, C b) { return mk<C>(a.x - b.x, a.y - b.y); }
+template <typename C>
+__device__ __forceinline__ C cmul(C a, C b) {
+  return mk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+template <typename C>
+__device__ __forceinline__ C cmulc(C a, C b) {
+  return mk<C>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+// v * exp(SIGN 2 pi i J / M), J and M known at compile time
+template <int SIGN, int J, int M, typename C>
+__device__ __forceinline__ C twc(C v) {
+  constexpr int j = J % M;
+  if constexpr (j == 0) {
+    return v;
+  } else if constexpr (2 * j == M) {
+    return mk<C>(-v.x, -v.y);
+  } else if constexpr (4 * j == M) {  // times SIGN i
+    return SIGN < 0 ? mk<C>(v.y, -v.x) : mk<C>(-v.y, v.x);
+  } else if constexpr (4 * j == 3 * M) {  // times -SIGN i
+    return SIGN < 0 ? mk<C>(-v.y, v.x) : mk<C>(v.y, -v.x);
+  } else {
+    using R = decltype(v.x);
+    constexpr CosSin w = turn(j, M);
+    constexpr R c = (R)w.c;
+    constexpr R s = (R)(SIGN * w.s);
+    return mk<C>(v.x * c - v.y * s, v.x * s + v.y * c);
+  }
+}
+
+// In-register DFT of length M: v[k] <- sum_e v[e] exp(SIGN 2 pi i e k / M).
+template <int M, int SIGN, typename C>
+__device__ __forceinline__ void dft(C (&v)[M]) {
+  using R = decltype(v[0].x);
+  if constexpr (M == 1) {
+  } else if constexpr (M == 2) {
+    const C a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if constexpr (M == 3) {
+    const R h = (R)0.866025403784438646763723170752936183;  // sqrt(3)/2
+    const C t1 = cadd(v[1], v[2]);
+    const C t2 = mk<C>(v[0].x - (R)0.5 * t1.x, v[0].y - (R)0.5 * t1.y);
+    const C d = csub(v[1], v[2]);
+    const C t3 = SIGN < 0 ? mk<C>(h * d.y, -h * d.x) : mk<C>(-h * d.y, h * d.x);
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(t2, t3);
+    v[2] = csub(t2, t3);
+  } else if constexpr (M == 4) {
+    const C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    const C t2 = cadd(v[1], v[3]), d = csub(v[1], v[3]);
+    const C t3 = SIGN < 0 ? mk<C>(d.y, -d.x) : mk<C>(-d.y, d.x);
+    v[0] = cadd(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[2] = csub(t0, t2);
+    v[3] = csub(t1, t3);
+  } else {
+    // decimation in time: e = p + P q, k = k' + Q j
+    constexpr int P = (M % 4 == 0) ? 4 : ((M % 2 == 0) ? 2 : 3);
+    constexpr int Q = M / P;
+    static_assert(P * Q == M, "DFT length must be 2^a 3^b");
+    C sub[P][Q];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) sub[p][q] = v[p + P * q];
+      dft<Q, SIGN>(sub[p]);
+    }
+    sfor<Q>([&](auto kc) {
+      constexpr int k = decltype(kc)::value;
+      C t[P];
+      sfor<P>([&](auto pc) {
+        constexpr int p = decltype(pc)::value;
+        t[p] = twc<SIGN, p * k, M>(sub[p][k]);
+      });
+      dft<P, SIGN>(t);
+#pragma unroll
+      for (int j = 0; j < P; ++j) v[k + Q * j] = t[j];
+    });
+  }
+}
+
+// ------------------------------------------------------------------ plans
+
+// Lines per tile: 128 bytes of complex values per row of the tile.
 template <typename R>
-__device__ cplx_t<R> *fft_lines(cplx_t<R> *A, cplx_t<R> *B, const cplx_t<R> *tw, int n, int lines,
-                                const Radices &rad, int sign) {
-  typedef cplx_t<R> C;
-  int m = 1;
-  const R s3 = (R)0.86602540378443864676;  // sqrt(3)/2
-  for (int st = 0; st < rad.nf; ++st) {
-    const int r = rad.f[st];
-    const int l = n / (m * r);
-    const int step = n / (l * r);
-    const int nb = n / r;
-    for (int t = threadIdx.x; t < lines * nb; t += blockDim.x) {
-      const int line = t / nb, bf = t - line * nb;
-      const int j = bf / m, k = bf - j * m;
-      const C *a = A + line * n;
-      C *b = B + line * n;
-      C v[4];
+constexpr int kW = sizeof(R) == 4 ? 16 : 8;
+
+// N = N1 * N2 and threads per block.
+template <typename R, int N>
+struct Cfg;
+template <> struct Cfg<float, 48> { static constexpr int N1 = 8, N2 = 6, T = 128; };
+template <> struct Cfg<float, 64> { static constexpr int N1 = 8, N2 = 8, T = 128; };
+template <> struct Cfg<float, 128> { static constexpr int N1 = 16, N2 = 8, T = 128; };
+template <> struct Cfg<float, 216> { static constexpr int N1 = 12, N2 = 18, T = 96; };
+template <> struct Cfg<float, 256> { static constexpr int N1 = 16, N2 = 16, T = 256; };
+template <> struct Cfg<double, 48> { static constexpr int N1 = 8, N2 = 6, T = 64; };
+template <> struct Cfg<double, 64> { static constexpr int N1 = 8, N2 = 8, T = 64; };
+template <> struct Cfg<double, 128> { static constexpr int N1 = 16, N2 = 8, T = 64; };
+template <> struct Cfg<double, 216> { static constexpr int N1 = 12, N2 = 18, T = 96; };
+template <> struct Cfg<double, 256> { static constexpr int N1 = 16, N2 = 16, T = 128; };
+
+template <typename R, int N>
+constexpr size_t smem_bytes() {
+  // twiddles + two tiles of N rows of W+1 complex (one pad column)
+  return sizeof(cplx_t<R>) * (size_t)(N + 2 * (kW<R> + 1) * N);
+}
+
+// tw[j] = exp(-2 pi i j / N), from double-precision sincospi
+template <typename R, int N, int T>
+__device__ __forceinline__ void load_twiddles(cplx_t<R> *tw) {
+  for (int j = threadIdx.x; j < N; j += T) {
+    double s, c;
+    sincospi(2.0 * (double)j / (double)N, &s, &c);
+    tw[j] = mk<cplx_t<R>>((R)c, (R)-s);
+  }
+}
+
+// Stage A on a tile held in `src` (tile element (li, e) at li + (W+1) e),
+// result with twiddles into `dst` (element (li, s, k1) at li + (W+1)(k1 + N1 s)).
+// Elements e >= in_lim are zero.
+template <typename R, int N, int SIGN>
+__device__ __forceinline__ void stage_a_smem(const cplx_t<R> *src, cplx_t<R> *dst, const cplx_t<R> *tw,
+                                             int in_lim) {
+  using C = cplx_t<R>;
+  constexpr int N1 = Cfg<R, N>::N1, N2 = Cfg<R, N>::N2, T = Cfg<R, N>::T;
+  constexpr int W = kW<R>, WP = W + 1, UA = W * N2;
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (q < r) v[q] = a[(q * l + j) * m + k];
-      C o[4];
-      if (r == 2) {
-        o[0] = cadd(v[0], v[1]);
-        o[1] = csub(v[0], v[1]);
-      } else if (r == 4) {
-        const C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]), t2 = cadd(v[1], v[3]);
-        const C d = csub(v[1], v[3]);
-        C t3;  // d * (-i) forward, d * (+i) inverse
-        if (sign < 0) { t3.x = d.y; t3.y = -d.x; } else { t3.x = -d.y; t3.y = d.x; }
-        o[0] = cadd(t0, t2);
-        o[1] = cadd(t1, t3);
-        o[2] = csub(t0, t2);
-        o[3] = csub(t1, t3);
-      } else {
-        const C t1 = cadd(v[1], v[2]);
-        C t2;
-        t2.x = v[0].x - (R)0.5 * t1.x;
-        t2.y = v[0].y - (R)0.5 * t1.y;
-        const C d = csub(v[1], v[2]);
-        C t3;  // s3 * d * (-i) forward, s3 * d * (+i) inverse
-        if (sign < 0) { t3.x = s3 * d.y; t3.y = -s3 * d.x; } else { t3.x = -s3 * d.y; t3.y = s3 * d.x; }
-        o[0] = cadd(v[0], t1);
-        o[1] = cadd(t2, t3);
-        o[2] = csub(t2, t3);
+  for (int it = 0; it < (UA + T - 1) / T; ++it) {
+    const int u = threadIdx.x + it * T;
+    if (u < UA) {
+      const int li = u % W, s = u / W;
+      C v[N1];
+#pragma unroll
+      for (int q = 0; q < N1; ++q) {
+        const int e = s + N2 * q;
+        v[q] = e < in_lim ? src[li + WP * e] : mk<C>(0, 0);
       }
-      // decimation in frequency: output u of butterfly j takes w^(j*u)
-      C *ob = b + (j * r) * m + k;
+      dft<N1, SIGN>(v);
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        if (u < r) {
-          C val = o[u];
-          if (u > 0 && j > 0) {
-            C w = tw[j * u * step];
-            if (sign > 0) w.y = -w.y;
-            val = cmul(val, w);
-          }
-          ob[u * m] = val;
+      for (int k1 = 0; k1 < N1; ++k1)
+        dst[li + WP * (k1 + N1 * s)] = SIGN < 0 ? cmul(v[k1], tw[s * k1]) : cmulc(v[k1], tw[s * k1]);
+    }
+  }
+}
+
+// Stage B from `src` (stage A layout) into tile layout `dst` (li + (W+1) k).
+template <typename R, int N, int SIGN>
+__device__ __forceinline__ void stage_b_smem(const cplx_t<R> *src, cplx_t<R> *dst) {
+  using C = cplx_t<R>;
+  constexpr int N1 = Cfg<R, N>::N1, N2 = Cfg<R, N>::N2, T = Cfg<R, N>::T;
+  constexpr int W = kW<R>, WP = W + 1, UB = W * N1;
+#pragma unroll
+  for (int it = 0; it < (UB + T - 1) / T; ++it) {
+    const int u = threadIdx.x + it * T;
+    if (u < UB) {
+      const int li = u % W, k1 = u / W;
+      C v[N2];
+#pragma unroll
+      for (int s = 0; s < N2; ++s) v[s] = src[li + WP * (k1 + N1 * s)];
+      dft<N2, SIGN>(v);
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) dst[li + WP * (k1 + N1 * k2)] = v[k2];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ kernels
+
+// x pass, forward r2c.  Real lines L = (b*sup + z)*sup + y, x < sup, are
+// taken in pairs as one complex line (a + i b); the two half spectra are
+// separated with the Hermitian symmetry of real transforms.
+template <typename R, int N>
+__global__ void __launch_bounds__(Cfg<R, N>::T) k_x_r2c(const R *__restrict__ rho, cplx_t<R> *__restrict__ spec,
+                                                        int sup, int nhp, int64_t nlines) {
+  using C = cplx_t<R>;
+  constexpr int T = Cfg<R, N>::T, W = kW<R>, WP = W + 1, NH = N / 2 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *tw = reinterpret_cast<C *>(smem_raw);
+  C *t0 = tw + N, *t1 = t0 + WP * N;
+  load_twiddles<R, N, T>(tw);
+  const int64_t L0 = (int64_t)blockIdx.x * (2 * W);
+  for (int p = 0; p < W; ++p) {
+    const int64_t La = L0 + 2 * p, Lb = La + 1;
+    for (int x = threadIdx.x; x < sup; x += T) {
+      const R a = La < nlines ? rho[La * sup + x] : (R)0;
+      const R b = Lb < nlines ? rho[Lb * sup + x] : (R)0;
+      t0[p + WP * x] = mk<C>(a, b);
+    }
+  }
+  __syncthreads();
+  stage_a_smem<R, N, -1>(t0, t1, tw, sup);
+  __syncthreads();
+  stage_b_smem<R, N, -1>(t1, t0);
+  __syncthreads();
+  const int64_t ss = (int64_t)sup * sup;
+  for (int p = 0; p < W; ++p) {
+    const int64_t La = L0 + 2 * p;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int64_t L = La + h;
+      if (L >= nlines) break;
+      const int64_t b = L / ss;
+      const int64_t rem = L - b * ss;
+      const int64_t z = rem / sup, y = rem - z * sup;
+      C *row = spec + ((b * N + z) * N + y) * nhp;
+      for (int kx = threadIdx.x; kx < NH; kx += T) {
+        const C zk = t0[p + WP * kx];
+        const C zm = t0[p + WP * ((N - kx) % N)];
+        C out;
+        if (h == 0) out = mk<C>((R)0.5 * (zk.x + zm.x), (R)0.5 * (zk.y - zm.y));
+        else out = mk<C>((R)0.5 * (zk.y + zm.y), (R)0.5 * (zm.x - zk.x));
+        row[kx] = out;
+      }
+    }
+  }
+}
+
+// x pass, c2r into compact cubes of side olim: lines L = (b*olim + z)*olim
+// + y, out[L*olim + x] = x-th real value / scale.  Two Hermitian half
+// spectra become one complex line (a + i b); only the real parts of the DC
+// and Nyquist bins are used.
+template <typename R, int N>
+__global__ void __launch_bounds__(Cfg<R, N>::T) k_x_c2r(const cplx_t<R> *__restrict__ spec, R *__restrict__ out,
+                                                        int olim, int nhp, int64_t nlines, R scale) {
+  using C = cplx_t<R>;
+  constexpr int T = Cfg<R, N>::T, W = kW<R>, WP = W + 1, NH = N / 2 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *tw = reinterpret_cast<C *>(smem_raw);
+  C *t0 = tw + N, *t1 = t0 + WP * N;
+  load_twiddles<R, N, T>(tw);
+  const int64_t L0 = (int64_t)blockIdx.x * (2 * W);
+  const int64_t oo = (int64_t)olim * olim;
+  for (int p = 0; p < W; ++p) {
+    const int64_t La = L0 + 2 * p, Lb = La + 1;
+    const C *ra = nullptr, *rb = nullptr;
+    if (La < nlines) {
+      const int64_t b = La / oo, rem = La - b * oo, z = rem / olim, y = rem - z * olim;
+      ra = spec + ((b * N + z) * N + y) * nhp;
+    }
+    if (Lb < nlines) {
+      const int64_t b = Lb / oo, rem = Lb - b * oo, z = rem / olim, y = rem - z * olim;
+      rb = spec + ((b * N + z) * N + y) * nhp;
+    }
+    for (int kx = threadIdx.x; kx < NH; kx += T) {
+      C a = ra ? ra[kx] : mk<C>(0, 0);
+      C b = rb ? rb[kx] : mk<C>(0, 0);
+      if (kx == 0 || kx == N / 2) {
+        a.y = 0;
+        b.y = 0;
+      }
+      t0[p + WP * kx] = mk<C>(a.x - b.y, a.y + b.x);
+      if (kx > 0 && kx < N / 2) t0[p + WP * (N - kx)] = mk<C>(a.x + b.y, b.x - a.y);
+    }
+  }
+  __syncthreads();
+  stage_a_smem<R, N, +1>(t0, t1, tw, N);
+  __syncthreads();
+  stage_b_smem<R, N, +1>(t1, t0);
+  __syncthreads();
+  for (int p = 0; p < W; ++p) {
+    const int64_t La = L0 + 2 * p;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int64_t L = La + h;
+      if (L >= nlines) break;
+      for (int x = threadIdx.x; x < olim; x += T) {
+        const C v = t0[p + WP * x];
+        out[L * olim + x] = (h == 0 ? v.x : v.y) / scale;
+      }
+    }
+  }
+}
+
+// Strided pass over tiles of W consecutive kx.  Line (b, other, kx) starts at
+// spec + b*bstride + other*ostride + kx, element e at + e*estride.  Elements
+// e >= in_lim are zero; elements e < out_lim are written.  CONV: forward
+// transform, multiplication by the real Green table (index ((e*N + other)*NH
+// + kx)) and inverse transform; otherwise one transform of sign SIGN.  A
+// block handles halos [b0, b0 + nbb) of the batch.
+template <typename R, int N, int SIGN, bool CONV>
+__global__ void __launch_bounds__(Cfg<R, N>::T) k_lines(cplx_t<R> *__restrict__ spec, const R *__restrict__ green,
+                                                        int64_t bstride, int64_t ostride, int64_t estride,
+                                                        int nother, int ntiles, int nbb, int batch, int in_lim,
+                                                        int out_lim) {
+  using C = cplx_t<R>;
+  constexpr int N1 = Cfg<R, N>::N1, N2 = Cfg<R, N>::N2, T = Cfg<R, N>::T;
+  constexpr int W = kW<R>, WP = W + 1, NH = N / 2 + 1;
+  constexpr int UA = W * N2, UB = W * N1;
+  constexpr int IA = (UA + T - 1) / T, IB = (UB + T - 1) / T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *tw = reinterpret_cast<C *>(smem_raw);
+  C *const buf0 = tw + N;
+  load_twiddles<R, N, T>(tw);
+  int64_t bid = blockIdx.x;
+  const int tile = (int)(bid % ntiles);
+  bid /= ntiles;
+  const int other = (int)(bid % nother);
+  const int b0 = (int)(bid / nother) * nbb;
+  const int b1 = min(batch, b0 + nbb);
+  const int kx0 = tile * W;
+  R g[CONV ? IB : 1][CONV ? N2 : 1];
+  if constexpr (CONV) {
+#pragma unroll
+    for (int it = 0; it < IB; ++it) {
+      const int u = threadIdx.x + it * T;
+      const int li = u % W, k1 = u / W, kx = kx0 + li;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) {
+        const int e = k1 + N1 * k2;
+        g[it][k2] = (u < UB && kx < NH) ? green[((int64_t)e * N + other) * NH + kx] : (R)0;
+      }
+    }
+  }
+  __syncthreads();
+  int parity = 0;
+  for (int b = b0; b < b1; ++b) {
+    C *base = spec + (int64_t)b * bstride + (int64_t)other * ostride + kx0;
+    C *bA = buf0 + parity * (WP * N);
+    // stage A: global -> registers -> DFT over q -> twiddle -> shared
+#pragma unroll
+    for (int it = 0; it < IA; ++it) {
+      const int u = threadIdx.x + it * T;
+      if (u < UA) {
+        const int li = u % W, s = u / W;
+        const bool col = kx0 + li < NH;
+        C v[N1];
+#pragma unroll
+        for (int q = 0; q < N1; ++q) {
+          const int e = s + N2 * q;
+          v[q] = (col && e < in_lim) ? base[(int64_t)e * estride + li] : mk<C>(0, 0);
+        }
+        dft<N1, CONV ? -1 : SIGN>(v);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) {
+          const C w = tw[s * k1];
+          bA[li + WP * (k1 + N1 * s)] = (CONV || SIGN < 0) ? cmul(v[k1], w) : cmulc(v[k1], w);
         }
       }
     }
     __syncthreads();
-    C *tmp = A; A = B; B = tmp;
-    m *= r;
-  }
-  return A;
-}
-
-template <typename R>
-__device__ __forceinline__ cplx_t<R> *smem_base() {
-  extern __shared__ __align__(16) unsigned char fft_smem[];
-  return reinterpret_cast<cplx_t<R> *>(fft_smem);
-}
-
-// x pass, forward r2c: lines (y,z) in [0,sup)^2 of every grid.
-template <typename R>
-__global__ void __launch_bounds__(FT) k_fft_x_r2c(const R *__restrict__ rho, cplx_t<R> *__restrict__ spec,
-                                                  int n, int sup, int lpb, int64_t nlines, Radices rad) {
-  typedef cplx_t<R> C;
-  C *tw = smem_base<R>();
-  C *A = tw + n, *B = A + lpb * n;
-  make_twiddles<R>(tw, n);
-  const int nh = n / 2 + 1;
-  const int64_t l0 = (int64_t)blockIdx.x * lpb;
-  const int nl = (int)(nlines - l0 < (int64_t)lpb ? nlines - l0 : (int64_t)lpb);
-  for (int t = threadIdx.x; t < nl * n; t += blockDim.x) {
-    const int li = t / n, x = t - li * n;
-    const int64_t L = l0 + li;  // (b*sup + z)*sup + y
-    C v;
-    v.x = x < sup ? rho[L * sup + x] : (R)0;
-    v.y = 0;
-    A[li * n + x] = v;
-  }
-  __syncthreads();
-  C *res = fft_lines<R>(A, B, tw, n, nl, rad, -1);
-  for (int t = threadIdx.x; t < nl * nh; t += blockDim.x) {
-    const int li = t / nh, kx = t - li * nh;
-    const int64_t L = l0 + li;
-    const int64_t b = L / ((int64_t)sup * sup);
-    const int rem = (int)(L - b * sup * sup);
-    const int z = rem / sup, y = rem - z * sup;
-    spec[((b * n + z) * n + y) * nh + kx] = res[li * n + kx];
-  }
-}
-
-// y or z pass over tiles of `lpb` consecutive kx.  AXIS 1: lines (kx, z),
-// z < other_lim, elements y; AXIS 2: lines (kx, ky), ky < other_lim,
-// elements z.  Elements >= in_lim are zero; elements < out_lim are written.
-// With green != null (AXIS 2 only) the forward transform is followed by the
-// Green multiplication and the inverse transform.
-template <typename R, int AXIS>
-__global__ void __launch_bounds__(FT) k_fft_yz(cplx_t<R> *__restrict__ spec, const R *__restrict__ green,
-                                               int n, int other_lim, int in_lim, int out_lim,
-                                               int sign, int lpb, Radices rad) {
-  typedef cplx_t<R> C;
-  C *tw = smem_base<R>();
-  C *A = tw + n, *B = A + lpb * n;
-  make_twiddles<R>(tw, n);
-  const int nh = n / 2 + 1;
-  const int ntx = (nh + lpb - 1) / lpb;
-  int64_t bid = blockIdx.x;
-  const int tx = (int)(bid % ntx);
-  bid /= ntx;
-  const int other = (int)(bid % other_lim);
-  const int64_t b = bid / other_lim;
-  const int kx0 = tx * lpb;
-  const int nl = min(lpb, nh - kx0);
-  auto addr = [&](int e, int kx) -> int64_t {
-    return AXIS == 1 ? ((b * n + other) * n + e) * nh + kx : ((b * n + e) * n + other) * nh + kx;
-  };
-  for (int t = threadIdx.x; t < nl * n; t += blockDim.x) {
-    const int e = t / nl, li = t - e * nl;
-    C v;
-    if (e < in_lim) v = spec[addr(e, kx0 + li)];
-    else { v.x = 0; v.y = 0; }
-    A[li * n + e] = v;
-  }
-  __syncthreads();
-  C *res = fft_lines<R>(A, B, tw, n, nl, rad, sign);
-  if (AXIS == 2 && green) {
-    C *other_buf = (res == A) ? B : A;
-    for (int t = threadIdx.x; t < nl * n; t += blockDim.x) {
-      const int li = t / n, e = t - li * n;
-      const R g = green[((int64_t)e * n + other) * nh + kx0 + li];
-      res[t].x *= g;
-      res[t].y *= g;
+    // stage B: DFT over s (and for CONV: Green, inverse DFT over k2, twiddle)
+    C *bB = buf0 + (parity ^ 1) * (WP * N);
+#pragma unroll
+    for (int it = 0; it < IB; ++it) {
+      const int u = threadIdx.x + it * T;
+      if (u < UB) {
+        const int li = u % W, k1 = u / W;
+        C v[N2];
+#pragma unroll
+        for (int s = 0; s < N2; ++s) v[s] = bA[li + WP * (k1 + N1 * s)];
+        dft<N2, CONV ? -1 : SIGN>(v);
+        if constexpr (CONV) {
+#pragma unroll
+          for (int k2 = 0; k2 < N2; ++k2) {
+            v[k2].x *= g[it][k2];
+            v[k2].y *= g[it][k2];
+          }
+          dft<N2, +1>(v);
+#pragma unroll
+          for (int s = 0; s < N2; ++s) bB[li + WP * (k1 + N1 * s)] = cmulc(v[s], tw[s * k1]);
+        } else {
+          if (kx0 + li < NH) {
+#pragma unroll
+            for (int k2 = 0; k2 < N2; ++k2) {
+              const int e = k1 + N1 * k2;
+              if (e < out_lim) base[(int64_t)e * estride + li] = v[k2];
+            }
+          }
+        }
+      }
     }
-    __syncthreads();
-    res = fft_lines<R>(res, other_buf, tw, n, nl, rad, +1);
-  }
-  for (int t = threadIdx.x; t < nl * out_lim; t += blockDim.x) {
-    const int e = t / nl, li = t - e * nl;
-    spec[addr(e, kx0 + li)] = res[li * n + e];
-  }
-}
-
-// x pass, c2r: lines (y,z) in [0,out)^2; out[x] = Re(line[x]) / scale for
-// x < out, written to a compact cube of side `ostride`.
-template <typename R>
-__global__ void __launch_bounds__(FT) k_fft_x_c2r(const cplx_t<R> *__restrict__ spec, R *__restrict__ out,
-                                                  int n, int olim, int lpb, int64_t nlines, R scale,
-                                                  Radices rad) {
-  typedef cplx_t<R> C;
-  C *tw = smem_base<R>();
-  C *A = tw + n, *B = A + lpb * n;
-  make_twiddles<R>(tw, n);
-  const int nh = n / 2 + 1;
-  const int64_t l0 = (int64_t)blockIdx.x * lpb;
-  const int nl = (int)(nlines - l0 < (int64_t)lpb ? nlines - l0 : (int64_t)lpb);
-  for (int t = threadIdx.x; t < nl * nh; t += blockDim.x) {
-    const int li = t / nh, kx = t - li * nh;
-    const int64_t L = l0 + li;  // (b*olim + z)*olim + y
-    const int64_t b = L / ((int64_t)olim * olim);
-    const int rem = (int)(L - b * olim * olim);
-    const int z = rem / olim, y = rem - z * olim;
-    C c = spec[((b * n + z) * n + y) * nh + kx];
-    if (kx == 0 || kx == n / 2) {
-      c.y = 0;
-      A[li * n + kx] = c;
-    } else {
-      A[li * n + kx] = c;
-      C cc;
-      cc.x = c.x;
-      cc.y = -c.y;
-      A[li * n + n - kx] = cc;
+    if constexpr (CONV) {
+      __syncthreads();
+      // stage A': inverse DFT over k1 -> element s + N2 q
+#pragma unroll
+      for (int it = 0; it < IA; ++it) {
+        const int u = threadIdx.x + it * T;
+        if (u < UA) {
+          const int li = u % W, s = u / W;
+          C v[N1];
+#pragma unroll
+          for (int k1 = 0; k1 < N1; ++k1) v[k1] = bB[li + WP * (k1 + N1 * s)];
+          dft<N1, +1>(v);
+          if (kx0 + li < NH) {
+#pragma unroll
+            for (int q = 0; q < N1; ++q) {
+              const int e = s + N2 * q;
+              if (e < out_lim) base[(int64_t)e * estride + li] = v[q];
+            }
+          }
+        }
+      }
     }
-  }
-  __syncthreads();
-  C *res = fft_lines<R>(A, B, tw, n, nl, rad, +1);
-  for (int t = threadIdx.x; t < nl * olim; t += blockDim.x) {
-    const int li = t / olim, x = t - li * olim;
-    out[(l0 + li) * olim + x] = res[li * n + x].x / scale;
+    // CONV: the next stage A writes tile `parity` only after every thread
+    // passed the barrier above, i.e. finished reading it.  Plain passes
+    // alternate the tiles instead.
+    if constexpr (!CONV) parity ^= 1;
   }
 }
 
 template <typename R>
-__global__ void k_real_to_cplx(const R *__restrict__ g, cplx_t<R> *__restrict__ spec, int64_t cnt) {
+__global__ void k_real_to_cplx(const R *__restrict__ g, cplx_t<R> *__restrict__ spec, int n, int nhp) {
+  const int nh = n / 2 + 1;
+  const int64_t cnt = (int64_t)nh * n * n;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt;
        i += (int64_t)gridDim.x * blockDim.x) {
-    cplx_t<R> c;
-    c.x = g[i];
-    c.y = 0;
-    spec[i] = c;
+    const int64_t row = i / nh;
+    const int kx = (int)(i - row * nh);
+    spec[row * nhp + kx] = mk<cplx_t<R>>(g[i], (R)0);
   }
 }
 
-template <typename R>
-int lines_per_block(int n) {
-  // two line buffers of lpb*n complex plus the twiddles within 48 KB
-  const int bytes = (int)sizeof(cplx_t<R>);
-  int lpb = (48 * 1024 / bytes - n) / (2 * n);
-  if (lpb > 16) lpb = 16;
-  return lpb < 1 ? 1 : lpb;
+template <typename K>
+int32_t allow_smem(K kernel, size_t bytes) {
+  PYFOF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return kOk;
 }
 
-template <typename R>
-size_t smem_for(int n, int lpb) {
-  return sizeof(cplx_t<R>) * (size_t)(n + 2 * lpb * n);
+// Shared-memory limits of every kernel of grid N, set once per process.
+template <typename R, int N>
+int32_t prepare() {
+  static std::once_flag once;
+  static int32_t status = kOk;
+  std::call_once(once, [] {
+    const size_t sm = smem_bytes<R, N>();
+    int32_t r = kOk;
+    if (r == kOk) r = allow_smem(k_x_r2c<R, N>, sm);
+    if (r == kOk) r = allow_smem(k_x_c2r<R, N>, sm);
+    if (r == kOk) r = allow_smem(k_lines<R, N, -1, false>, sm);
+    if (r == kOk) r = allow_smem(k_lines<R, N, +1, false>, sm);
+    if (r == kOk) r = allow_smem(k_lines<R, N, -1, true>, sm);
+    status = r;
+  });
+  return status;
+}
+
+template <typename R, int N>
+int32_t convolve_n(R *rho, cplx_t<R> *spec, const R *green, int sup, int batch, cudaStream_t s) {
+  PYFOF_TRY((prepare<R, N>()));
+  constexpr int W = kW<R>, T = Cfg<R, N>::T;
+  const int nhp = (int)spec_row<R>(N);
+  const int ntiles = nhp / W;
+  const size_t sm = smem_bytes<R, N>();
+  const int64_t bstride = (int64_t)N * N * nhp;
+  const int64_t nlines = (int64_t)batch * sup * sup;
+  k_x_r2c<R, N><<<(unsigned)ceil_div(nlines, 2 * W), T, sm, s>>>(rho, spec, sup, nhp, nlines);
+  PYFOF_CHECK_LAUNCH();
+  // y forward: lines (kx, z < sup), input y < sup, output all y
+  k_lines<R, N, -1, false><<<(unsigned)((int64_t)ntiles * sup * batch), T, sm, s>>>(
+      spec, nullptr, bstride, (int64_t)N * nhp, nhp, sup, ntiles, 1, batch, sup, N);
+  PYFOF_CHECK_LAUNCH();
+  // z: forward, Green, inverse; lines (kx, ky), input and output z < sup;
+  // halos split into chunks so that the grid fills the device
+  const int64_t per = (int64_t)ntiles * N;
+  const int nchunk = (int)std::max<int64_t>(1, std::min<int64_t>(batch, ceil_div(4 * kNumSMs, per)));
+  const int nbb = (int)ceil_div(batch, nchunk);
+  const int nchunk_used = (int)ceil_div(batch, nbb);
+  k_lines<R, N, -1, true><<<(unsigned)(per * nchunk_used), T, sm, s>>>(
+      spec, green, bstride, nhp, (int64_t)N * nhp, N, ntiles, nbb, batch, sup, sup);
+  PYFOF_CHECK_LAUNCH();
+  // y inverse: lines (kx, z < sup), input all y, output y < sup
+  k_lines<R, N, +1, false><<<(unsigned)((int64_t)ntiles * sup * batch), T, sm, s>>>(
+      spec, nullptr, bstride, (int64_t)N * nhp, nhp, sup, ntiles, 1, batch, N, sup);
+  PYFOF_CHECK_LAUNCH();
+  const R n3 = (R)((double)N * N * N);
+  k_x_c2r<R, N><<<(unsigned)ceil_div(nlines, 2 * W), T, sm, s>>>(spec, rho, sup, nhp, nlines, n3);
+  PYFOF_CHECK_LAUNCH();
+  return kOk;
+}
+
+template <typename R, int N>
+int32_t c2r_full_n(const R *green, cplx_t<R> *spec, R *out, cudaStream_t s) {
+  PYFOF_TRY((prepare<R, N>()));
+  constexpr int W = kW<R>, T = Cfg<R, N>::T;
+  const int nhp = (int)spec_row<R>(N);
+  const int ntiles = nhp / W;
+  const size_t sm = smem_bytes<R, N>();
+  const int64_t cnt = (int64_t)(N / 2 + 1) * N * N;
+  k_real_to_cplx<R><<<(unsigned)std::min<int64_t>(ceil_div(cnt, 256), 4096), 256, 0, s>>>(green, spec, N, nhp);
+  PYFOF_CHECK_LAUNCH();
+  const int64_t bstride = (int64_t)N * N * nhp;
+  // z inverse over all ky, then y inverse over all z
+  k_lines<R, N, +1, false><<<(unsigned)((int64_t)ntiles * N), T, sm, s>>>(
+      spec, nullptr, bstride, nhp, (int64_t)N * nhp, N, ntiles, 1, 1, N, N);
+  PYFOF_CHECK_LAUNCH();
+  k_lines<R, N, +1, false><<<(unsigned)((int64_t)ntiles * N), T, sm, s>>>(
+      spec, nullptr, bstride, (int64_t)N * nhp, nhp, N, ntiles, 1, 1, N, N);
+  PYFOF_CHECK_LAUNCH();
+  const int64_t nlines = (int64_t)N * N;
+  k_x_c2r<R, N><<<(unsigned)ceil_div(nlines, 2 * W), T, sm, s>>>(spec, out, N, nhp, nlines, (R)1);
+  PYFOF_CHECK_LAUNCH();
+  return kOk;
 }
 
 }  // namespace
@@ -280,65 +593,30 @@ size_t smem_for(int n, int lpb) {
 template <typename R>
 int32_t pm_convolve_batch(R *rho, cplx_t<R> *spec, const R *green, int n, int sup, int batch,
                           cudaStream_t s) {
-  const Radices rad = factor(n);
-  if (rad.nf < 0 || n > 256 || sup > n / 2 + 1) {
-    set_error("unsupported FFT size %d", n);
+  if (sup < 1 || sup > n / 2 + 1 || batch < 1) {
+    set_error("invalid convolution batch (n %d, support %d, batch %d)", n, sup, batch);
     return kInvalid;
   }
-  const int nh = n / 2 + 1;
-  const int lpb = lines_per_block<R>(n);
-  const size_t sm = smem_for<R>(n, lpb);
-  // x r2c
-  {
-    const int64_t nlines = (int64_t)batch * sup * sup;
-    k_fft_x_r2c<R><<<(unsigned)ceil_div(nlines, lpb), FT, sm, s>>>(rho, spec, n, sup, lpb, nlines, rad);
-    PYFOF_CHECK_LAUNCH();
+  switch (n) {
+    case 48: return convolve_n<R, 48>(rho, spec, green, sup, batch, s);
+    case 64: return convolve_n<R, 64>(rho, spec, green, sup, batch, s);
+    case 128: return convolve_n<R, 128>(rho, spec, green, sup, batch, s);
+    case 216: return convolve_n<R, 216>(rho, spec, green, sup, batch, s);
+    case 256: return convolve_n<R, 256>(rho, spec, green, sup, batch, s);
+    default: set_error("unsupported FFT size %d", n); return kInvalid;
   }
-  const int ntx = (nh + lpb - 1) / lpb;
-  // y forward: lines (kx, z<sup), input y<sup, output all y
-  k_fft_yz<R, 1><<<(unsigned)((int64_t)batch * sup * ntx), FT, sm, s>>>(spec, nullptr, n, sup, sup, n, -1,
-                                                                        lpb, rad);
-  PYFOF_CHECK_LAUNCH();
-  // z forward, Green multiply, z inverse: lines (kx, ky), input z<sup, output z<sup
-  k_fft_yz<R, 2><<<(unsigned)((int64_t)batch * n * ntx), FT, sm, s>>>(spec, green, n, n, sup, sup, -1, lpb,
-                                                                      rad);
-  PYFOF_CHECK_LAUNCH();
-  // y inverse: lines (kx, z<sup), input all y, output y<sup
-  k_fft_yz<R, 1><<<(unsigned)((int64_t)batch * sup * ntx), FT, sm, s>>>(spec, nullptr, n, sup, n, sup, +1,
-                                                                        lpb, rad);
-  PYFOF_CHECK_LAUNCH();
-  // x c2r into the support cube, divided by n^3
-  {
-    const int64_t nlines = (int64_t)batch * sup * sup;
-    const R n3 = (R)((double)n * n * n);
-    k_fft_x_c2r<R><<<(unsigned)ceil_div(nlines, lpb), FT, sm, s>>>(spec, rho, n, sup, lpb, nlines, n3, rad);
-    PYFOF_CHECK_LAUNCH();
-  }
-  return kOk;
 }
 
 template <typename R>
 int32_t c2r_full(const R *green, cplx_t<R> *spec, R *out, int n, cudaStream_t s) {
-  const Radices rad = factor(n);
-  if (rad.nf < 0 || n > 256) {
-    set_error("unsupported FFT size %d", n);
-    return kInvalid;
+  switch (n) {
+    case 48: return c2r_full_n<R, 48>(green, spec, out, s);
+    case 64: return c2r_full_n<R, 64>(green, spec, out, s);
+    case 128: return c2r_full_n<R, 128>(green, spec, out, s);
+    case 216: return c2r_full_n<R, 216>(green, spec, out, s);
+    case 256: return c2r_full_n<R, 256>(green, spec, out, s);
+    default: set_error("unsupported FFT size %d", n); return kInvalid;
   }
-  const int nh = n / 2 + 1;
-  const int lpb = lines_per_block<R>(n);
-  const size_t sm = smem_for<R>(n, lpb);
-  const int64_t cnt = (int64_t)nh * n * n;
-  k_real_to_cplx<R><<<(unsigned)std::min<int64_t>(ceil_div(cnt, 256), 4096), 256, 0, s>>>(green, spec, cnt);
-  PYFOF_CHECK_LAUNCH();
-  const int ntx = (nh + lpb - 1) / lpb;
-  k_fft_yz<R, 2><<<(unsigned)((int64_t)n * ntx), FT, sm, s>>>(spec, nullptr, n, n, n, n, +1, lpb, rad);
-  PYFOF_CHECK_LAUNCH();
-  k_fft_yz<R, 1><<<(unsigned)((int64_t)n * ntx), FT, sm, s>>>(spec, nullptr, n, n, n, n, +1, lpb, rad);
-  PYFOF_CHECK_LAUNCH();
-  const int64_t nlines = (int64_t)n * n;
-  k_fft_x_c2r<R><<<(unsigned)ceil_div(nlines, lpb), FT, sm, s>>>(spec, out, n, n, lpb, nlines, (R)1, rad);
-  PYFOF_CHECK_LAUNCH();
-  return kOk;
 }
 
 template int32_t pm_convolve_batch<float>(float *, float2 *, const float *, int, int, int, cudaStream_t);

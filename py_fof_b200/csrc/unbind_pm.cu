@@ -160,7 +160,7 @@ int32_t get_green(Context &ctx, int n, double soft, double range, int truncated,
   R *grid = nullptr;
   cplx_t<R> *spec = nullptr;
   PYFOF_CUDA(cudaMallocAsync(&grid, sizeof(R) * (size_t)n * n * n, s));
-  PYFOF_CUDA(cudaMallocAsync(&spec, sizeof(cplx_t<R>) * cnt, s));
+  PYFOF_CUDA(cudaMallocAsync(&spec, sizeof(cplx_t<R>) * spec_elems<R>(n), s));
   int32_t r = c2r_full<R>((const R *)t->g, spec, grid, n, s);
   if (r == kOk) {
     self_extract_kernel<R><<<1, 128, 0, s>>>(grid, n, (R *)t->self);
@@ -1233,7 +1233,7 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
       for (int h : pend) if (H[h].n == n) grp.push_back(h);
       if (grp.empty()) continue;
       const int sup = n / 2 + 1;
-      const size_t spec_bytes = sizeof(cplx_t<R>) * (size_t)(n / 2 + 1) * n * n;
+      const size_t spec_bytes = sizeof(cplx_t<R>) * (size_t)spec_elems<R>(n);
       const size_t per = spec_bytes + sizeof(R) * (size_t)sup * sup * sup;
       const int maxb = (int)std::max<size_t>(1, budget / per);
       for (size_t g0 = 0; g0 < grp.size(); g0 += maxb) {
@@ -1244,7 +1244,7 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
         if (!dslot) { set_error("workspace exhausted (slots)"); return kAlloc; }
         PYFOF_CUDA(cudaMemcpyAsync(dslot, hslot.data(), sizeof(int32_t) * nh, cudaMemcpyHostToDevice, s));
         R *rho = W.carve<R>((size_t)nb * sup * sup * sup);
-        cplx_t<R> *spec = W.carve<cplx_t<R>>((size_t)nb * (n / 2 + 1) * n * n);
+        cplx_t<R> *spec = W.carve<cplx_t<R>>((size_t)nb * spec_elems<R>(n));
         if (!rho || !spec) { set_error("workspace exhausted (PM grids)"); return kAlloc; }
         const int64_t ng = (int64_t)nb * sup * sup * sup;
         pm_zero_kernel<R><<<(unsigned)std::min<int64_t>(ceil_div(ng, BLK), 148 * 16), BLK, 0, s>>>(rho, ng);
@@ -1269,14 +1269,14 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
       if (regs.empty()) continue;
       const int nin = r == 2 ? 128 : 216;
       const int sup = nin / 2 + 1;
-      const size_t per = sizeof(cplx_t<R>) * (size_t)(nin / 2 + 1) * nin * nin + sizeof(R) * (size_t)sup * sup * sup;
+      const size_t per = sizeof(cplx_t<R>) * (size_t)spec_elems<R>(nin) + sizeof(R) * (size_t)sup * sup * sup;
       const int maxb = (int)std::max<size_t>(1, budget / per);
       const R *gin = (const R *)(r == 2 ? g_r2 : g_r4)->g;
       for (size_t g0 = 0; g0 < regs.size(); g0 += maxb) {
         const int nb = (int)std::min<size_t>(maxb, regs.size() - g0);
         int32_t *dbatch = W.carve<int32_t>(nb);
         R *rho = W.carve<R>((size_t)nb * sup * sup * sup);
-        cplx_t<R> *spec = W.carve<cplx_t<R>>((size_t)nb * (nin / 2 + 1) * nin * nin);
+        cplx_t<R> *spec = W.carve<cplx_t<R>>((size_t)nb * spec_elems<R>(nin));
         if (!dbatch || !rho || !spec) { set_error("workspace exhausted (inner grids)"); return kAlloc; }
         PYFOF_CUDA(cudaMemcpyAsync(dbatch, regs.data() + g0, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s));
         const int64_t ng = (int64_t)nb * sup * sup * sup;
