@@ -285,25 +285,46 @@ __global__ void __launch_bounds__(BLK) pm_extent_kernel(const Members m, const P
   }
 }
 
-// C2 cell key of every PM member (bound_build_cells :3166-3172)
+// C2 cell key of every PM member (bound_build_cells :3166-3172), and a sort
+// key that orders the members of a cell along a Morton curve of its
+// (2^(sb/3))^3 sub-cells.
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
+  uint32_t r = 0;
+  for (int b = 0; b < 3; ++b) r |= ((v >> b) & 1u) << (3 * b);
+  return r;
+}
+
 __global__ void pm_cellkey_kernel(const Members m, const PmHalo *__restrict__ H,
                                   const int32_t *__restrict__ mhalo, int64_t M,
-                                  uint32_t *__restrict__ key, uint32_t sentinel) {
+                                  uint32_t *__restrict__ key, uint32_t sentinel, int sb,
+                                  uint32_t *__restrict__ skey) {
+  const int sub = 1 << (sb / 3);
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
        k += (int64_t)gridDim.x * blockDim.x) {
     const int h = mhalo[k];
-    if (h < 0) { key[k] = sentinel; continue; }
+    if (h < 0) {
+      key[k] = sentinel;
+      skey[k] = sentinel << sb;
+      continue;
+    }
     const PmHalo &p = H[h];
     int64_t c[3];
+    uint32_t f[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const double u = (double)m.q[d][k] / (double)p.spacing;
-      double v = floor((u - p.u_min[d]) / p.cw_u) + 1.0;
+      const double g = (u - p.u_min[d]) / p.cw_u;
+      double v = floor(g) + 1.0;
       if (!(v >= 1.0)) v = 1.0;
       if (v > (double)p.nc[d]) v = (double)p.nc[d];
       c[d] = (int64_t)v - 1;
+      double fr = (g - (double)c[d]) * (double)sub;
+      fr = fr < 0.0 ? 0.0 : (fr > (double)(sub - 1) ? (double)(sub - 1) : fr);
+      f[d] = (uint32_t)fr;
     }
-    key[k] = (uint32_t)(p.cell_off + c[0] + (int64_t)p.nc[0] * (c[1] + (int64_t)p.nc[1] * c[2]));
+    const uint32_t cell = (uint32_t)(p.cell_off + c[0] + (int64_t)p.nc[0] * (c[1] + (int64_t)p.nc[1] * c[2]));
+    key[k] = cell;
+    skey[k] = (cell << sb) | (spread3(f[0]) | (spread3(f[1]) << 1) | (spread3(f[2]) << 2));
   }
 }
 
@@ -414,30 +435,72 @@ __device__ __forceinline__ T c2_delta(T r, T ht, T hs) {
 // units there) and the region refinement ratio for two-level halos
 // (bound_two_level_pp_full, :1088-1343).  Both are
 //     phi_i += w_j * -(a/(6 pi)) * (D(d, eps) - D(d, a_i)),  d < a_i.
-template <typename R>
-__global__ void pm_sr_kernel(const Members m, const PmHalo *__restrict__ H,
-                             const int32_t *__restrict__ mhalo, const uint8_t *__restrict__ keep,
-                             const uint8_t *__restrict__ pr, const uint32_t *__restrict__ ckey,
-                             const uint32_t *__restrict__ cstart, const uint32_t *__restrict__ cmem,
-                             int64_t M, double a_val, double app, R *__restrict__ phi_sr) {
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    const int h = mhalo[k];
-    if (h < 0 || !keep[k]) continue;
+// After a refresh the members removed since the previous pass take their
+// terms back out (bound_c2_update_incremental_cells :3490-3552,
+// bound_two_level_pp_update :1345-1498): UPDATE sums over those sources only
+// and subtracts.
+//
+// Work is organised by target chunks: a warp takes up to 32 members of one
+// C2 cell, in cell order (within a cell sorted by a Morton sub-key, so a
+// chunk is spatially compact).  Sources are scanned cell by cell in
+// coalesced batches of 32; a source enters the pair loop only if it lies
+// within the chunk's largest cutoff of the chunk's bounding box, so the
+// divergent pair arithmetic runs almost only on pairs that interact.
+struct SrChunk {
+  uint32_t cell, e0;
+};
+
+template <typename R, bool UPDATE>
+__global__ void __launch_bounds__(256) sr_gather_kernel(
+    const PmHalo *__restrict__ H, const int32_t *__restrict__ mhalo, const uint8_t *__restrict__ keep,
+    const uint8_t *__restrict__ pr, const SrChunk *__restrict__ chunks, int64_t nchunks,
+    const uint32_t *__restrict__ cstart, const uint32_t *__restrict__ cmem, const float4 *__restrict__ src4,
+    const uint32_t *__restrict__ rpos, const uint32_t *__restrict__ rsrc, double a_val, double app,
+    R *__restrict__ phi_sr) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t ch = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; ch < nchunks; ch += nw) {
+    const SrChunk C = chunks[ch];
+    const uint32_t cend = cstart[C.cell + 1];
+    const uint32_t e = C.e0 + lane;
+    const bool valid = e < cend;
+    const int64_t k = valid ? (int64_t)cmem[e] : -1;
+    const int h = mhalo[cmem[C.e0]];
     const PmHalo &p = H[h];
     if (!p.pending) continue;
+    const bool active = valid && keep[k] != 0;
+    if (!__any_sync(FULL, active)) continue;
+    float4 me = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid) me = src4[e];
     const double sp = (double)p.spacing;
-    const int ri = pr[k];
+    const int ri = active ? (int)pr[k] : 64;
     const R ai = (R)(3.5 * sp / (double)ri);
     const R a2 = ai * ai;
-    const R eps = (R)(double)(float)app;
-    const R fac = (R)(a_val / (6.0 * kPi));
-    int kk = (int)ceil((3.5 / (double)ri) / p.cw_u - 1e-9);
+    // chunk bounding box of the active targets and its largest cutoff
+    float lo[3] = {active ? me.x : 3e38f, active ? me.y : 3e38f, active ? me.z : 3e38f};
+    float hi[3] = {active ? me.x : -3e38f, active ? me.y : -3e38f, active ? me.z : -3e38f};
+    int rmin = ri;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = fminf(lo[d], __shfl_xor_sync(FULL, lo[d], o));
+        hi[d] = fmaxf(hi[d], __shfl_xor_sync(FULL, hi[d], o));
+      }
+      rmin = min(rmin, __shfl_xor_sync(FULL, rmin, o));
+    }
+    // conservative filter radius (a little above every lane's cutoff)
+    const float amax = (float)(3.5 * sp / (double)rmin) * 1.0001f + 1e-30f;
+    const float amax2 = amax * amax;
+    int kk = (int)ceil((3.5 / (double)rmin) / p.cw_u - 1e-9);
     kk = kk < 1 ? 1 : (kk > 4 ? 4 : kk);
-    const int64_t local = (int64_t)ckey[k] - p.cell_off;
+    const int64_t local = (int64_t)C.cell - p.cell_off;
     const int64_t n0 = p.nc[0], n1 = p.nc[1], n2 = p.nc[2];
     const int64_t cx = local % n0, cy = (local / n0) % n1, cz = local / (n0 * n1);
-    const float xi = m.q[0][k], yi = m.q[1][k], zi = m.q[2][k];
+    const R eps = (R)(double)(float)app;
+    const R fac = (R)(a_val / (6.0 * kPi));
+    const bool tl = p.two_level != 0;
     R acc = 0, comp = 0;
     for (int64_t z = cz - kk; z <= cz + kk; ++z) {
       if (z < 0 || z >= n2) continue;
@@ -446,91 +509,105 @@ __global__ void pm_sr_kernel(const Members m, const PmHalo *__restrict__ H,
         for (int64_t x = cx - kk; x <= cx + kk; ++x) {
           if (x < 0 || x >= n0) continue;
           const int64_t c = p.cell_off + x + n0 * (y + n1 * z);
-          for (uint32_t e = cstart[c]; e < cstart[c + 1]; ++e) {
-            const int64_t j = cmem[e];
-            if (j == k || !keep[j]) continue;
-            R dx, dy, dz;
-            if (p.two_level) {
-              dx = (R)m.q[0][j] - (R)xi; dy = (R)m.q[1][j] - (R)yi; dz = (R)m.q[2][j] - (R)zi;
-            } else {
-              dx = (R)__fsub_rn(m.q[0][j], xi); dy = (R)__fsub_rn(m.q[1][j], yi);
-              dz = (R)__fsub_rn(m.q[2][j], zi);
+          uint32_t s0 = cstart[c], s1 = cstart[c + 1];
+          if (UPDATE) {
+            s0 = rpos[s0];
+            s1 = rpos[s1];
+          }
+          for (uint32_t base = s0; base < s1; base += 32) {
+            const uint32_t t = base + lane;
+            uint32_t se = 0;
+            float4 sv = make_float4(0.f, 0.f, 0.f, 0.f);
+            bool cand = false;
+            if (t < s1) {
+              se = UPDATE ? rsrc[t] : t;
+              sv = src4[se];
+              cand = UPDATE || keep[cmem[se]] != 0;
+              const float bx = fmaxf(fmaxf(lo[0] - sv.x, sv.x - hi[0]), 0.f);
+              const float by = fmaxf(fmaxf(lo[1] - sv.y, sv.y - hi[1]), 0.f);
+              const float bz = fmaxf(fmaxf(lo[2] - sv.z, sv.z - hi[2]), 0.f);
+              cand = cand && (bx * bx + by * by + bz * bz <= amax2);
             }
-            const R r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 < a2) {
-              const R d = sqrt(r2);
-              const R dphi = -(fac * (depth_c<R>(d, eps) - depth_c<R>(d, ai)));
-              const R yv = (R)m.w[j] * dphi - comp;
-              const R t = acc + yv;
-              comp = (t - acc) - yv;
-              acc = t;
+            unsigned mask = __ballot_sync(FULL, cand);
+            while (mask) {
+              const int bl = __ffs(mask) - 1;
+              mask &= mask - 1;
+              const float jx = __shfl_sync(FULL, sv.x, bl), jy = __shfl_sync(FULL, sv.y, bl);
+              const float jz = __shfl_sync(FULL, sv.z, bl), jw = __shfl_sync(FULL, sv.w, bl);
+              const uint32_t je = __shfl_sync(FULL, se, bl);
+              if (active && je != e) {
+                R dx, dy, dz;
+                if (tl) {
+                  dx = (R)jx - (R)me.x; dy = (R)jy - (R)me.y; dz = (R)jz - (R)me.z;
+                } else {
+                  dx = (R)__fsub_rn(jx, me.x); dy = (R)__fsub_rn(jy, me.y); dz = (R)__fsub_rn(jz, me.z);
+                }
+                const R r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 < a2) {
+                  const R d = sqrt(r2);
+                  const R dphi = -(fac * (depth_c<R>(d, eps) - depth_c<R>(d, ai)));
+                  const R yv = (R)jw * dphi - comp;
+                  const R tt = acc + yv;
+                  comp = (tt - acc) - yv;
+                  acc = tt;
+                }
+              }
             }
           }
         }
       }
     }
-    phi_sr[k] = acc;
+    if (active) {
+      if (UPDATE) phi_sr[k] -= acc;
+      else phi_sr[k] = acc;
+    }
   }
 }
 
-// Incremental short-range update after a refresh (bound_c2_update_
-// incremental_cells :3490-3552, bound_two_level_pp_update :1345-1498): every
-// member removed since the previous pass takes its pair terms back out of the
-// kept members within their cutoff.  jd[k] marks such members and is cleared.
-template <typename R>
-__global__ void pm_sr_update_kernel(const Members m, const PmHalo *__restrict__ H,
-                                    const int32_t *__restrict__ mhalo, const uint8_t *__restrict__ keep,
-                                    uint8_t *__restrict__ jd, const uint8_t *__restrict__ pr,
-                                    const uint32_t *__restrict__ ckey, const uint32_t *__restrict__ cstart,
-                                    const uint32_t *__restrict__ cmem, int64_t M, double a_val, double app,
-                                    R *__restrict__ phi_sr) {
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    if (!jd[k]) continue;
-    jd[k] = 0;
-    const int h = mhalo[k];
-    if (h < 0) continue;
-    const PmHalo &p = H[h];
-    if (!p.pending) continue;
-    const double sp = (double)p.spacing;
-    const R eps = (R)(double)(float)app;
-    const R fac = (R)(a_val / (6.0 * kPi));
-    int kk = p.two_level ? (int)ceil(3.5 / p.cw_u - 1e-9) : 1;
-    kk = kk < 1 ? 1 : (kk > 4 ? 4 : kk);
-    const int64_t local = (int64_t)ckey[k] - p.cell_off;
-    const int64_t n0 = p.nc[0], n1 = p.nc[1], n2 = p.nc[2];
-    const int64_t cx = local % n0, cy = (local / n0) % n1, cz = local / (n0 * n1);
-    const float xj = m.q[0][k], yj = m.q[1][k], zj = m.q[2][k];
-    const R wj = (R)m.w[k];
-    for (int64_t z = cz - kk; z <= cz + kk; ++z) {
-      if (z < 0 || z >= n2) continue;
-      for (int64_t y = cy - kk; y <= cy + kk; ++y) {
-        if (y < 0 || y >= n1) continue;
-        for (int64_t x = cx - kk; x <= cx + kk; ++x) {
-          if (x < 0 || x >= n0) continue;
-          const int64_t c = p.cell_off + x + n0 * (y + n1 * z);
-          for (uint32_t e = cstart[c]; e < cstart[c + 1]; ++e) {
-            const int64_t i = cmem[e];
-            if (i == k || !keep[i]) continue;
-            const R ai = (R)(3.5 * sp / (double)pr[i]);
-            R dx, dy, dz;
-            if (p.two_level) {
-              dx = (R)m.q[0][i] - (R)xj; dy = (R)m.q[1][i] - (R)yj; dz = (R)m.q[2][i] - (R)zj;
-            } else {
-              dx = (R)__fsub_rn(m.q[0][i], xj); dy = (R)__fsub_rn(m.q[1][i], yj);
-              dz = (R)__fsub_rn(m.q[2][i], zj);
-            }
-            const R r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 < ai * ai) {
-              const R d = sqrt(r2);
-              const R dphi = -(fac * (depth_c<R>(d, eps) - depth_c<R>(d, ai)));
-              atomicAdd(&phi_sr[i], -wj * dphi);
-            }
-          }
-        }
-      }
-    }
+// Cell-ordered copy of the members' positions and weights.
+__global__ void sr_pack_kernel(const Members m, const uint32_t *__restrict__ cmem, int64_t n,
+                               float4 *__restrict__ src4) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = cmem[e];
+    src4[e] = make_float4(m.q[0][k], m.q[1][k], m.q[2][k], m.w[k]);
   }
+}
+
+// Target chunks: ceil(members / 32) per cell.
+__global__ void sr_chunk_count_kernel(const uint32_t *__restrict__ cstart, int64_t ncell,
+                                      uint32_t *__restrict__ cnt) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncell;
+       c += (int64_t)gridDim.x * blockDim.x)
+    cnt[c] = (cstart[c + 1] - cstart[c] + 31u) / 32u;
+}
+
+__global__ void sr_chunk_fill_kernel(const uint32_t *__restrict__ cstart, const uint32_t *__restrict__ coff,
+                                     int64_t ncell, SrChunk *__restrict__ chunks) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncell;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t n = (cstart[c + 1] - cstart[c] + 31u) / 32u;
+    for (uint32_t i = 0; i < n; ++i) chunks[coff[c] + i] = SrChunk{(uint32_t)c, cstart[c] + 32u * i};
+  }
+}
+
+// Members removed since the previous pass, in cell order: flag (and clear
+// the removal mark) per cell-ordered position.
+__global__ void sr_removed_flag_kernel(const uint32_t *__restrict__ cmem, int64_t n, uint8_t *__restrict__ jd,
+                                       uint32_t *__restrict__ flag) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = cmem[e];
+    flag[e] = jd[k];
+    jd[k] = 0;
+  }
+}
+
+__global__ void sr_removed_fill_kernel(const uint32_t *__restrict__ flag, const uint32_t *__restrict__ rpos,
+                                       int64_t n, uint32_t *__restrict__ rsrc) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x)
+    if (flag[e]) rsrc[rpos[e]] = (uint32_t)e;
 }
 
 // ---------------------------------------------------------------- two-level
@@ -1134,14 +1211,45 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
            *vb = W.carve<uint32_t>(M);
   if (!ckey || !cstart || !ka || !va || !kb || !vb) { set_error("workspace exhausted (C2 cells)"); return kAlloc; }
   const uint32_t sentinel = (uint32_t)ncell;
-  pm_cellkey_kernel<<<gM, BLK, 0, s>>>(m, dH, mhalo, M, ckey, sentinel);
+  // Morton sub-key bits inside a cell (a multiple of 3, the key within 32 bits)
+  const int sb = std::max(0, std::min(9, 32 - bits_for((uint64_t)ncell))) / 3 * 3;
+  uint32_t *skey = W.carve<uint32_t>(M);
+  if (!skey) { set_error("workspace exhausted (C2 cells)"); return kAlloc; }
+  pm_cellkey_kernel<<<gM, BLK, 0, s>>>(m, dH, mhalo, M, ckey, sentinel, sb, skey);
   PYFOF_CHECK_LAUNCH();
   PYFOF_CUDA(cudaMemsetAsync(cstart, 0, sizeof(uint32_t) * (ncell + 2), s));
   pm_cellcount_kernel<<<gM, BLK, 0, s>>>(ckey, M, sentinel, cstart);
   PYFOF_CHECK_LAUNCH();
   PYFOF_TRY(exclusive_scan_u32(cstart, cstart, ncell + 1, nullptr, W, s));
   uint32_t *sk, *cmem;
-  PYFOF_TRY(radix_sort_pairs(ckey, nullptr, M, bits_for((uint64_t)ncell), ka, va, kb, vb, &sk, &cmem, W, s));
+  PYFOF_TRY(radix_sort_pairs(skey, nullptr, M, bits_for((uint64_t)sentinel << sb), ka, va, kb, vb, &sk, &cmem,
+                             W, s));
+  // cell-ordered positions and weights, target chunks, removal lists
+  uint32_t npm = 0;
+  PYFOF_CUDA(cudaMemcpyAsync(&npm, cstart + ncell, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  uint32_t *chcnt = W.carve<uint32_t>(ncell + 1);
+  if (!chcnt) { set_error("workspace exhausted (C2 chunks)"); return kAlloc; }
+  PYFOF_CUDA(cudaMemsetAsync(chcnt, 0, sizeof(uint32_t) * (ncell + 1), s));
+  const unsigned gC = (unsigned)std::min<int64_t>(ceil_div(std::max<int64_t>(ncell, 1), BLK), 148 * 16);
+  sr_chunk_count_kernel<<<gC, BLK, 0, s>>>(cstart, ncell, chcnt);
+  PYFOF_CHECK_LAUNCH();
+  PYFOF_TRY(exclusive_scan_u32(chcnt, chcnt, ncell + 1, nullptr, W, s));
+  uint32_t nchunk = 0;
+  PYFOF_CUDA(cudaMemcpyAsync(&nchunk, chcnt + ncell, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaStreamSynchronize(s));
+  float4 *src4 = W.carve<float4>(std::max<uint32_t>(npm, 1));
+  SrChunk *chunks = W.carve<SrChunk>(std::max<uint32_t>(nchunk, 1));
+  uint32_t *rflag = W.carve<uint32_t>((size_t)npm + 1), *rpos = W.carve<uint32_t>((size_t)npm + 1);
+  uint32_t *rsrc = W.carve<uint32_t>(std::max<uint32_t>(npm, 1));
+  if (!src4 || !chunks || !rflag || !rpos || !rsrc) { set_error("workspace exhausted (C2 sources)"); return kAlloc; }
+  PYFOF_CUDA(cudaMemsetAsync(rflag, 0, sizeof(uint32_t) * ((size_t)npm + 1), s));
+  const unsigned gP = (unsigned)std::min<int64_t>(ceil_div(std::max<uint32_t>(npm, 1), BLK), 148 * 16);
+  sr_pack_kernel<<<gP, BLK, 0, s>>>(m, cmem, npm, src4);
+  PYFOF_CHECK_LAUNCH();
+  sr_chunk_fill_kernel<<<gC, BLK, 0, s>>>(cstart, chcnt, ncell, chunks);
+  PYFOF_CHECK_LAUNCH();
+  const unsigned gS = (unsigned)std::min<int64_t>(ceil_div((int64_t)std::max<uint32_t>(nchunk, 1) * 32, 256),
+                                                  148 * 32);
   // per-member refinement ratio, refined-region sources and targets
   const int na = (int)act.size();
   uint8_t *pr = W.carve<uint8_t>(M);
@@ -1294,12 +1402,20 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
         PYFOF_CHECK_LAUNCH();
       }
     }
-    if (pass == 1)
-      pm_sr_kernel<R><<<gM, BLK, 0, s>>>(m, dH, mhalo, keep, pr, ckey, cstart, cmem, M, a.a_val, a.softening, c2);
-    else
-      pm_sr_update_kernel<R><<<gM, BLK, 0, s>>>(m, dH, mhalo, keep, jd, pr, ckey, cstart, cmem, M, a.a_val,
-                                                a.softening, c2);
-    PYFOF_CHECK_LAUNCH();
+    if (pass == 1) {
+      sr_gather_kernel<R, false><<<gS, 256, 0, s>>>(dH, mhalo, keep, pr, chunks, nchunk, cstart, cmem, src4,
+                                                    nullptr, nullptr, a.a_val, a.softening, c2);
+      PYFOF_CHECK_LAUNCH();
+    } else {
+      sr_removed_flag_kernel<<<gP, BLK, 0, s>>>(cmem, npm, jd, rflag);
+      PYFOF_CHECK_LAUNCH();
+      PYFOF_TRY(exclusive_scan_u32(rflag, rpos, (int64_t)npm + 1, nullptr, W, s));
+      sr_removed_fill_kernel<<<gP, BLK, 0, s>>>(rflag, rpos, npm, rsrc);
+      PYFOF_CHECK_LAUNCH();
+      sr_gather_kernel<R, true><<<gS, 256, 0, s>>>(dH, mhalo, keep, pr, chunks, nchunk, cstart, cmem, src4,
+                                                   rpos, rsrc, a.a_val, a.softening, c2);
+      PYFOF_CHECK_LAUNCH();
+    }
     pm_inner_kernel<R><<<(unsigned)pend.size(), IBLK, 0, s>>>(m, dH, dpend, (int)pend.size(), keep, jd, c1, phi_in, c2, phi,
                                                            en, (float)a.b_val, a.np_halo_min, phi_only,
                                                            ctx.d_flags);
