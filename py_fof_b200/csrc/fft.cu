@@ -262,84 +262,89 @@ __device__ __forceinline__ void stage_b_smem(const cplx_t<R> *src, cplx_t<R> *ds
 
 // ------------------------------------------------------------------ kernels
 
-// x pass, forward r2c.  Real lines L = (b*sup + z)*sup + y, x < sup, are
-// taken in pairs as one complex line (a + i b); the two half spectra are
-// separated with the Hermitian symmetry of real transforms.
+// x pass, forward r2c.  Real lines L = (b*SUP + z)*SUP + y, x < SUP
+// (SUP = N/2 + 1), are taken in pairs as one complex line (a + i b); the two
+// half spectra are separated with the Hermitian symmetry of real
+// transforms.  All loops have compile-time trip counts, so every thread
+// issues its loads before the first one returns.
 template <typename R, int N>
 __global__ void __launch_bounds__(Cfg<R, N>::T) k_x_r2c(const R *__restrict__ rho, cplx_t<R> *__restrict__ spec,
-                                                        int sup, int nhp, int64_t nlines) {
+                                                        int nhp, int nlines) {
   using C = cplx_t<R>;
-  constexpr int T = Cfg<R, N>::T, W = kW<R>, WP = W + 1, NH = N / 2 + 1;
+  constexpr int T = Cfg<R, N>::T, W = kW<R>, WP = W + 1, NH = N / 2 + 1, SUP = N / 2 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *tw = reinterpret_cast<C *>(smem_raw);
   C *t0 = tw + N, *t1 = t0 + WP * N;
   load_twiddles<R, N, T>(tw);
-  const int64_t L0 = (int64_t)blockIdx.x * (2 * W);
-  for (int p = 0; p < W; ++p) {
-    const int64_t La = L0 + 2 * p, Lb = La + 1;
-    for (int x = threadIdx.x; x < sup; x += T) {
-      const R a = La < nlines ? rho[La * sup + x] : (R)0;
-      const R b = Lb < nlines ? rho[Lb * sup + x] : (R)0;
-      t0[p + WP * x] = mk<C>(a, b);
+  const int L0 = blockIdx.x * (2 * W);
+  const int nl = min(2 * W, nlines - L0);
+  const R *src = rho + (int64_t)L0 * SUP;
+#pragma unroll
+  for (int it = 0; it < (W * SUP + T - 1) / T; ++it) {
+    const int idx = threadIdx.x + it * T;
+    if (idx < W * SUP) {
+      const int p = idx / SUP, x = idx - p * SUP;
+      const R va = 2 * p < nl ? src[(2 * p) * SUP + x] : (R)0;
+      const R vb = 2 * p + 1 < nl ? src[(2 * p + 1) * SUP + x] : (R)0;
+      t0[p + WP * x] = mk<C>(va, vb);
     }
   }
   __syncthreads();
-  stage_a_smem<R, N, -1>(t0, t1, tw, sup);
+  stage_a_smem<R, N, -1>(t0, t1, tw, SUP);
   __syncthreads();
   stage_b_smem<R, N, -1>(t1, t0);
   __syncthreads();
-  const int64_t ss = (int64_t)sup * sup;
-  for (int p = 0; p < W; ++p) {
-    const int64_t La = L0 + 2 * p;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int64_t L = La + h;
-      if (L >= nlines) break;
-      const int64_t b = L / ss;
-      const int64_t rem = L - b * ss;
-      const int64_t z = rem / sup, y = rem - z * sup;
-      C *row = spec + ((b * N + z) * N + y) * nhp;
-      for (int kx = threadIdx.x; kx < NH; kx += T) {
-        const C zk = t0[p + WP * kx];
-        const C zm = t0[p + WP * ((N - kx) % N)];
-        C out;
-        if (h == 0) out = mk<C>((R)0.5 * (zk.x + zm.x), (R)0.5 * (zk.y - zm.y));
-        else out = mk<C>((R)0.5 * (zk.y + zm.y), (R)0.5 * (zm.x - zk.x));
-        row[kx] = out;
-      }
+  for (int it = 0; it < (2 * W * NH + T - 1) / T; ++it) {
+    const int idx = threadIdx.x + it * T;
+    const int lr = idx / NH, kx = idx - lr * NH;
+    if (lr < nl) {
+      const int L = L0 + lr, p = lr >> 1;
+      const int b = L / (SUP * SUP), rem = L - b * (SUP * SUP);
+      const int z = rem / SUP, y = rem - z * SUP;
+      const C zk = t0[p + WP * kx];
+      const C zm = t0[p + WP * ((N - kx) % N)];
+      C out;
+      if ((lr & 1) == 0) out = mk<C>((R)0.5 * (zk.x + zm.x), (R)0.5 * (zk.y - zm.y));
+      else out = mk<C>((R)0.5 * (zk.y + zm.y), (R)0.5 * (zm.x - zk.x));
+      spec[(((int64_t)b * N + z) * N + y) * nhp + kx] = out;
     }
   }
 }
 
-// x pass, c2r into compact cubes of side olim: lines L = (b*olim + z)*olim
-// + y, out[L*olim + x] = x-th real value / scale.  Two Hermitian half
+// x pass, c2r into compact cubes of side OLIM: lines L = (b*OLIM + z)*OLIM
+// + y, out[L*OLIM + x] = x-th real value / scale.  Two Hermitian half
 // spectra become one complex line (a + i b); only the real parts of the DC
 // and Nyquist bins are used.
-template <typename R, int N>
+template <typename R, int N, int OLIM>
 __global__ void __launch_bounds__(Cfg<R, N>::T) k_x_c2r(const cplx_t<R> *__restrict__ spec, R *__restrict__ out,
-                                                        int olim, int nhp, int64_t nlines, R scale) {
+                                                        int nhp, int nlines, R scale) {
   using C = cplx_t<R>;
   constexpr int T = Cfg<R, N>::T, W = kW<R>, WP = W + 1, NH = N / 2 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *tw = reinterpret_cast<C *>(smem_raw);
   C *t0 = tw + N, *t1 = t0 + WP * N;
   load_twiddles<R, N, T>(tw);
-  const int64_t L0 = (int64_t)blockIdx.x * (2 * W);
-  const int64_t oo = (int64_t)olim * olim;
-  for (int p = 0; p < W; ++p) {
-    const int64_t La = L0 + 2 * p, Lb = La + 1;
-    const C *ra = nullptr, *rb = nullptr;
-    if (La < nlines) {
-      const int64_t b = La / oo, rem = La - b * oo, z = rem / olim, y = rem - z * olim;
-      ra = spec + ((b * N + z) * N + y) * nhp;
-    }
-    if (Lb < nlines) {
-      const int64_t b = Lb / oo, rem = Lb - b * oo, z = rem / olim, y = rem - z * olim;
-      rb = spec + ((b * N + z) * N + y) * nhp;
-    }
-    for (int kx = threadIdx.x; kx < NH; kx += T) {
-      C a = ra ? ra[kx] : mk<C>(0, 0);
-      C b = rb ? rb[kx] : mk<C>(0, 0);
+  const int L0 = blockIdx.x * (2 * W);
+  const int nl = min(2 * W, nlines - L0);
+#pragma unroll
+  for (int it = 0; it < (W * NH + T - 1) / T; ++it) {
+    const int idx = threadIdx.x + it * T;
+    if (idx < W * NH) {
+      const int p = idx / NH, kx = idx - p * NH;
+      C a = mk<C>(0, 0), b = mk<C>(0, 0);
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
+        const int lr = 2 * p + hh;
+        if (lr < nl) {
+          const int L = L0 + lr;
+          const int bb = L / (OLIM * OLIM), rem = L - bb * (OLIM * OLIM);
+          const int z = rem / OLIM, y = rem - z * OLIM;
+          const C v = spec[(((int64_t)bb * N + z) * N + y) * nhp + kx];
+          if (hh == 0) a = v;
+          else b = v;
+        }
+      }
       if (kx == 0 || kx == N / 2) {
         a.y = 0;
         b.y = 0;
@@ -353,16 +358,15 @@ __global__ void __launch_bounds__(Cfg<R, N>::T) k_x_c2r(const cplx_t<R> *__restr
   __syncthreads();
   stage_b_smem<R, N, +1>(t1, t0);
   __syncthreads();
-  for (int p = 0; p < W; ++p) {
-    const int64_t La = L0 + 2 * p;
+  R *dst = out + (int64_t)L0 * OLIM;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int64_t L = La + h;
-      if (L >= nlines) break;
-      for (int x = threadIdx.x; x < olim; x += T) {
-        const C v = t0[p + WP * x];
-        out[L * olim + x] = (h == 0 ? v.x : v.y) / scale;
-      }
+  for (int it = 0; it < (W * OLIM + T - 1) / T; ++it) {
+    const int idx = threadIdx.x + it * T;
+    if (idx < W * OLIM) {
+      const int p = idx / OLIM, x = idx - p * OLIM;
+      const C v = t0[p + WP * x];
+      if (2 * p < nl) dst[(2 * p) * OLIM + x] = v.x / scale;
+      if (2 * p + 1 < nl) dst[(2 * p + 1) * OLIM + x] = v.y / scale;
     }
   }
 }
@@ -521,7 +525,8 @@ int32_t prepare() {
     const size_t sm = smem_bytes<R, N>();
     int32_t r = kOk;
     if (r == kOk) r = allow_smem(k_x_r2c<R, N>, sm);
-    if (r == kOk) r = allow_smem(k_x_c2r<R, N>, sm);
+    if (r == kOk) r = allow_smem(k_x_c2r<R, N, N / 2 + 1>, sm);
+    if (r == kOk) r = allow_smem(k_x_c2r<R, N, N>, sm);
     if (r == kOk) r = allow_smem(k_lines<R, N, -1, false>, sm);
     if (r == kOk) r = allow_smem(k_lines<R, N, +1, false>, sm);
     if (r == kOk) r = allow_smem(k_lines<R, N, -1, true>, sm);
@@ -539,7 +544,7 @@ int32_t convolve_n(R *rho, cplx_t<R> *spec, const R *green, int sup, int batch, 
   const size_t sm = smem_bytes<R, N>();
   const int64_t bstride = (int64_t)N * N * nhp;
   const int64_t nlines = (int64_t)batch * sup * sup;
-  k_x_r2c<R, N><<<(unsigned)ceil_div(nlines, 2 * W), T, sm, s>>>(rho, spec, sup, nhp, nlines);
+  k_x_r2c<R, N><<<(unsigned)ceil_div(nlines, 2 * W), T, sm, s>>>(rho, spec, nhp, (int)nlines);
   PYFOF_CHECK_LAUNCH();
   // y forward: lines (kx, z < sup), input y < sup, output all y
   k_lines<R, N, -1, false><<<(unsigned)((int64_t)ntiles * sup * batch), T, sm, s>>>(
@@ -559,7 +564,7 @@ int32_t convolve_n(R *rho, cplx_t<R> *spec, const R *green, int sup, int batch, 
       spec, nullptr, bstride, (int64_t)N * nhp, nhp, sup, ntiles, 1, batch, N, sup);
   PYFOF_CHECK_LAUNCH();
   const R n3 = (R)((double)N * N * N);
-  k_x_c2r<R, N><<<(unsigned)ceil_div(nlines, 2 * W), T, sm, s>>>(spec, rho, sup, nhp, nlines, n3);
+  k_x_c2r<R, N, N / 2 + 1><<<(unsigned)ceil_div(nlines, 2 * W), T, sm, s>>>(spec, rho, nhp, (int)nlines, n3);
   PYFOF_CHECK_LAUNCH();
   return kOk;
 }
@@ -583,7 +588,7 @@ int32_t c2r_full_n(const R *green, cplx_t<R> *spec, R *out, cudaStream_t s) {
       spec, nullptr, bstride, (int64_t)N * nhp, nhp, N, ntiles, 1, 1, N, N);
   PYFOF_CHECK_LAUNCH();
   const int64_t nlines = (int64_t)N * N;
-  k_x_c2r<R, N><<<(unsigned)ceil_div(nlines, 2 * W), T, sm, s>>>(spec, out, N, nhp, nlines, (R)1);
+  k_x_c2r<R, N, N><<<(unsigned)ceil_div(nlines, 2 * W), T, sm, s>>>(spec, out, nhp, (int)nlines, (R)1);
   PYFOF_CHECK_LAUNCH();
   return kOk;
 }
@@ -593,7 +598,7 @@ int32_t c2r_full_n(const R *green, cplx_t<R> *spec, R *out, cudaStream_t s) {
 template <typename R>
 int32_t pm_convolve_batch(R *rho, cplx_t<R> *spec, const R *green, int n, int sup, int batch,
                           cudaStream_t s) {
-  if (sup < 1 || sup > n / 2 + 1 || batch < 1) {
+  if (sup != n / 2 + 1 || batch < 1 || (int64_t)batch * sup * sup >= (int64_t)1 << 30) {
     set_error("invalid convolution batch (n %d, support %d, batch %d)", n, sup, batch);
     return kInvalid;
   }
