@@ -117,8 +117,14 @@ int32_t pyfof_halo_potential_direct_static(const float *q, const float *w, int32
  *   mp        (total_np) float64, NULL means unit masses
  *   np_halo   (nhalo) particle count of every input region
  *   in_halo, halo_id  (total_np) int32 outputs; ang_mom (3,nhalo) float64
- *             Fortran order (ang_mom[3*h+d]) output
- * Returns ierr. */
+ *             Fortran order (ang_mom[3*h+d]) output; all three are written
+ *             in full on success and zeroed on failure
+ * Returns ierr: the reference codes (0 ok, 1 invalid input, 2 span above
+ * s_15, 3 allocation, 4 non-finite, 10 n_threads > 256), plus 5 when a mass
+ * is not positive and finite (the reference raises that in Python before
+ * its call, py_fof/__init__.py:259-260; here the device checks it) and 20
+ * for a CUDA failure (pyfof_last_error has the detail).  Positions are
+ * copied first; velocity and mass copies overlap with the linking. */
 int32_t pyfof_run(const double *xp, const double *vp, const double *mp, int32_t layout,
                   const int32_t *np_halo, int32_t nhalo, int64_t total_np, double L_Box,
                   double linking_length, int32_t np_halo_min, int32_t bound_check,

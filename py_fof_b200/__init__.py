@@ -49,6 +49,9 @@ class FofCall:
         return vp, mp
 
 
+_MASS_ERROR = "All particle masses in mp_list must be positive and finite"
+
+
 def _as_3n(xp_list_norm):
     if len(xp_list_norm) == 1:
         x = xp_list_norm[0]
@@ -61,10 +64,14 @@ def _as_3n(xp_list_norm):
 def _prepare(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2, np_halo_min=10,
              bound_check=False, verbose=0, return_ang_mom=False, n_threads=None, mp_list=None,
              softening=None, z=0.0, box=300.0, h0=0.67, omega_m=0.3, omega_l=0.7, n_sim=None,
-             units='cube', include_hubble_flow=False, ng=None, ng_global=None):
+             units='cube', include_hubble_flow=False, ng=None, ng_global=None,
+             check_masses=True):
     """Validation and unit conversion of _fof_core (py_fof/__init__.py:168-329).
 
     Returns either a FofCall or, for total_np == 0, the final empty result.
+    With check_masses=False the per-particle mass check (positive and
+    finite) is left to the native library, which runs it on the device and
+    reports it as ierr 5; _finish raises the same ValueError for it.
     """
     if units not in ('cube', 'physical'):
         raise ValueError(f"units must be 'cube' or 'physical', got '{units}'")
@@ -146,8 +153,8 @@ def _prepare(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2, np_halo_min
         else:
             raise ValueError("Unsupported mp_list type")
 
-        if not np.all(np.isfinite(mp_raw)) or not np.all(mp_raw > 0):
-            raise ValueError("All particle masses in mp_list must be positive and finite")
+        if check_masses and (not np.all(np.isfinite(mp_raw)) or not np.all(mp_raw > 0)):
+            raise ValueError(_MASS_ERROR)
 
     z_val = float(z)
     if 1.0 + z_val <= 0.0:
@@ -226,6 +233,8 @@ def _finish(call: FofCall, in_halo_out, halo_id_out, ang_mom_out, ierr):
             raise ValueError("Candidate halo span exceeds 15 Mpc limit (s_15)")
         elif ierr == 4:
             raise ValueError("Non-finite values (NaN/Inf) encountered during calculation")
+        elif ierr == 5:
+            raise ValueError(_MASS_ERROR)
         elif ierr == 10:
             raise ValueError("n_threads exceeds maximum supported slots (256)")
         else:
@@ -256,7 +265,8 @@ def _fof_core(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2,
                     return_ang_mom=return_ang_mom, n_threads=n_threads, mp_list=mp_list,
                     softening=softening, z=z, box=box, h0=h0, omega_m=omega_m,
                     omega_l=omega_l, n_sim=n_sim, units=units,
-                    include_hubble_flow=include_hubble_flow, ng=ng, ng_global=ng_global)
+                    include_hubble_flow=include_hubble_flow, ng=ng, ng_global=ng_global,
+                    check_masses=False)
     if not isinstance(call, FofCall):
         return call
     in_halo, halo_id, ang_mom, ierr = _native_call(call)

@@ -153,8 +153,9 @@ def run(xp, vp, mp, np_halo, nhalo, L_Box, link, np_halo_min, bound_check, verbo
     if mp is not None:
         mp = np.ascontiguousarray(mp, dtype=np.float64)
     nph = np.ascontiguousarray(np_halo, dtype=np.int32)
-    in_halo = np.zeros(n, dtype=np.int32)
-    halo_id = np.zeros(n, dtype=np.int32)
+    # written in full by the library (zeros on every failure path)
+    in_halo = np.empty(n, dtype=np.int32)
+    halo_id = np.empty(n, dtype=np.int32)
     ang_mom = np.zeros((3, max(int(nhalo), 0)), dtype=np.float64, order="F")
     ierr = L.pyfof_run(_ptr(xp), _ptr(vp), _ptr(mp), layout, nph.ctypes.data_as(_i32p),
                        int(nhalo), n, float(L_Box), float(link), int(np_halo_min),

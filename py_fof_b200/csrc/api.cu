@@ -41,6 +41,9 @@ Context::~Context() {
     cudaStreamSynchronize(stream);
   }
   if (own_stream) cudaStreamDestroy(own_stream);
+  if (aux_stream) cudaStreamDestroy(aux_stream);
+  if (ev_alloc) cudaEventDestroy(ev_alloc);
+  if (ev_inputs) cudaEventDestroy(ev_inputs);
   for (auto &e : ev) if (e) cudaEventDestroy(e);
   if (d_flags) cudaFree(d_flags);
   if (h_flags) cudaFreeHost(h_flags);
@@ -67,6 +70,9 @@ int32_t get_context(int device, Context **out) {
     PYFOF_CUDA(cudaMalloc(&c->d_flags, sizeof(int32_t) * FLAG_COUNT));
     PYFOF_CUDA(cudaMallocHost(&c->h_flags, sizeof(int32_t) * FLAG_COUNT));
     for (auto &e : c->ev) PYFOF_CUDA(cudaEventCreate(&e));
+    PYFOF_CUDA(cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking));
+    PYFOF_CUDA(cudaEventCreateWithFlags(&c->ev_alloc, cudaEventDisableTiming));
+    PYFOF_CUDA(cudaEventCreateWithFlags(&c->ev_inputs, cudaEventDisableTiming));
     cudaMemPool_t pool;
     PYFOF_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
     uint64_t thr = UINT64_MAX;  // keep freed blocks cached in the pool
@@ -254,28 +260,15 @@ int32_t pyfof_halo_potential(const float *q, const float *w, int32_t np, double 
   return r;
 }
 
-int32_t pyfof_run(const double *xp, const double *vp, const double *mp, int32_t layout,
-                  const int32_t *np_halo, int32_t nhalo, int64_t total_np, double L_Box,
-                  double linking_length, int32_t np_halo_min, int32_t bound_check,
-                  int32_t verbose, double softening, double a_val, double b_val,
-                  double s_15_val, int32_t n_threads, int64_t ng_val, double ng_global_val,
-                  int32_t *in_halo, int32_t *halo_id, double *ang_mom) {
-  if (total_np > 0) {
-    if (in_halo) std::memset(in_halo, 0, sizeof(int32_t) * (size_t)total_np);
-    if (halo_id) std::memset(halo_id, 0, sizeof(int32_t) * (size_t)total_np);
-  }
-  if (ang_mom && nhalo > 0) std::memset(ang_mom, 0, sizeof(double) * 3 * (size_t)nhalo);
-  int32_t r = validate(nhalo, total_np, np_halo, n_threads);
-  if (r != kOk) return r;
-  if (nhalo <= 0 || total_np <= 0) return kOk;
-  if (!xp || !in_halo || !halo_id || !ang_mom) {
-    set_error("null argument");
-    return kInvalid;
-  }
-  if (bound_check && !vp) {
-    set_error("vp is required when bound_check is set");
-    return kInvalid;
-  }
+// Host-memory call.  Positions are copied first on the call's stream; the
+// velocities and masses follow on the context's second stream and are
+// waited for only after the linking, so their copies overlap with it.
+static int32_t run_host(const double *xp, const double *vp, const double *mp, int32_t layout,
+                        const int32_t *np_halo, int32_t nhalo, int64_t total_np, double L_Box,
+                        double linking_length, int32_t np_halo_min, int32_t bound_check,
+                        int32_t verbose, double softening, double a_val, double b_val,
+                        double s_15_val, int32_t n_threads, int64_t ng_val, double ng_global_val,
+                        int32_t *in_halo, int32_t *halo_id, double *ang_mom) {
   Context *cp;
   PYFOF_TRY(get_context(g_default_device, &cp));
   Context &ctx = *cp;
@@ -294,10 +287,22 @@ int32_t pyfof_run(const double *xp, const double *vp, const double *mp, int32_t 
     set_error("device allocation failed for %zu particles", n);
     return kAlloc;
   }
+  const bool side = vp || mp;
+  if (side) {
+    // the buffers were allocated in the order of stream s
+    PYFOF_CUDA(cudaEventRecord(ctx.ev_alloc, s));
+    PYFOF_CUDA(cudaStreamWaitEvent(ctx.aux_stream, ctx.ev_alloc, 0));
+  }
   PYFOF_CUDA(cudaMemcpyAsync((void *)a.xp, xp, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
   if (vp)
-    PYFOF_CUDA(cudaMemcpyAsync((void *)a.vp, vp, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
-  if (mp) PYFOF_CUDA(cudaMemcpyAsync((void *)a.mp, mp, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    PYFOF_CUDA(cudaMemcpyAsync((void *)a.vp, vp, sizeof(double) * 3 * n, cudaMemcpyHostToDevice,
+                               ctx.aux_stream));
+  if (mp)
+    PYFOF_CUDA(cudaMemcpyAsync((void *)a.mp, mp, sizeof(double) * n, cudaMemcpyHostToDevice, ctx.aux_stream));
+  if (side) {
+    PYFOF_CUDA(cudaEventRecord(ctx.ev_inputs, ctx.aux_stream));
+    a.inputs_ready = ctx.ev_inputs;
+  }
   PYFOF_CUDA(cudaMemsetAsync(a.in_halo, 0, sizeof(int32_t) * n, s));
   PYFOF_CUDA(cudaMemsetAsync(a.halo_id, 0, sizeof(int32_t) * n, s));
   a.soa = layout == PYFOF_LAYOUT_SOA ? 1 : 0;
@@ -320,11 +325,14 @@ int32_t pyfof_run(const double *xp, const double *vp, const double *mp, int32_t 
   ctx.timing = g_timing != 0;
   a.bound_fp64 = g_bound_fp64;
   a.bound_per_halo = g_bound_per_halo;
-  r = fof_run(ctx, a);
+  int32_t r = fof_run(ctx, a);
   if (r == kOk) {
     cudaMemcpyAsync(in_halo, a.in_halo, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(halo_id, a.halo_id, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);
   }
+  // an early failure may leave the side copies in flight: their buffers are
+  // released in the order of stream s, after them
+  if (side) cudaStreamWaitEvent(s, ctx.ev_inputs, 0);
   cudaError_t e = cudaStreamSynchronize(s);
   if (r == kOk && e != cudaSuccess) {
     set_error("CUDA failure: %s", cudaGetErrorString(e));
@@ -333,11 +341,43 @@ int32_t pyfof_run(const double *xp, const double *vp, const double *mp, int32_t 
   if (ctx.timing && r == kOk) record_stage_times(ctx);
   ctx.work.release();
   cudaStreamSynchronize(s);
-  if (r != kOk) {
-    std::memset(in_halo, 0, sizeof(int32_t) * n);
-    std::memset(halo_id, 0, sizeof(int32_t) * n);
-    std::memset(ang_mom, 0, sizeof(double) * 3 * (size_t)nhalo);
+  return r;
+}
+
+int32_t pyfof_run(const double *xp, const double *vp, const double *mp, int32_t layout,
+                  const int32_t *np_halo, int32_t nhalo, int64_t total_np, double L_Box,
+                  double linking_length, int32_t np_halo_min, int32_t bound_check,
+                  int32_t verbose, double softening, double a_val, double b_val,
+                  double s_15_val, int32_t n_threads, int64_t ng_val, double ng_global_val,
+                  int32_t *in_halo, int32_t *halo_id, double *ang_mom) {
+  // outputs are written in full on success and zeroed on every other path
+  auto zero = [&]() {
+    if (total_np > 0) {
+      if (in_halo) std::memset(in_halo, 0, sizeof(int32_t) * (size_t)total_np);
+      if (halo_id) std::memset(halo_id, 0, sizeof(int32_t) * (size_t)total_np);
+    }
+    if (ang_mom && nhalo > 0) std::memset(ang_mom, 0, sizeof(double) * 3 * (size_t)nhalo);
+  };
+  int32_t r = validate(nhalo, total_np, np_halo, n_threads);
+  if (r == kOk && (nhalo <= 0 || total_np <= 0)) {
+    zero();
+    return kOk;
   }
+  if (r == kOk && (!xp || !in_halo || !halo_id || !ang_mom)) {
+    set_error("null argument");
+    r = kInvalid;
+  }
+  if (r == kOk && bound_check && !vp) {
+    set_error("vp is required when bound_check is set");
+    r = kInvalid;
+  }
+  if (r == kOk) {
+    std::memset(ang_mom, 0, sizeof(double) * 3 * (size_t)nhalo);
+    r = run_host(xp, vp, mp, layout, np_halo, nhalo, total_np, L_Box, linking_length, np_halo_min,
+                 bound_check, verbose, softening, a_val, b_val, s_15_val, n_threads, ng_val,
+                 ng_global_val, in_halo, halo_id, ang_mom);
+  }
+  if (r != kOk) zero();
   return r;
 }
 

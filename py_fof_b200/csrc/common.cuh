@@ -19,6 +19,9 @@ enum : int32_t {
   kSpan = 2,         // candidate span exceeds the 15 Mpc limit
   kAlloc = 3,        // allocation failure
   kNonFinite = 4,    // NaN/Inf encountered
+  kMass = 5,         // a particle mass is not positive and finite (the
+                     // reference raises this in Python before its call,
+                     // py_fof/__init__.py:259-260; here the device checks)
   kThreads = 10,     // n_threads > 256
   kCuda = 20,        // CUDA runtime failure (no reference counterpart)
 };

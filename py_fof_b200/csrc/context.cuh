@@ -46,6 +46,8 @@ struct Context {
   int device = 0;
   cudaStream_t stream = nullptr;      // stream all work is issued on
   cudaStream_t own_stream = nullptr;  // the context's own stream (default)
+  cudaStream_t aux_stream = nullptr;  // host-to-device copies of vp and mp
+  cudaEvent_t ev_alloc = nullptr, ev_inputs = nullptr;
   Arena work;    // per-call device memory, released at the end of every call
   int32_t *d_flags = nullptr;  // device status words (error codes, counters)
   int32_t *h_flags = nullptr;  // pinned mirror

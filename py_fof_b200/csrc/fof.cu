@@ -952,6 +952,33 @@ int32_t fof_plain_angmom(Context &ctx, const FofArgs &a, FofState &st) {
   return kOk;
 }
 
+// Every mass positive and finite (py_fof/__init__.py:259-260).
+__global__ void check_mass_kernel(const double *__restrict__ mp, int64_t n, int32_t *__restrict__ bad) {
+  int found = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double m = mp[i];
+    found |= !(m > 0.0 && m <= 1.7976931348623157e308);
+  }
+  if (__syncthreads_or(found) && threadIdx.x == 0) atomicExch(bad, 1);
+}
+
+int32_t check_masses(Context &ctx, const double *mp, int64_t n) {
+  cudaStream_t s = ctx.stream;
+  int32_t *bad = ctx.d_flags + FLAG_COUNT_C;
+  PYFOF_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t), s));
+  const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(n, BLK), (int64_t)kNumSMs * 8);
+  check_mass_kernel<<<grid, BLK, 0, s>>>(mp, n, bad);
+  PYFOF_CHECK_LAUNCH();
+  PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags + FLAG_COUNT_C, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  PYFOF_CUDA(cudaStreamSynchronize(s));
+  if (ctx.h_flags[FLAG_COUNT_C]) {
+    set_error("all particle masses must be positive and finite");
+    return kMass;
+  }
+  return kOk;
+}
+
 int32_t fof_run(Context &ctx, const FofArgs &a) {
   FofState st;
   ctx.conv_timer.reset();
@@ -960,6 +987,8 @@ int32_t fof_run(Context &ctx, const FofArgs &a) {
   if (ctx.timing) cudaEventRecord(ctx.ev[2], ctx.stream);
   PYFOF_TRY(fof_link_stage(ctx, a, st));
   PYFOF_TRY(fof_candidates_stage(ctx, a, st, !a.bound_check));
+  if (a.inputs_ready) PYFOF_CUDA(cudaStreamWaitEvent(ctx.stream, a.inputs_ready, 0));
+  if (a.mp) PYFOF_TRY(check_masses(ctx, a.mp, a.total_np));
   if (ctx.timing) cudaEventRecord(ctx.ev[3], ctx.stream);
   if (!a.bound_check) PYFOF_TRY(fof_plain_angmom(ctx, a, st));
   else PYFOF_TRY(unbind_stage(ctx, a, st));

@@ -23,6 +23,9 @@ struct FofArgs {
   double ng_global = 512.0;
   int32_t bound_fp64 = 0;  // 1: plain FP64 unbinding path instead of the FP32 product path
   int32_t bound_per_halo = 0;  // 1: FP64, one halo per launch sequence (the plain baseline)
+  // recorded when vp and mp are on the device (they may still be copying
+  // while the linking runs); null when they are already there
+  cudaEvent_t inputs_ready = nullptr;
   // outputs (device): in_halo, halo_id (N int32); ang_mom host (3,nhalo) F-order
   int32_t *in_halo = nullptr, *halo_id = nullptr;
   double *ang_mom = nullptr;

@@ -180,3 +180,23 @@ def test_canonical_partition_matches():
     d = W.plummer_box(20 ** 3, 20.0, 3, seed=12)
     g, o = _both(d["xp"], L_Box=20.0, linking_length=0.25, np_halo_min=2)
     assert np.array_equal(canonical(g[1]), canonical(o[1]))
+
+
+@pytest.mark.parametrize("bad_mass", [0.0, -1.0, np.nan, np.inf])
+@pytest.mark.parametrize("bound", [False, True])
+def test_invalid_masses_rejected_on_device(bad_mass, bound):
+    """The mass check (py_fof/__init__.py:259-260) runs on the device for
+    the native call and raises the reference's ValueError; the oracle path
+    keeps the host check, with the same message."""
+    d = W.plummer_box(12 ** 3, 12.0, 2, seed=21, with_velocities=True, lognormal_mass=0.3)
+    mp = d["mp"].copy()
+    mp[777] = bad_mass
+    kw = dict(vp_list=d["vp"], mp_list=mp, L_Box=12.0, linking_length=0.2, np_halo_min=10,
+              bound_check=bound, ng_global=512.0)
+    with pytest.raises(ValueError, match="positive and finite"):
+        P.fof(d["xp"], **kw)
+    with pytest.raises(ValueError, match="positive and finite"):
+        oracle_core(d["xp"], **kw)
+    # the library stays usable and a valid call afterwards is unaffected
+    kw["mp_list"] = d["mp"]
+    assert np.array_equal(P._fof_core(d["xp"], **kw)[1], oracle_core(d["xp"], **kw)[1])
