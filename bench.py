@@ -313,7 +313,10 @@ def run_b200(args):
             dist.destroy_process_group()
         if rank == 0:
             print(json.dumps({"profile_run": args.workload, "ms_per_step": ms_max,
-                              "gpu_launches": launches}), flush=True)
+                              "gpu_launches": launches, "pm_fft_bytes_per_call": mean(st, "pm_fft_bytes"),
+                              "pm_fft_ms_per_call": mean(st, "pm_fft"), "pm_solves": counts["pm_solves"],
+                              "link_ms": mean(st, "link"), "cells": _native.get_stat("cells")}),
+                  flush=True)
         return 0
 
     unbind = None

@@ -257,9 +257,9 @@ __device__ __forceinline__ void link_pair(int *parent, int p, int q, int &rp, in
 __global__ void __launch_bounds__(BLK, 3) fof_link_kernel(
     const float4 *__restrict__ pos, const uint32_t *__restrict__ skey,
     const uint32_t *__restrict__ prid, const RegionDev *__restrict__ R,
-    const uint32_t *__restrict__ cell_start, int *parent, int64_t n_active, LinkParams P,
+    const uint32_t *__restrict__ cell_start, int *parent, int64_t w0, int64_t w1, LinkParams P,
     DenseIndex D, int32_t *flags) {
-  for (int64_t w = (int64_t)blockIdx.x * BLK + threadIdx.x; w < n_active;
+  for (int64_t w = w0 + (int64_t)blockIdx.x * BLK + threadIdx.x; w < w1;
        w += (int64_t)gridDim.x * BLK) {
     const int64_t p = D.order[w];
     const float4 me = pos[p];
@@ -794,6 +794,7 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
     P.rp2_lo = (float)(P.rp2 * (1.0 - 4e-6));
     P.rp2_hi = (float)(P.rp2 * (1.0 + 4e-6));
     DenseIndex D{};
+    int64_t ndense_p = 0;  // particles in dense cells (the head of D.order)
     // slack: relative 1e-4 for the FP32 distance arithmetic, 8 FP32 ulps of
     // the box size for the rounding of positions and query endpoints
     D.reach = (float)(a.link * (1.0 + 1e-4) + 8.0 * 1.1920928955078125e-07 * (std::fabs(L) + 1.0));
@@ -824,7 +825,7 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
                                  cudaMemcpyDeviceToHost, s));
       PYFOF_CUDA(cudaStreamSynchronize(s));
       const int64_t ndense = (uint32_t)ctx.h_flags[FLAG_COUNT_B];
-      const int64_t ndense_p = (uint32_t)ctx.h_flags[FLAG_COUNT_C];
+      ndense_p = (uint32_t)ctx.h_flags[FLAG_COUNT_C];
       fof_order_kernel<<<grid, BLK, 0, s>>>(pflag, prank, n_active, ndense_p, order);
       PYFOF_CHECK_LAUNCH();
       uint32_t *tab = W.carve<uint32_t>(std::max<int64_t>(ndense, 1) * D.stride);
@@ -843,10 +844,19 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
       D.order = order;
       ctx.last_dense = ndense;
     }
+    // dense-cell particles and the rest as two launches: the long pair loops
+    // of the dense part do not hold back blocks of the short sparse work
     if (ctx.timing) cudaEventRecord(ctx.ev[0], s);
-    fof_link_kernel<<<grid, BLK, 0, s>>>(pos, skey, prid, dR, cstart, parent, n_active, P, D,
-                                         ctx.d_flags);
-    PYFOF_CHECK_LAUNCH();
+    if (ndense_p > 0) {
+      fof_link_kernel<<<grid, BLK, 0, s>>>(pos, skey, prid, dR, cstart, parent, 0, ndense_p, P, D,
+                                           ctx.d_flags);
+      PYFOF_CHECK_LAUNCH();
+    }
+    if (n_active > ndense_p) {
+      fof_link_kernel<<<grid, BLK, 0, s>>>(pos, skey, prid, dR, cstart, parent, ndense_p, n_active, P,
+                                           D, ctx.d_flags);
+      PYFOF_CHECK_LAUNCH();
+    }
     if (ctx.timing) cudaEventRecord(ctx.ev[1], s);
   }
   st.dR = dR;
