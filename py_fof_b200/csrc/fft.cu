@@ -551,9 +551,17 @@ int32_t convolve_n(R *rho, cplx_t<R> *spec, const R *green, int sup, int batch, 
       spec, nullptr, bstride, (int64_t)N * nhp, nhp, sup, ntiles, 1, batch, sup, N);
   PYFOF_CHECK_LAUNCH();
   // z: forward, Green, inverse; lines (kx, ky), input and output z < sup;
-  // halos split into chunks so that the grid fills the device
+  // halos split into chunks so that the grid is at least four full waves
   const int64_t per = (int64_t)ntiles * N;
-  const int nchunk = (int)std::max<int64_t>(1, std::min<int64_t>(batch, ceil_div(4 * kNumSMs, per)));
+  static int conv_blocks_per_sm = 0;
+  if (!conv_blocks_per_sm) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_lines<R, N, -1, true>, T, sm) != cudaSuccess || b < 1)
+      b = 1;
+    conv_blocks_per_sm = b;
+  }
+  const int64_t slots = (int64_t)conv_blocks_per_sm * kNumSMs;
+  const int nchunk = (int)std::max<int64_t>(1, std::min<int64_t>(batch, ceil_div(4 * slots, per)));
   const int nbb = (int)ceil_div(batch, nchunk);
   const int nchunk_used = (int)ceil_div(batch, nbb);
   k_lines<R, N, -1, true><<<(unsigned)(per * nchunk_used), T, sm, s>>>(

@@ -358,6 +358,190 @@ __global__ void __launch_bounds__(BLK, 3) fof_link_kernel(
   }
 }
 
+// Dense cells, warp-cooperative: a warp takes a chunk of up to 32 particles
+// of one dense cell (consecutive in sub-cell order, so the chunk is
+// compact) and walks the neighbour cells and sub-cells that the chunk's
+// bounding box widened by `reach` can touch.  Sources come in coalesced
+// batches of 32; a source enters the pair loop only if it lies inside the
+// widened box, and then every lane tests it against its own particle with
+// the exact reference test.  Each pair is tested from the same side as in
+// the per-particle kernel (lower cell; in the own cell the lower sorted
+// position), so the set of linked pairs, and with it the partition, is the
+// same.
+struct DenseChunk {
+  uint32_t cell, e0;  // dense cell (global cell index), first index in its dpos list
+};
+
+__global__ void __launch_bounds__(BLK, 2) fof_link_dense_kernel(
+    const float4 *__restrict__ pos, const uint32_t *__restrict__ prid, const RegionDev *__restrict__ R,
+    const uint32_t *__restrict__ cell_start, int *parent, const DenseChunk *__restrict__ chunks,
+    int64_t nchunks, LinkParams P, DenseIndex D, int32_t *flags) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * BLK) >> 5;
+  for (int64_t ch = ((int64_t)blockIdx.x * BLK + threadIdx.x) >> 5; ch < nchunks; ch += nw) {
+    const DenseChunk C = chunks[ch];
+    const int64_t cb = cell_start[C.cell];
+    const int64_t cn = (int64_t)cell_start[C.cell + 1] - cb;
+    const int64_t k = (int64_t)C.e0 + lane;
+    const bool valid = k < cn;
+    float4 me = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid) me = D.dpos[cb + k];
+    const int ip = valid ? __float_as_int(me.w) : -1;
+    const RegionDev &r = R[prid[cb]];
+    const int64_t local = (int64_t)C.cell - (int64_t)r.cell_off;
+    const int64_t N0 = r.N[0], N1 = r.N[1], N2 = r.N[2];
+    const int64_t ixyz[3] = {local % N0, (local / N0) % N1, local / (N0 * N1)};
+    const int64_t Nd[3] = {N0, N1, N2};
+    const bool per = r.periodic != 0;
+    // chunk bounding box
+    float bl[3] = {valid ? me.x : 3e38f, valid ? me.y : 3e38f, valid ? me.z : 3e38f};
+    float bh[3] = {valid ? me.x : -3e38f, valid ? me.y : -3e38f, valid ? me.z : -3e38f};
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        bl[d] = fminf(bl[d], __shfl_xor_sync(FULL, bl[d], o));
+        bh[d] = fmaxf(bh[d], __shfl_xor_sync(FULL, bh[d], o));
+      }
+    int lo[3], hi[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const bool pd = (r.pdim >> d) & 1;
+      if (Nd[d] == 1) { lo[d] = 0; hi[d] = 0; continue; }
+      const float clo = cell_lower(r, d, ixyz[d]);
+      const float chi = cell_lower(r, d, ixyz[d] + 1);
+      const bool below = __fsub_rn(bl[d], D.reach) < clo;
+      const bool above = __fadd_rn(bh[d], D.reach) >= chi;
+      if (pd && Nd[d] == 2) { lo[d] = 0; hi[d] = (below || above) ? 1 : 0; }
+      else { lo[d] = below ? -1 : 0; hi[d] = above ? 1 : 0; }
+    }
+    int rp = -1;  // cached root of this lane's particle
+    for (int dz = lo[2]; dz <= hi[2]; ++dz) {
+      int64_t jz = ixyz[2] + dz;
+      float shz = 0.f;
+      if ((r.pdim >> 2) & 1) {
+        if (jz < 0) { jz += N2; shz = (float)P.L; } else if (jz >= N2) { jz -= N2; shz = -(float)P.L; }
+      } else if (jz < 0 || jz >= N2) continue;
+      for (int dy = lo[1]; dy <= hi[1]; ++dy) {
+        int64_t jy = ixyz[1] + dy;
+        float shy = 0.f;
+        if ((r.pdim >> 1) & 1) {
+          if (jy < 0) { jy += N1; shy = (float)P.L; } else if (jy >= N1) { jy -= N1; shy = -(float)P.L; }
+        } else if (jy < 0 || jy >= N1) continue;
+        for (int dx = lo[0]; dx <= hi[0]; ++dx) {
+          int64_t jx = ixyz[0] + dx;
+          float shx = 0.f;
+          if (r.pdim & 1) {
+            if (jx < 0) { jx += N0; shx = (float)P.L; } else if (jx >= N0) { jx -= N0; shx = -(float)P.L; }
+          } else if (jx < 0 || jx >= N0) continue;
+          const int64_t jl = jx + N0 * (jy + N1 * jz);
+          if (jl < local) continue;
+          const uint64_t jc = r.cell_off + (uint64_t)jl;
+          const int64_t b = cell_start[jc];
+          const int64_t e = cell_start[jc + 1];
+          const bool own = (jl == local);
+          const float sh[3] = {shx, shy, shz};
+          // the widened box in the neighbour cell's frame
+          // (no bound along periodic axes of one or two cells: a partner may
+          // sit across either face there, through the minimum image)
+          float wl[3], wh[3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            if (((r.pdim >> d) & 1) && Nd[d] <= 2) {
+              wl[d] = -3e38f;
+              wh[d] = 3e38f;
+            } else {
+              wl[d] = __fsub_rn(__fadd_rn(bl[d], sh[d]), D.reach);
+              wh[d] = __fadd_rn(__fadd_rn(bh[d], sh[d]), D.reach);
+            }
+          }
+          // source ranges: one range for a plain cell, one per sub-cell row
+          // for a dense cell
+          const bool dense = (e - b > DENSE_T) && r.sub_ok;
+          int slo[3] = {0, 0, 0}, shi[3] = {0, 0, 0};
+          const uint32_t *tab = nullptr;
+          if (dense) {
+            tab = D.tab + (int64_t)D.rank[jc] * D.stride;
+            const int64_t jcoord[3] = {jx, jy, jz};
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              const float clo = cell_lower(r, d, jcoord[d]);
+              slo[d] = sub_of(wl[d], clo, r.inv_sub[d], r.sub[d]);
+              shi[d] = sub_of(wh[d], clo, r.inv_sub[d], r.sub[d]);
+            }
+          }
+          for (int sz = slo[2]; sz <= shi[2]; ++sz)
+            for (int sy = slo[1]; sy <= shi[1]; ++sy) {
+              int64_t k0, k1;
+              if (dense) {
+                const int s0 = slo[0] + r.sub[0] * (sy + r.sub[1] * sz);
+                k0 = tab[s0];
+                k1 = tab[s0 + (shi[0] - slo[0]) + 1];
+              } else {
+                k0 = 0;
+                k1 = e - b;
+              }
+              for (int64_t base = k0; base < k1; base += 32) {
+                const int64_t t = base + lane;
+                float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+                int q = -1;
+                bool cand = false;
+                if (t < k1) {
+                  if (dense) {
+                    o = D.dpos[b + t];
+                    q = __float_as_int(o.w);
+                  } else {
+                    o = pos[b + t];
+                    q = (int)(b + t);
+                  }
+                  cand = o.x >= wl[0] && o.x <= wh[0] && o.y >= wl[1] && o.y <= wh[1] && o.z >= wl[2] &&
+                         o.z <= wh[2];
+                }
+                unsigned mask = __ballot_sync(FULL, cand);
+                while (mask) {
+                  const int src = __ffs(mask) - 1;
+                  mask &= mask - 1;
+                  float4 so;
+                  so.x = __shfl_sync(FULL, o.x, src);
+                  so.y = __shfl_sync(FULL, o.y, src);
+                  so.z = __shfl_sync(FULL, o.z, src);
+                  so.w = 0.f;
+                  const int qs = __shfl_sync(FULL, q, src);
+                  if (valid && !(own && qs <= ip)) {
+                    const bool lk = per ? linked_pbc(me, so, P) : linked_open(me, so, P.rp2_open);
+                    if (lk) link_pair(parent, ip, qs, rp, flags);
+                  }
+                }
+              }
+            }
+        }
+      }
+    }
+  }
+}
+
+// Chunks of up to 32 particles per dense cell.
+__global__ void fof_dense_chunk_count_kernel(const uint32_t *__restrict__ list, const uint32_t *__restrict__ cs,
+                                             int64_t ndense, uint32_t *__restrict__ cnt) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ndense;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t c = list[i];
+    cnt[i] = (cs[c + 1] - cs[c] + 31u) / 32u;
+  }
+}
+
+__global__ void fof_dense_chunk_fill_kernel(const uint32_t *__restrict__ list, const uint32_t *__restrict__ cs,
+                                            const uint32_t *__restrict__ off, int64_t ndense,
+                                            DenseChunk *__restrict__ chunks) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ndense;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t c = list[i];
+    const uint32_t n = (cs[c + 1] - cs[c] + 31u) / 32u;
+    for (uint32_t j = 0; j < n; ++j) chunks[off[i] + j] = DenseChunk{c, 32u * j};
+  }
+}
+
 __global__ void fof_dense_flag_kernel(const uint32_t *__restrict__ cs,
                                       const uint64_t *__restrict__ cell_off,
                                       const RegionDev *__restrict__ R, int nreg, int64_t ncell,
@@ -795,6 +979,8 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
     P.rp2_hi = (float)(P.rp2 * (1.0 + 4e-6));
     DenseIndex D{};
     int64_t ndense_p = 0;  // particles in dense cells (the head of D.order)
+    int64_t ndense_chunks = 0;
+    DenseChunk *dchunks = nullptr;
     // slack: relative 1e-4 for the FP32 distance arithmetic, 8 FP32 ulps of
     // the box size for the rounding of positions and query endpoints
     D.reach = (float)(a.link * (1.0 + 1e-4) + 8.0 * 1.1920928955078125e-07 * (std::fabs(L) + 1.0));
@@ -837,6 +1023,22 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
         fof_dense_build_kernel<<<(unsigned)ndense, BLK, 0, s>>>(list, cstart, pos, dR, dcoff, nreg,
                                                                 D.stride, tab, dpos);
         PYFOF_CHECK_LAUNCH();
+        // warp chunks of the dense cells
+        uint32_t *coff = W.carve<uint32_t>(ndense + 1);
+        if (!coff) { set_error("workspace exhausted (dense chunks)"); return kAlloc; }
+        PYFOF_CUDA(cudaMemsetAsync(coff, 0, sizeof(uint32_t) * (ndense + 1), s));
+        const unsigned lgrid = (unsigned)std::min<int64_t>(ceil_div(ndense, BLK), (int64_t)kNumSMs * 16);
+        fof_dense_chunk_count_kernel<<<lgrid, BLK, 0, s>>>(list, cstart, ndense, coff);
+        PYFOF_CHECK_LAUNCH();
+        PYFOF_TRY(exclusive_scan_u32(coff, coff, ndense + 1, nullptr, W, s));
+        uint32_t nch = 0;
+        PYFOF_CUDA(cudaMemcpyAsync(&nch, coff + ndense, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        PYFOF_CUDA(cudaStreamSynchronize(s));
+        ndense_chunks = nch;
+        dchunks = W.carve<DenseChunk>(std::max<uint32_t>(nch, 1));
+        if (!dchunks) { set_error("workspace exhausted (dense chunks)"); return kAlloc; }
+        fof_dense_chunk_fill_kernel<<<lgrid, BLK, 0, s>>>(list, cstart, coff, ndense, dchunks);
+        PYFOF_CHECK_LAUNCH();
       }
       D.rank = drank;
       D.tab = tab;
@@ -847,9 +1049,10 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
     // dense-cell particles and the rest as two launches: the long pair loops
     // of the dense part do not hold back blocks of the short sparse work
     if (ctx.timing) cudaEventRecord(ctx.ev[0], s);
-    if (ndense_p > 0) {
-      fof_link_kernel<<<grid, BLK, 0, s>>>(pos, skey, prid, dR, cstart, parent, 0, ndense_p, P, D,
-                                           ctx.d_flags);
+    if (ndense_chunks > 0) {
+      const unsigned dgrid = (unsigned)std::min<int64_t>(ceil_div(ndense_chunks * 32, BLK), (int64_t)kNumSMs * 24);
+      fof_link_dense_kernel<<<dgrid, BLK, 0, s>>>(pos, prid, dR, cstart, parent, dchunks, ndense_chunks, P, D,
+                                                  ctx.d_flags);
       PYFOF_CHECK_LAUNCH();
     }
     if (n_active > ndense_p) {

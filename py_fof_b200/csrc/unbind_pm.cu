@@ -451,7 +451,7 @@ struct SrChunk {
 };
 
 template <typename R, bool UPDATE>
-__global__ void __launch_bounds__(256) sr_gather_kernel(
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) sr_gather_kernel(
     const PmHalo *__restrict__ H, const int32_t *__restrict__ mhalo, const uint8_t *__restrict__ keep,
     const uint8_t *__restrict__ pr, const SrChunk *__restrict__ chunks, int64_t nchunks,
     const uint32_t *__restrict__ cstart, const uint32_t *__restrict__ cmem, const float4 *__restrict__ src4,
