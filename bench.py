@@ -2,7 +2,8 @@
 """Benchmark of the py_fof B200 hot path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload fof_unbind_256|fof_256|fof_128|fof_64]
+                    [--workload fof_unbind_256|fof_unbind_128|fof_256|fof_128|fof_64|
+                                unbind_nfw_20k|unbind_nfw_2k]
 
 One step = one full ``fof()`` call over one synthetic particle set.  The
 default workload is FoF + unbinding (bound_check=True, cube units,
@@ -48,26 +49,31 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# name: (n_side, bound_check); box side = n_side, halos = 4096 (n_side/256)^3
+# Plummer boxes: name -> (n_side, bound_check); box side n_side, 4096
+# (n_side/256)^3 halos.  NFW lists: name -> (halos, largest halo).
 WORKLOADS = {
-    "fof_unbind_256": (256, True),
-    "fof_unbind_128": (128, True),
-    "fof_256": (256, False),
-    "fof_128": (128, False),
-    "fof_64": (64, False),
+    "fof_unbind_256": ("box", 256, True),
+    "fof_unbind_128": ("box", 128, True),
+    "fof_256": ("box", 256, False),
+    "fof_128": ("box", 128, False),
+    "fof_64": ("box", 64, False),
+    "unbind_nfw_20k": ("nfw", 20000, 2_000_000),
+    "unbind_nfw_2k": ("nfw", 2000, 200_000),
 }
-# CPU sample of each workload: a sub-volume with the same recipe and density
+# CPU sample of each workload: a sub-volume with the same recipe and density,
+# or the first halos of the same list
 CPU_SAMPLE = {
     "fof_unbind_256": "fof_unbind_128",
     "fof_unbind_128": "fof_unbind_128",
     "fof_256": "fof_64",
     "fof_128": "fof_64",
     "fof_64": "fof_64",
+    "unbind_nfw_20k": "unbind_nfw_20k:300",
+    "unbind_nfw_2k": "unbind_nfw_2k:300",
 }
 LINK = 0.2
 NP_MIN = 10
 SOFTENING = 0.1
-S15 = 15.0 * 0.67 * 256.0 / 300.0  # the 256-box value, kept for its sub-volumes
 # algorithmic bytes of the linking kernel: 12 B position read, 4 B parent
 # read, 4 B parent write per particle plus a 4 B cell offset per cell
 LINK_BYTES_PER_PARTICLE = 20
@@ -151,48 +157,68 @@ class ClockSampler:
 
 
 def make_workload(name, seed=0):
+    """Synthetic input of a workload: dict(xp (3,N), vp, mp (None = unit
+    masses), np_halo, L, bound, s15, regions (the per-region arrays of a
+    list input, else None)).  "name:K" keeps the first K regions of a list."""
     from py_fof_b200 import workloads as W
-    side, bound = WORKLOADS[name]
-    halos = max(1, int(round(4096 * (side / 256.0) ** 3)))
-    d = W.plummer_box(side ** 3, float(side), halos, seed=seed, with_velocities=bound,
-                      lognormal_mass=0.3 if bound else None)
-    return d, float(side), bound
+    base, _, keep = name.partition(":")
+    kind, a, b = WORKLOADS[base]
+    if kind == "box":
+        side, bound = a, b
+        halos = max(1, int(round(4096 * (side / 256.0) ** 3)))
+        d = W.plummer_box(side ** 3, float(side), halos, seed=seed, with_velocities=bound,
+                          lognormal_mass=0.3 if bound else None)
+        # a sub-volume keeps the 256-box s_15 (the same physical scales)
+        return dict(xp=d["xp"], vp=d["vp"], mp=d["mp"], np_halo=[side ** 3], L=float(side),
+                    bound=bound, s15=15.0 * 0.67 * 256.0 / 300.0, ng_global=256.0, regions=None)
+    xs, vs = W.nfw_halos(a, seed=seed, mmax=b)
+    if keep:
+        xs, vs = xs[:int(keep)], vs[:int(keep)]
+    return dict(xp=np.ascontiguousarray(np.hstack(xs)), vp=np.ascontiguousarray(np.hstack(vs)), mp=None,
+                np_halo=[x.shape[1] for x in xs], L=512.0, bound=True,
+                s15=15.0 * 0.67 * 512.0 / 300.0, ng_global=512.0, regions=(xs, vs))
 
 
-def cpu_port_run(d, L, bound, threads):
+def cpu_port_run(wl, threads):
     """One call of the CPU restatement (oracle/) on the workload."""
     from oracle import oracle as O
-    xp = np.asfortranarray(d["xp"])
+    xp = np.asfortranarray(wl["xp"])
     n = xp.shape[1]
-    vp = np.asfortranarray(d["vp"]) if d["vp"] is not None else np.zeros((3, n), order="F")
-    mp = d["mp"] if d["mp"] is not None else np.ones(n)
+    vp = np.asfortranarray(wl["vp"]) if wl["vp"] is not None else np.zeros((3, n), order="F")
+    mp = wl["mp"] if wl["mp"] is not None else np.ones(n)
+    nph = np.asarray(wl["np_halo"], np.int32)
     t0 = time.perf_counter()
-    _, hid, _, ierr = O.fof_fortran(xp, vp, mp, np.array([n], np.int32), 1, L, LINK, NP_MIN,
-                                    int(bound), 0, SOFTENING, 1.0, 0.0, S15, threads, n)
+    _, hid, _, ierr = O.fof_fortran(xp, vp, mp, nph, len(nph), wl["L"], LINK, NP_MIN,
+                                    int(wl["bound"]), 0, SOFTENING, 1.0, 0.0, wl["s15"], threads, n)
     dt = time.perf_counter() - t0
     if ierr:
         raise RuntimeError(f"oracle ierr={ierr}")
     return dt, int(hid.max()), O.last_threads()
 
 
+def _sample_kind(name, workload):
+    if ":" in name:
+        return f"the first {name.partition(':')[2]} halos of the {workload} list"
+    return f"a sub-volume of {workload} with the same recipe and density"
+
+
 def cpu_baseline(workload, seed, budget_s=15.0):
     """The oracle on a bounded sample of `workload`, repeated for ~budget_s."""
     name = CPU_SAMPLE[workload]
-    d, L, bound = make_workload(name, seed)
+    wl = make_workload(name, seed)
     threads = os.cpu_count() or 1
-    cpu_port_run(d, L, bound, threads)  # first call builds the Green's function tables
+    cpu_port_run(wl, threads)  # first call builds the Green's function tables
     dts = []
     deadline = time.perf_counter() + budget_s
     used = threads
     while time.perf_counter() < deadline or not dts:
-        dt, _, used = cpu_port_run(d, L, bound, threads)
+        dt, _, used = cpu_port_run(wl, threads)
         dts.append(dt)
-    n = d["xp"].shape[1]
+    n = wl["xp"].shape[1]
     return {"value": n / (sum(dts) / len(dts)) / 1e6, "unit": "Mpart/s", "cores": used,
             "kind": "port",
-            "sample": f"{name}: {n} particles, same recipe and density as {workload} "
-                      f"(a sub-volume), {len(dts)} calls after one untimed call, "
-                      "reference thread policy"}
+            "sample": f"{name}: {n} particles, {_sample_kind(name, workload)}, {len(dts)} calls "
+                      "after one untimed call, reference thread policy"}
 
 
 def run_reference(args):
@@ -203,14 +229,15 @@ def run_reference(args):
     if rank != 0:
         return 0
     name = CPU_SAMPLE[args.workload]
-    d, L, bound = make_workload(name, args.seed)
-    n = d["xp"].shape[1]
+    wl = make_workload(name, args.seed)
+    n = wl["xp"].shape[1]
+    L, bound = wl["L"], wl["bound"]
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
-        cpu_port_run(d, L, bound, threads)
+        cpu_port_run(wl, threads)
     times, used = [], threads
     for _ in range(args.steps):
-        dt, _, used = cpu_port_run(d, L, bound, threads)
+        dt, _, used = cpu_port_run(wl, threads)
         times.append(dt)
     t = sum(times) / len(times)
     v = n / t / 1e6
@@ -222,8 +249,8 @@ def run_reference(args):
         "config": {"workload": args.workload, "particles": n, "L_Box": L, "link": LINK,
                    "np_halo_min": NP_MIN, "bound_check": bound, "softening": SOFTENING},
         "cpu_baseline": {"value": v, "unit": "Mpart/s", "cores": used, "kind": "port",
-                         "sample": f"{name}: {n} particles per step, same recipe and density "
-                                   f"as {args.workload} (a sub-volume), reference thread policy"},
+                         "sample": f"{name}: {n} particles per step, "
+                                   f"{_sample_kind(name, args.workload)}, reference thread policy"},
         "e2e": {"value": v, "unit": "Mpart/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -249,7 +276,9 @@ def run_b200(args):
     L_ = _native.load()
     if L_.pyfof_init(local) != 0:
         raise RuntimeError(_native.last_error())
-    d, Lbox, bound = make_workload(args.workload, args.seed)
+    d = make_workload(args.workload, args.seed)
+    Lbox, bound, s15 = d["L"], d["bound"], d["s15"]
+    nph = list(d["np_halo"])
     n = d["xp"].shape[1]
     dev = torch.device("cuda", local)
     xp = torch.from_numpy(d["xp"]).to(dev)
@@ -264,8 +293,8 @@ def run_b200(args):
     def step():
         _, ierr = _native.run_device(
             xp.data_ptr(), vp.data_ptr() if vp is not None else 0,
-            mp.data_ptr() if mp is not None else 0, _native.LAYOUT_SOA, [n], 1, n, Lbox, LINK,
-            NP_MIN, int(bound), 0, SOFTENING, 1.0, 0.0, S15, 0, ih.data_ptr(), hid.data_ptr())
+            mp.data_ptr() if mp is not None else 0, _native.LAYOUT_SOA, nph, len(nph), n, Lbox, LINK,
+            NP_MIN, int(bound), 0, SOFTENING, 1.0, 0.0, s15, 0, ih.data_ptr(), hid.data_ptr())
         if ierr:
             raise RuntimeError(f"ierr={ierr}: {_native.last_error()}")
         return {k: _native.last_stage_ms(k) for k in ("link", "fof", "unbind", "call", "pm_fft")} | {
@@ -350,10 +379,13 @@ def run_b200(args):
         p.copy_(torch.from_numpy(a))
         return p.numpy()
 
-    xp_h, vp_h, mp_h = pinned(d["xp"]), pinned(d["vp"]), pinned(d["mp"])
+    if d["regions"] is None:
+        xp_h, vp_h, mp_h = pinned(d["xp"]), pinned(d["vp"]), pinned(d["mp"])
+    else:  # list input, as the reference API takes it
+        xp_h, vp_h, mp_h = list(d["regions"][0]), list(d["regions"][1]), None
     _native.set_stream(0)
     kw = dict(vp_list=vp_h, mp_list=mp_h, L_Box=Lbox, linking_length=LINK, np_halo_min=NP_MIN,
-              bound_check=bound, softening=SOFTENING, ng_global=256.0)
+              bound_check=bound, softening=SOFTENING, ng_global=d["ng_global"])
     for _ in range(max(1, min(args.warmup, 2))):
         P.fof(xp_h, **kw)
     e2e_t = []
@@ -403,7 +435,7 @@ def run_b200(args):
         "data": "synthetic",
         "config": {"workload": args.workload, "particles": n, "L_Box": Lbox, "link": LINK,
                    "np_halo_min": NP_MIN, "bound_check": bound, "softening": SOFTENING,
-                   "s_15": S15, "groups": ngroups, "unbinding": "fp32 batched" if bound else None,
+                   "s_15": s15, "regions": len(nph), "groups": ngroups, "unbinding": "fp32 batched" if bound else None,
                    "l2": "inputs larger than L2 (402 MB positions)" if n >= 2 ** 24 else
                          "inputs smaller than L2",
                    "parallelism": f"replicas x{world}"},
