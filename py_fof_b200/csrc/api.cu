@@ -24,7 +24,7 @@ int g_timing = 0;
 }  // namespace
 
 void set_error(const char *fmt, ...) {
-  char buf[1024];
+  char buf[4096];
   va_list ap;
   va_start(ap, fmt);
   vsnprintf(buf, sizeof(buf), fmt, ap);
@@ -124,6 +124,27 @@ static int32_t validate(int32_t nhalo, int64_t total_np, const int32_t *np_halo,
   return kOk;
 }
 
+// An allocation failure reports what the call held and what it asked for.
+static void note_alloc_failure(Context &ctx, int32_t r) {
+  if (r != kAlloc) return;
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  // the largest blocks held, in allocation order
+  std::string big;
+  size_t thr = ctx.work.bytes / 50;
+  for (size_t i = 0; i < ctx.work.sizes.size(); ++i)
+    if (ctx.work.sizes[i] >= thr && big.size() < 200)
+      big += " #" + std::to_string(i) + ":" + std::to_string(ctx.work.sizes[i] >> 20) + "MiB";
+  big += " first:";
+  for (size_t i = 0; i < ctx.work.sizes.size() && i < 40; ++i) big += " " + std::to_string(ctx.work.sizes[i]);
+  big += " last:";
+  for (size_t i = ctx.work.sizes.size() > 20 ? ctx.work.sizes.size() - 20 : 0; i < ctx.work.sizes.size(); ++i)
+    big += " " + std::to_string(ctx.work.sizes[i]);
+  set_error("%s (call holds %.3f GB in %zu blocks, failed request %.3f GB, device free %.3f of %.3f GB;%s)",
+            last_error().c_str(), ctx.work.bytes / 1e9, ctx.work.sizes.size(), ctx.work.last_fail / 1e9,
+            free_b / 1e9, total_b / 1e9, big.c_str());
+}
+
 // stage_ms: [0] linking kernel, [1] binning to candidates, [2] unbinding (or
 // the plain ang_mom pass), [3] the whole call on the device
 static void record_stage_times(Context &ctx) {
@@ -141,6 +162,7 @@ static int32_t run_common(Context &ctx, FofArgs &a) {
   a.bound_fp64 = g_bound_fp64;
   a.bound_per_halo = g_bound_per_halo;
   int32_t r = fof_run(ctx, a);
+  note_alloc_failure(ctx, r);
   cudaError_t e = cudaStreamSynchronize(ctx.stream);
   if (r == kOk && e != cudaSuccess) {
     set_error("CUDA failure: %s", cudaGetErrorString(e));
@@ -326,6 +348,7 @@ static int32_t run_host(const double *xp, const double *vp, const double *mp, in
   a.bound_fp64 = g_bound_fp64;
   a.bound_per_halo = g_bound_per_halo;
   int32_t r = fof_run(ctx, a);
+  note_alloc_failure(ctx, r);
   if (r == kOk) {
     cudaMemcpyAsync(in_halo, a.in_halo, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(halo_id, a.halo_id, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);

@@ -65,23 +65,33 @@ constexpr int kNumSMs = 148;
 struct Arena {
   cudaStream_t stream = nullptr;
   std::vector<void *> ptrs;
-  size_t bytes = 0;
+  std::vector<size_t> sizes;
+  size_t bytes = 0;      // held by this call
+  size_t last_fail = 0;  // size of the last request that failed
   template <class T>
   T *carve(size_t count) {
     void *p = nullptr;
     size_t b = (count ? count : 1) * sizeof(T);
     if (cudaMallocAsync(&p, b, stream) != cudaSuccess) {
       cudaGetLastError();
+      last_fail = b;
       return nullptr;
     }
     ptrs.push_back(p);
+    sizes.push_back(b);
     bytes += b;
     return reinterpret_cast<T *>(p);
   }
-  void release() {
-    for (void *p : ptrs) cudaFreeAsync(p, stream);
-    ptrs.clear();
-    bytes = 0;
+  void release() { release_to(0); }
+  // Blocks are freed in reverse order down to a mark taken earlier.
+  size_t mark() const { return ptrs.size(); }
+  void release_to(size_t m) {
+    while (ptrs.size() > m) {
+      cudaFreeAsync(ptrs.back(), stream);
+      bytes -= sizes.back();
+      ptrs.pop_back();
+      sizes.pop_back();
+    }
   }
 };
 

@@ -211,11 +211,13 @@ __device__ __forceinline__ bool linked_pbc(float4 a, float4 b, const LinkParams 
 }
 
 // Cells with more than DENSE_T particles carry a sub-cell index (sub[d]
-// slabs per axis, each at least one linking length wide): the particles of
-// the cell are listed by sub-cell in dpos[], sub_tab holds the offsets.  A
-// pair test against such a cell only visits the sub-cells that overlap the
-// cube of half-width `reach` around the particle, which contains every
-// partner the exact distance test can accept.
+// slabs per axis, each at least one linking length wide; a single slab when
+// the cell is narrower than two linking lengths): the particles of the cell
+// are listed by sub-cell in dpos[], sub_tab holds the offsets.  A pair test
+// against such a cell only visits the sub-cells that overlap the cube of
+// half-width `reach` around the particle, which contains every partner the
+// exact distance test can accept.  Their particles are linked by the
+// warp-cooperative kernel.
 constexpr int DENSE_T = 12;
 constexpr int SUB_MAX = 216;
 
@@ -321,7 +323,7 @@ __global__ void __launch_bounds__(BLK, 3) fof_link_kernel(
           const int64_t b = cell_start[jc];
           const int64_t e = cell_start[jc + 1];
           const bool own = (jl == local);
-          if (e - b > DENSE_T && r.sub_ok) {
+          if (e - b > DENSE_T) {
             const uint32_t *tab = D.tab + (int64_t)D.rank[jc] * D.stride;
             const int64_t jcoord[3] = {jx, jy, jz};
             const double sh[3] = {shx, shy, shz};
@@ -458,7 +460,7 @@ __global__ void __launch_bounds__(BLK, 2) fof_link_dense_kernel(
           }
           // source ranges: one range for a plain cell, one per sub-cell row
           // for a dense cell
-          const bool dense = (e - b > DENSE_T) && r.sub_ok;
+          const bool dense = e - b > DENSE_T;
           int slo[3] = {0, 0, 0}, shi[3] = {0, 0, 0};
           const uint32_t *tab = nullptr;
           if (dense) {
@@ -548,12 +550,7 @@ __global__ void fof_dense_flag_kernel(const uint32_t *__restrict__ cs,
                                       uint32_t *__restrict__ flag) {
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncell;
        c += (int64_t)gridDim.x * blockDim.x) {
-    uint32_t f = 0;
-    if (cs[c + 1] - cs[c] > (uint32_t)DENSE_T) {
-      const int rid = nreg == 1 ? 0 : region_of_key(cell_off, nreg, (uint64_t)c);
-      f = R[rid].sub_ok ? 1u : 0u;
-    }
-    flag[c] = f;
+    flag[c] = cs[c + 1] - cs[c] > (uint32_t)DENSE_T ? 1u : 0u;
   }
 }
 

@@ -23,7 +23,7 @@ struct RegionDev {
   int32_t pdim;      // bit d set: axis d is periodic
   int32_t periodic;  // any axis periodic: dist2_pbc is used for every pair
   int32_t active;    // np >= np_halo_min
-  int32_t sub_ok;    // dense cells of this region get a sub-cell index
+  int32_t sub_ok;    // dense cells of this region have more than one sub-cell
   int32_t sub[3];    // sub-cells per axis (each at least one linking length)
   float inv_sub[3];  // sub-cells per unit length
 };

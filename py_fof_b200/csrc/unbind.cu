@@ -420,9 +420,24 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
   }
   if (!pm.empty()) {
     if (a.bound_per_halo) {
+      // each halo on its own: its members as the whole member set, its
+      // scratch sized by and freed with it
       for (int32_t c : pm) {
-        const std::vector<int32_t> one(1, c);
-        PYFOF_TRY(unbind_pm(ctx, a, rules, m, tasks, one, res, keep, st.phi_out, 0));
+        const HaloTask &t = tasks[c];
+        Members mh = m;
+        for (int d = 0; d < 3; ++d) {
+          mh.q[d] += t.off;
+          mh.v[d] += t.off;
+        }
+        mh.w += t.off;
+        mh.pid += t.off;
+        std::vector<HaloTask> th(1, t);
+        th[0].off = 0;
+        const std::vector<int32_t> one(1, 0);
+        const size_t mk = W.mark();
+        PYFOF_TRY(unbind_pm(ctx, a, rules, mh, th, one, res + c, keep + t.off,
+                            st.phi_out ? st.phi_out + t.off : nullptr, 0));
+        W.release_to(mk);
       }
     } else {
       PYFOF_TRY(unbind_pm(ctx, a, rules, m, tasks, pm, res, keep, st.phi_out, 0));

@@ -1325,14 +1325,35 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
     return ctx.h_flags[FLAG_ERR];
   }
 
-  // grid batches per class, bounded by a spectrum budget
+  // grid batches per class, bounded by a spectrum budget; one scratch area,
+  // sized for the largest batch, serves every batch of every pass
   const size_t budget = (size_t)8 << 30;
+  auto round256 = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  auto batch_bytes = [&](int n, int nb) {
+    const size_t sup = n / 2 + 1;
+    return round256(sizeof(R) * nb * sup * sup * sup) + sizeof(cplx_t<R>) * (size_t)nb * spec_elems<R>(n);
+  };
+  auto max_batch = [&](int n) { return (int)std::max<size_t>(1, budget / batch_bytes(n, 1)); };
+  size_t scratch_bytes = 256;
+  for (int n : {48, 64, 128, 256}) {
+    int cnt = 0;
+    for (int h = 0; h < nh; ++h) cnt += H[h].n == n;
+    if (cnt) scratch_bytes = std::max(scratch_bytes, batch_bytes(n, std::min(cnt, max_batch(n))));
+  }
+  for (int r : {2, 4}) {
+    int cnt = 0;
+    for (int ia = 0; ia < na; ++ia) cnt += act[ia].r == r;
+    const int nin = r == 2 ? 128 : 216;
+    if (cnt) scratch_bytes = std::max(scratch_bytes, batch_bytes(nin, std::min(cnt, max_batch(nin))));
+  }
+  unsigned char *scratch = W.carve<unsigned char>(scratch_bytes);
+  int32_t *dpend = W.carve<int32_t>(nh), *dslot = W.carve<int32_t>(nh);
+  int32_t *dbatch = W.carve<int32_t>(std::max(na, 1));
+  if (!scratch || !dpend || !dslot || !dbatch) { set_error("workspace exhausted (PM grids)"); return kAlloc; }
   for (int pass = 1; pass <= kMaxPasses; ++pass) {
     std::vector<int32_t> pend;
     for (int h = 0; h < nh; ++h) if (H[h].pending) pend.push_back(h);
     if (pend.empty()) break;
-    int32_t *dpend = W.carve<int32_t>(pend.size());
-    if (!dpend) { set_error("workspace exhausted (pending)"); return kAlloc; }
     PYFOF_CUDA(cudaMemcpyAsync(dpend, pend.data(), sizeof(int32_t) * pend.size(), cudaMemcpyHostToDevice, s));
     pm_mkeep_kernel<<<(unsigned)pend.size(), 256, 0, s>>>(m, dH, dpend, (int)pend.size(), keep);
     PYFOF_CHECK_LAUNCH();
@@ -1341,19 +1362,14 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
       for (int h : pend) if (H[h].n == n) grp.push_back(h);
       if (grp.empty()) continue;
       const int sup = n / 2 + 1;
-      const size_t spec_bytes = sizeof(cplx_t<R>) * (size_t)spec_elems<R>(n);
-      const size_t per = spec_bytes + sizeof(R) * (size_t)sup * sup * sup;
-      const int maxb = (int)std::max<size_t>(1, budget / per);
+      const int maxb = max_batch(n);
       for (size_t g0 = 0; g0 < grp.size(); g0 += maxb) {
         const int nb = (int)std::min<size_t>(maxb, grp.size() - g0);
         std::vector<int32_t> hslot(nh, -1);
         for (int j = 0; j < nb; ++j) hslot[grp[g0 + j]] = j;
-        int32_t *dslot = W.carve<int32_t>(nh);
-        if (!dslot) { set_error("workspace exhausted (slots)"); return kAlloc; }
         PYFOF_CUDA(cudaMemcpyAsync(dslot, hslot.data(), sizeof(int32_t) * nh, cudaMemcpyHostToDevice, s));
-        R *rho = W.carve<R>((size_t)nb * sup * sup * sup);
-        cplx_t<R> *spec = W.carve<cplx_t<R>>((size_t)nb * spec_elems<R>(n));
-        if (!rho || !spec) { set_error("workspace exhausted (PM grids)"); return kAlloc; }
+        R *rho = reinterpret_cast<R *>(scratch);
+        cplx_t<R> *spec = reinterpret_cast<cplx_t<R> *>(scratch + round256(sizeof(R) * (size_t)nb * sup * sup * sup));
         const int64_t ng = (int64_t)nb * sup * sup * sup;
         pm_zero_kernel<R><<<(unsigned)std::min<int64_t>(ceil_div(ng, BLK), 148 * 16), BLK, 0, s>>>(rho, ng);
         PYFOF_CHECK_LAUNCH();
@@ -1377,15 +1393,12 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
       if (regs.empty()) continue;
       const int nin = r == 2 ? 128 : 216;
       const int sup = nin / 2 + 1;
-      const size_t per = sizeof(cplx_t<R>) * (size_t)spec_elems<R>(nin) + sizeof(R) * (size_t)sup * sup * sup;
-      const int maxb = (int)std::max<size_t>(1, budget / per);
+      const int maxb = max_batch(nin);
       const R *gin = (const R *)(r == 2 ? g_r2 : g_r4)->g;
       for (size_t g0 = 0; g0 < regs.size(); g0 += maxb) {
         const int nb = (int)std::min<size_t>(maxb, regs.size() - g0);
-        int32_t *dbatch = W.carve<int32_t>(nb);
-        R *rho = W.carve<R>((size_t)nb * sup * sup * sup);
-        cplx_t<R> *spec = W.carve<cplx_t<R>>((size_t)nb * spec_elems<R>(nin));
-        if (!dbatch || !rho || !spec) { set_error("workspace exhausted (inner grids)"); return kAlloc; }
+        R *rho = reinterpret_cast<R *>(scratch);
+        cplx_t<R> *spec = reinterpret_cast<cplx_t<R> *>(scratch + round256(sizeof(R) * (size_t)nb * sup * sup * sup));
         PYFOF_CUDA(cudaMemcpyAsync(dbatch, regs.data() + g0, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s));
         const int64_t ng = (int64_t)nb * sup * sup * sup;
         pm_zero_kernel<R><<<(unsigned)std::min<int64_t>(ceil_div(ng, BLK), 148 * 16), BLK, 0, s>>>(rho, ng);

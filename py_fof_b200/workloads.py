@@ -110,17 +110,21 @@ def config2(seed=0, n_side=256):
 
 
 def nfw_halos(n_halos, seed=0, mmin=20, mmax=2_000_000, s15=17.152, link=0.2, kick_frac=0.1,
-              mean_density=None):
+              mean_density=None, sizes=None):
     """List of isolated NFW spheres (one region each) for batched unbinding.
 
     The virial radius is set by a fixed mean density inside R_vir chosen so
     that the largest halo spans at most 0.9 * s15 (R_vir <= 0.45 s15).
-    Returns (xp_list, vp_list).
+    Member counts follow dN/dM ~ M^-1.9 on [mmin, mmax] unless `sizes`
+    gives them.  Returns (xp_list, vp_list).
     """
     rng = np.random.default_rng(seed)
     e = -0.9
     u = rng.random(n_halos)
-    sizes = np.floor((mmin ** e + u * (mmax ** e - mmin ** e)) ** (1.0 / e)).astype(np.int64)
+    if sizes is None:
+        sizes = np.floor((mmin ** e + u * (mmax ** e - mmin ** e)) ** (1.0 / e)).astype(np.int64)
+    else:
+        sizes = np.asarray(sizes, np.int64)
     rv_max = 0.45 * s15
     if mean_density is None:
         mean_density = mmax / (4.0 / 3.0 * np.pi * rv_max ** 3)
