@@ -21,6 +21,8 @@ G_CODE = 1.0 / (6.0 * np.pi)   # a/(6 pi) at z = 0 (bound_fortran.f90:2616)
 
 
 def _power_law_counts(rng, n_halos, total, mmin, mmax, slope=-1.9, floor=20):
+    if total < n_halos * floor:
+        raise ValueError(f"{total} halo particles cannot fill {n_halos} halos of at least {floor}")
     e = slope + 1.0
     u = rng.random(n_halos)
     m = (mmin ** e + u * (mmax ** e - mmin ** e)) ** (1.0 / e)
