@@ -143,6 +143,28 @@ int32_t pyfof_run_device(const double *d_xp, const double *d_vp, const double *d
                          double ng_global_val, int32_t *d_in_halo, int32_t *d_halo_id,
                          double *ang_mom);
 
+/* Slots: contexts of their own (CUDA streams, device scratch, status
+ * words) on one device, for callers that run several calls at once — the
+ * serving loop of py_fof_b200.serve runs one host thread per slot, so the
+ * calls of different slots overlap on the GPU.  No counterpart in the
+ * reference (its f2py module is not re-entrant).  pm_budget_bytes bounds
+ * the particle-mesh grid batches of the slot (0: the default of 8 GB).
+ * Calls on one slot are serialised; slots share the device's Green tables. */
+int32_t pyfof_slot_create(int32_t device, int64_t pm_budget_bytes, void **slot);
+int32_t pyfof_slot_destroy(void *slot);
+
+/* pyfof_run on a slot (same arguments, outputs and error codes). */
+int32_t pyfof_slot_run(void *slot, const double *xp, const double *vp, const double *mp,
+                       int32_t layout, const int32_t *np_halo, int32_t nhalo, int64_t total_np,
+                       double L_Box, double linking_length, int32_t np_halo_min, int32_t bound_check,
+                       int32_t verbose, double softening, double a_val, double b_val, double s_15_val,
+                       int32_t n_threads, int64_t ng_val, double ng_global_val, int32_t *in_halo,
+                       int32_t *halo_id, double *ang_mom);
+
+/* Statistics of the slot's last call (the pyfof_get_stat keys), plus
+ * "peak_bytes": the most device memory that call held at once. */
+int32_t pyfof_slot_stat(void *slot, const char *key, int64_t *value);
+
 #ifdef __cplusplus
 }
 #endif

@@ -34,7 +34,8 @@ _RUN_ARGS = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, 
 EXPORTED = ("pyfof_version", "pyfof_init", "pyfof_shutdown", "pyfof_last_error",
             "pyfof_set_option", "pyfof_set_stream", "pyfof_get_stat", "pyfof_last_link_ms", "pyfof_last_stage_ms",
             "pyfof_halo_potential", "pyfof_halo_potential_direct_static", "pyfof_run",
-            "pyfof_run_device")
+            "pyfof_run_device", "pyfof_slot_create", "pyfof_slot_destroy", "pyfof_slot_run",
+            "pyfof_slot_stat")
 
 
 class NativeLibraryError(RuntimeError):
@@ -80,6 +81,14 @@ def load():
         L.pyfof_run.argtypes = _RUN_ARGS
         L.pyfof_run_device.restype = ctypes.c_int32
         L.pyfof_run_device.argtypes = _RUN_ARGS
+        L.pyfof_slot_create.restype = ctypes.c_int32
+        L.pyfof_slot_create.argtypes = [ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(ctypes.c_void_p)]
+        L.pyfof_slot_destroy.restype = ctypes.c_int32
+        L.pyfof_slot_destroy.argtypes = [ctypes.c_void_p]
+        L.pyfof_slot_run.restype = ctypes.c_int32
+        L.pyfof_slot_run.argtypes = [ctypes.c_void_p] + list(_RUN_ARGS)
+        L.pyfof_slot_stat.restype = ctypes.c_int32
+        L.pyfof_slot_stat.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
         v = L.pyfof_version()
         if v != ABI_VERSION:
             raise NativeLibraryError(f"ABI version mismatch: library {v}, binding {ABI_VERSION}")
@@ -132,11 +141,12 @@ def _ptr(a):
 
 
 def run(xp, vp, mp, np_halo, nhalo, L_Box, link, np_halo_min, bound_check, verbose, softening,
-        a_val, b_val, s_15_val, n_threads, total_np, ng_val=256, ng_global_val=512.0):
+        a_val, b_val, s_15_val, n_threads, total_np, ng_val=256, ng_global_val=512.0, slot=None):
     """Host-memory call with the f2py argument order of fof_fortran.fof_fortran.
 
     xp, vp: (3,N) float64 arrays, C- or Fortran-contiguous (vp may be None);
-    mp: (N,) float64 or None.  Returns (in_halo, halo_id, ang_mom, ierr).
+    mp: (N,) float64 or None.  `slot`: a handle of slot_create, else the
+    default context.  Returns (in_halo, halo_id, ang_mom, ierr).
     """
     L = load()
     n = int(total_np)
@@ -157,13 +167,34 @@ def run(xp, vp, mp, np_halo, nhalo, L_Box, link, np_halo_min, bound_check, verbo
     in_halo = np.empty(n, dtype=np.int32)
     halo_id = np.empty(n, dtype=np.int32)
     ang_mom = np.zeros((3, max(int(nhalo), 0)), dtype=np.float64, order="F")
-    ierr = L.pyfof_run(_ptr(xp), _ptr(vp), _ptr(mp), layout, nph.ctypes.data_as(_i32p),
-                       int(nhalo), n, float(L_Box), float(link), int(np_halo_min),
-                       int(bound_check), int(verbose), float(softening), float(a_val),
-                       float(b_val), float(s_15_val), int(n_threads), int(ng_val),
-                       float(ng_global_val), _ptr(in_halo), _ptr(halo_id),
-                       ang_mom.ctypes.data_as(_dp))
+    args = (_ptr(xp), _ptr(vp), _ptr(mp), layout, nph.ctypes.data_as(_i32p),
+            int(nhalo), n, float(L_Box), float(link), int(np_halo_min),
+            int(bound_check), int(verbose), float(softening), float(a_val),
+            float(b_val), float(s_15_val), int(n_threads), int(ng_val),
+            float(ng_global_val), _ptr(in_halo), _ptr(halo_id), ang_mom.ctypes.data_as(_dp))
+    ierr = L.pyfof_run(*args) if slot is None else L.pyfof_slot_run(ctypes.c_void_p(slot), *args)
     return in_halo, halo_id, ang_mom, int(ierr)
+
+
+def slot_create(device=0, pm_budget_bytes=0):
+    """A slot of its own on `device` (calls on different slots overlap on
+    the GPU).  Returns the handle (an int)."""
+    h = ctypes.c_void_p()
+    if load().pyfof_slot_create(int(device), int(pm_budget_bytes), ctypes.byref(h)) != 0:
+        raise RuntimeError(last_error())
+    return h.value
+
+
+def slot_destroy(slot):
+    if load().pyfof_slot_destroy(ctypes.c_void_p(slot)) != 0:
+        raise RuntimeError(last_error())
+
+
+def slot_stat(slot, key):
+    v = ctypes.c_int64(0)
+    if load().pyfof_slot_stat(ctypes.c_void_p(slot), key.encode(), ctypes.byref(v)) != 0:
+        raise ValueError(last_error())
+    return int(v.value)
 
 
 def halo_potential(q, w, softening=0.1, a_val=1.0, s15=17.152, ng=256, fp64=False):

@@ -49,37 +49,57 @@ Context::~Context() {
   if (h_flags) cudaFreeHost(h_flags);
 }
 
+std::shared_ptr<GreenCache> g_green[64];
+
+// A context of its own: streams, status words, events; the Green tables are
+// shared by all contexts of a device.  Call with g_ctx_mu held.
+static int32_t create_context(int device, Context **out) {
+  if (device < 0 || device >= 64) {
+    set_error("invalid device %d", device);
+    return kInvalid;
+  }
+  int ndev = 0;
+  PYFOF_CUDA(cudaGetDeviceCount(&ndev));
+  if (device >= ndev) {
+    set_error("device %d not present (%d devices)", device, ndev);
+    return kInvalid;
+  }
+  PYFOF_CUDA(cudaSetDevice(device));
+  Context *c = new Context();
+  c->device = device;
+  if (!g_green[device]) g_green[device] = std::make_shared<GreenCache>();
+  c->green = g_green[device];
+  auto fail = [&](cudaError_t e) {
+    set_error("context creation: %s", cudaGetErrorString(e));
+    delete c;
+    return kCuda;
+  };
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+  c->stream = c->own_stream;
+  if ((e = cudaMalloc(&c->d_flags, sizeof(int32_t) * FLAG_COUNT)) != cudaSuccess) return fail(e);
+  if ((e = cudaMallocHost(&c->h_flags, sizeof(int32_t) * FLAG_COUNT)) != cudaSuccess) return fail(e);
+  for (auto &ev : c->ev)
+    if ((e = cudaEventCreate(&ev)) != cudaSuccess) return fail(e);
+  if ((e = cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+  if ((e = cudaEventCreateWithFlags(&c->ev_alloc, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+  if ((e = cudaEventCreateWithFlags(&c->ev_inputs, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+  cudaMemPool_t pool;
+  PYFOF_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+  uint64_t thr = UINT64_MAX;  // keep freed blocks cached in the pool
+  PYFOF_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  c->work.stream = c->stream;
+  *out = c;
+  return kOk;
+}
+
 int32_t get_context(int device, Context **out) {
   std::lock_guard<std::mutex> lk(g_ctx_mu);
   if (device < 0 || device >= 64) {
     set_error("invalid device %d", device);
     return kInvalid;
   }
-  if (!g_ctx[device]) {
-    int ndev = 0;
-    PYFOF_CUDA(cudaGetDeviceCount(&ndev));
-    if (device >= ndev) {
-      set_error("device %d not present (%d devices)", device, ndev);
-      return kInvalid;
-    }
-    PYFOF_CUDA(cudaSetDevice(device));
-    Context *c = new Context();
-    c->device = device;
-    PYFOF_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
-    c->stream = c->own_stream;
-    PYFOF_CUDA(cudaMalloc(&c->d_flags, sizeof(int32_t) * FLAG_COUNT));
-    PYFOF_CUDA(cudaMallocHost(&c->h_flags, sizeof(int32_t) * FLAG_COUNT));
-    for (auto &e : c->ev) PYFOF_CUDA(cudaEventCreate(&e));
-    PYFOF_CUDA(cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking));
-    PYFOF_CUDA(cudaEventCreateWithFlags(&c->ev_alloc, cudaEventDisableTiming));
-    PYFOF_CUDA(cudaEventCreateWithFlags(&c->ev_inputs, cudaEventDisableTiming));
-    cudaMemPool_t pool;
-    PYFOF_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
-    uint64_t thr = UINT64_MAX;  // keep freed blocks cached in the pool
-    PYFOF_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
-    c->work.stream = c->stream;
-    g_ctx[device] = c;
-  }
+  if (!g_ctx[device]) PYFOF_TRY(create_context(device, &g_ctx[device]));
   *out = g_ctx[device];
   return kOk;
 }
@@ -221,11 +241,7 @@ int32_t pyfof_set_stream(void *stream) {
   return kOk;
 }
 
-int32_t pyfof_get_stat(const char *key, int64_t *value) {
-  if (!key || !value) return kInvalid;
-  if (!std::strcmp(key, "launches")) { *value = g_launches.load(); return kOk; }
-  Context *c;
-  PYFOF_TRY(get_context(g_default_device, &c));
+static int32_t context_stat(const Context *c, const char *key, int64_t *value) {
   if (!std::strcmp(key, "cells")) { *value = c->last_cells; return kOk; }
   if (!std::strcmp(key, "active")) { *value = c->last_active; return kOk; }
   if (!std::strcmp(key, "candidates")) { *value = c->last_candidates; return kOk; }
@@ -236,8 +252,17 @@ int32_t pyfof_get_stat(const char *key, int64_t *value) {
   if (!std::strcmp(key, "refined_regions")) { *value = c->last_tl_regions; return kOk; }
   if (!std::strcmp(key, "pm_solves")) { *value = c->last_pm_solves; return kOk; }
   if (!std::strcmp(key, "pm_fft_bytes")) { *value = (int64_t)c->last_pm_fft_bytes; return kOk; }
+  if (!std::strcmp(key, "peak_bytes")) { *value = c->last_peak_bytes; return kOk; }
   set_error("unknown statistic %s", key);
   return kInvalid;
+}
+
+int32_t pyfof_get_stat(const char *key, int64_t *value) {
+  if (!key || !value) return kInvalid;
+  if (!std::strcmp(key, "launches")) { *value = g_launches.load(); return kOk; }
+  Context *c;
+  PYFOF_TRY(get_context(g_default_device, &c));
+  return context_stat(c, key, value);
 }
 
 int32_t pyfof_last_link_ms(float *ms) {
@@ -285,16 +310,12 @@ int32_t pyfof_halo_potential(const float *q, const float *w, int32_t np, double 
 // Host-memory call.  Positions are copied first on the call's stream; the
 // velocities and masses follow on the context's second stream and are
 // waited for only after the linking, so their copies overlap with it.
-static int32_t run_host(const double *xp, const double *vp, const double *mp, int32_t layout,
-                        const int32_t *np_halo, int32_t nhalo, int64_t total_np, double L_Box,
-                        double linking_length, int32_t np_halo_min, int32_t bound_check,
+static int32_t run_host(Context &ctx, const double *xp, const double *vp, const double *mp,
+                        int32_t layout, const int32_t *np_halo, int32_t nhalo, int64_t total_np,
+                        double L_Box, double linking_length, int32_t np_halo_min, int32_t bound_check,
                         int32_t verbose, double softening, double a_val, double b_val,
                         double s_15_val, int32_t n_threads, int64_t ng_val, double ng_global_val,
                         int32_t *in_halo, int32_t *halo_id, double *ang_mom) {
-  Context *cp;
-  PYFOF_TRY(get_context(g_default_device, &cp));
-  Context &ctx = *cp;
-  std::lock_guard<std::mutex> lk(ctx.mu);
   PYFOF_CUDA(cudaSetDevice(ctx.device));
   cudaStream_t s = ctx.stream;
   const size_t n = (size_t)total_np;
@@ -362,17 +383,22 @@ static int32_t run_host(const double *xp, const double *vp, const double *mp, in
     r = kCuda;
   }
   if (ctx.timing && r == kOk) record_stage_times(ctx);
+  ctx.last_peak_bytes = (int64_t)ctx.work.peak;
+  ctx.work.peak = 0;
   ctx.work.release();
   cudaStreamSynchronize(s);
   return r;
 }
 
-int32_t pyfof_run(const double *xp, const double *vp, const double *mp, int32_t layout,
-                  const int32_t *np_halo, int32_t nhalo, int64_t total_np, double L_Box,
-                  double linking_length, int32_t np_halo_min, int32_t bound_check,
-                  int32_t verbose, double softening, double a_val, double b_val,
-                  double s_15_val, int32_t n_threads, int64_t ng_val, double ng_global_val,
-                  int32_t *in_halo, int32_t *halo_id, double *ang_mom) {
+// The checks and output conventions of pyfof_run around run_host; ctx null
+// means the default device's context.
+static int32_t run_host_checked(Context *ctx, const double *xp, const double *vp, const double *mp,
+                                int32_t layout, const int32_t *np_halo, int32_t nhalo, int64_t total_np,
+                                double L_Box, double linking_length, int32_t np_halo_min,
+                                int32_t bound_check, int32_t verbose, double softening, double a_val,
+                                double b_val, double s_15_val, int32_t n_threads, int64_t ng_val,
+                                double ng_global_val, int32_t *in_halo, int32_t *halo_id,
+                                double *ang_mom) {
   // outputs are written in full on success and zeroed on every other path
   auto zero = [&]() {
     if (total_np > 0) {
@@ -394,14 +420,27 @@ int32_t pyfof_run(const double *xp, const double *vp, const double *mp, int32_t 
     set_error("vp is required when bound_check is set");
     r = kInvalid;
   }
+  if (r == kOk && !ctx) r = get_context(g_default_device, &ctx);
   if (r == kOk) {
     std::memset(ang_mom, 0, sizeof(double) * 3 * (size_t)nhalo);
-    r = run_host(xp, vp, mp, layout, np_halo, nhalo, total_np, L_Box, linking_length, np_halo_min,
-                 bound_check, verbose, softening, a_val, b_val, s_15_val, n_threads, ng_val,
-                 ng_global_val, in_halo, halo_id, ang_mom);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    r = run_host(*ctx, xp, vp, mp, layout, np_halo, nhalo, total_np, L_Box, linking_length,
+                 np_halo_min, bound_check, verbose, softening, a_val, b_val, s_15_val, n_threads,
+                 ng_val, ng_global_val, in_halo, halo_id, ang_mom);
   }
   if (r != kOk) zero();
   return r;
+}
+
+int32_t pyfof_run(const double *xp, const double *vp, const double *mp, int32_t layout,
+                  const int32_t *np_halo, int32_t nhalo, int64_t total_np, double L_Box,
+                  double linking_length, int32_t np_halo_min, int32_t bound_check,
+                  int32_t verbose, double softening, double a_val, double b_val,
+                  double s_15_val, int32_t n_threads, int64_t ng_val, double ng_global_val,
+                  int32_t *in_halo, int32_t *halo_id, double *ang_mom) {
+  return run_host_checked(nullptr, xp, vp, mp, layout, np_halo, nhalo, total_np, L_Box,
+                          linking_length, np_halo_min, bound_check, verbose, softening, a_val, b_val,
+                          s_15_val, n_threads, ng_val, ng_global_val, in_halo, halo_id, ang_mom);
 }
 
 int32_t pyfof_run_device(const double *d_xp, const double *d_vp, const double *d_mp,
@@ -462,6 +501,68 @@ int32_t pyfof_run_device(const double *d_xp, const double *d_vp, const double *d
     std::memset(ang_mom, 0, sizeof(double) * 3 * (size_t)nhalo);
   }
   return r;
+}
+
+// ---------------------------------------------------------------- slots
+// A slot is a context of its own (streams, scratch, status words) on one
+// device; calls on different slots run concurrently on the GPU.
+
+static bool valid_slot(void *slot) {
+  return slot && static_cast<Context *>(slot)->magic == Context::kMagic;
+}
+
+int32_t pyfof_slot_create(int32_t device, int64_t pm_budget_bytes, void **slot) {
+  if (!slot) {
+    set_error("pyfof_slot_create: null handle pointer");
+    return kInvalid;
+  }
+  *slot = nullptr;
+  Context *c = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    PYFOF_TRY(create_context(device, &c));
+  }
+  if (pm_budget_bytes > 0) c->pm_budget = (size_t)pm_budget_bytes;
+  *slot = c;
+  return kOk;
+}
+
+int32_t pyfof_slot_destroy(void *slot) {
+  if (!valid_slot(slot)) {
+    set_error("pyfof_slot_destroy: not a slot");
+    return kInvalid;
+  }
+  Context *c = static_cast<Context *>(slot);
+  {
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+  }
+  c->magic = 0;
+  delete c;
+  return kOk;
+}
+
+int32_t pyfof_slot_run(void *slot, const double *xp, const double *vp, const double *mp,
+                       int32_t layout, const int32_t *np_halo, int32_t nhalo, int64_t total_np,
+                       double L_Box, double linking_length, int32_t np_halo_min, int32_t bound_check,
+                       int32_t verbose, double softening, double a_val, double b_val, double s_15_val,
+                       int32_t n_threads, int64_t ng_val, double ng_global_val, int32_t *in_halo,
+                       int32_t *halo_id, double *ang_mom) {
+  if (!valid_slot(slot)) {
+    set_error("pyfof_slot_run: not a slot");
+    return kInvalid;
+  }
+  return run_host_checked(static_cast<Context *>(slot), xp, vp, mp, layout, np_halo, nhalo, total_np,
+                          L_Box, linking_length, np_halo_min, bound_check, verbose, softening, a_val,
+                          b_val, s_15_val, n_threads, ng_val, ng_global_val, in_halo, halo_id, ang_mom);
+}
+
+int32_t pyfof_slot_stat(void *slot, const char *key, int64_t *value) {
+  if (!valid_slot(slot) || !key || !value) {
+    set_error("pyfof_slot_stat: invalid arguments");
+    return kInvalid;
+  }
+  return context_stat(static_cast<Context *>(slot), key, value);
 }
 
 }  // extern "C"

@@ -67,6 +67,7 @@ struct Arena {
   std::vector<void *> ptrs;
   std::vector<size_t> sizes;
   size_t bytes = 0;      // held by this call
+  size_t peak = 0;       // most held at once since the last reset
   size_t last_fail = 0;  // size of the last request that failed
   template <class T>
   T *carve(size_t count) {
@@ -80,6 +81,7 @@ struct Arena {
     ptrs.push_back(p);
     sizes.push_back(b);
     bytes += b;
+    if (bytes > peak) peak = bytes;
     return reinterpret_cast<T *>(p);
   }
   void release() { release_to(0); }

@@ -10,7 +10,14 @@
 
 namespace pyfof {
 
-struct GreenTable;  // unbinding Green's function cache entry (unbind.cu)
+struct GreenTable;  // unbinding Green's function cache entry (unbind_pm.cu)
+
+// Green tables of one device, shared by all contexts of that device (they
+// are read-only once built; building one holds the lock).
+struct GreenCache {
+  std::mutex mu;
+  std::map<int64_t, std::shared_ptr<GreenTable>> tables;  // keyed by grid size and kind
+};
 
 // Device time of a launch group that repeats many times within one call
 // (bracketed by begin/end on the stream); collect() adds up the completed
@@ -43,6 +50,8 @@ struct GroupTimer {
 };
 
 struct Context {
+  static constexpr uint32_t kMagic = 0x50464f46u;
+  uint32_t magic = kMagic;  // cleared on destruction (slot handle check)
   int device = 0;
   cudaStream_t stream = nullptr;      // stream all work is issued on
   cudaStream_t own_stream = nullptr;  // the context's own stream (default)
@@ -52,7 +61,9 @@ struct Context {
   int32_t *d_flags = nullptr;  // device status words (error codes, counters)
   int32_t *h_flags = nullptr;  // pinned mirror
   std::mutex mu;
-  std::map<int64_t, std::shared_ptr<GreenTable>> green;  // keyed by grid size and kind
+  std::shared_ptr<GreenCache> green;
+  size_t pm_budget = (size_t)8 << 30;  // particle-mesh grid batch bytes
+  int64_t last_peak_bytes = 0;         // device memory the last call held at most
   cudaEvent_t ev[8] = {};
   // timing of the last call's stages (ms), filled when timing is enabled
   bool timing = false;

@@ -143,8 +143,9 @@ int32_t get_green(Context &ctx, int n, double soft, double range, int truncated,
                   std::shared_ptr<GreenTable> *out) {
   const int kind = range == 0.0 ? 0 : (range < 10.0 ? 1 : 2);
   const int64_t key = ((int64_t)n << 8) | (kind << 1) | (sizeof(R) == 8 ? 1 : 0);
-  auto it = ctx.green.find(key);
-  if (it != ctx.green.end()) { *out = it->second; return kOk; }
+  std::lock_guard<std::mutex> lk(ctx.green->mu);
+  auto it = ctx.green->tables.find(key);
+  if (it != ctx.green->tables.end()) { *out = it->second; return kOk; }
   auto t = std::make_shared<GreenTable>();
   t->n = n;
   t->fp64 = sizeof(R) == 8;
@@ -175,7 +176,7 @@ int32_t get_green(Context &ctx, int n, double soft, double range, int truncated,
     set_error("Green's function: zero assignment response");
     return kInvalid;
   }
-  ctx.green[key] = t;
+  ctx.green->tables[key] = t;
   *out = t;
   return kOk;
 }
@@ -1327,7 +1328,7 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
 
   // grid batches per class, bounded by a spectrum budget; one scratch area,
   // sized for the largest batch, serves every batch of every pass
-  const size_t budget = (size_t)8 << 30;
+  const size_t budget = ctx.pm_budget;
   auto round256 = [](size_t b) { return (b + 255) & ~(size_t)255; };
   auto batch_bytes = [&](int n, int nb) {
     const size_t sup = n / 2 + 1;
