@@ -475,18 +475,121 @@ def run_b200(args):
     return 0
 
 
+def serve_pool(seed=0, count=24):
+    """Distinct requests of the serving configuration, reduced: sizes
+    log-uniform on [1e4, 1e6] particles (the configuration goes to 1e8), the
+    64^3 recipe scaled to L_Box = N^(1/3) (64 halos per 262,144 particles);
+    every second request with unbinding (lognormal masses), half of those in
+    physical units; ng_global = 512 keeps s_15 above the candidate spans."""
+    from py_fof_b200 import workloads as W
+    rng = np.random.default_rng(seed)
+    pool = []
+    for k in range(count):
+        n = int(10 ** rng.uniform(4.0, 6.0))
+        L = float(n ** (1.0 / 3.0))
+        bound = k % 2 == 1
+        d = W.plummer_box(n, L, max(1, round(64 * n / 262144)), seed=seed * 1000 + k,
+                          with_velocities=bound, lognormal_mass=0.3 if bound else None)
+        kw = dict(L_Box=L, linking_length=LINK, np_halo_min=NP_MIN, ng_global=512.0)
+        if bound:
+            kw.update(vp_list=d["vp"], mp_list=d["mp"], bound_check=True, softening=SOFTENING)
+            if k % 4 == 3:
+                kw.update(units="physical", softening=0.05)
+        pool.append((d["xp"], kw, n))
+    return pool
+
+
+def _serve_run(pool, order, arrivals, slots):
+    """Submit pool[order[i]] at arrivals[i] (seconds from start); returns
+    (latencies ms, makespan s, particles, max concurrent)."""
+    from py_fof_b200 import serve
+    srv = serve.Server(slots=slots)
+    t0 = time.perf_counter()
+    futs = []
+    for i, k in enumerate(order):
+        dt = t0 + arrivals[i] - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        x, kw, _ = pool[k]
+        futs.append(srv.submit(x, **kw))
+    for f in futs:
+        f.result()
+    t1 = time.perf_counter()
+    lat = srv.latencies_ms()
+    most = srv.max_running
+    srv.close()
+    return lat, t1 - t0, sum(pool[k][2] for k in order), most
+
+
+def run_serve(args):
+    """--workload serve: requests with Poisson arrivals, served by the
+    continuous-batching loop (4 slots) and, on the same arrival times, one at
+    a time (1 slot); p50/p99 latency and throughput of both."""
+    import torch
+    import py_fof_b200 as P
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    pool = serve_pool(args.seed)
+    # calibration: every pool request alone (also builds the Green tables)
+    for x, kw, _ in pool:
+        P.fof_with_info(x, **kw)
+    svc = []
+    for x, kw, _ in pool:
+        t = time.perf_counter()
+        P.fof_with_info(x, **kw)
+        svc.append(time.perf_counter() - t)
+    rate = 1.25 / float(np.mean(svc))  # offered load: 1.25x one-at-a-time capacity
+    nreq = 30 * max(1, args.steps)
+    rng = np.random.default_rng(args.seed + 1)
+    order = rng.integers(0, len(pool), nreq)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    res = {}
+    for name, slots in (("one_at_a_time", 1), ("served", 4)):
+        lat, span, parts, most = _serve_run(pool, order, arrivals, slots)
+        res[name] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                     "req_per_s": nreq / span, "mpart_per_s": parts / span / 1e6, "slots": slots,
+                     "max_concurrent": most}
+    if rank != 0:
+        return 0
+    s = res["served"]
+    h2d = float(np.mean([24 * n * (2 if "vp_list" in kw else 1) + (8 * n if "mp_list" in kw else 0)
+                         for _, kw, n in (pool[k] for k in order)]))
+    line = {
+        "metric": "serve_mpart_per_s", "value": s["mpart_per_s"], "unit": "Mpart/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": 1, "ms_per_step": 1e3 / s["req_per_s"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 linking; f32 unbinding", "data": "synthetic",
+        "config": {"workload": "serve", "requests": nreq, "distinct_inputs": len(pool),
+                   "sizes": "log-uniform 1e4..1e6", "offered_req_per_s": rate,
+                   "arrivals": "Poisson", "unbinding_share": 0.5},
+        "serve": res,
+        "e2e": {"value": s["mpart_per_s"], "unit": "Mpart/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": float(np.mean([8 * pool[k][2] for k in order]))},
+        "service_alone_ms": {"mean": 1e3 * float(np.mean(svc)), "max": 1e3 * float(np.max(svc))},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="fof_unbind_256", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="fof_unbind_256", choices=sorted(WORKLOADS) + ["serve"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-run", action="store_true",
                     help="run only the warm-up and timed steps of the default path")
     args = ap.parse_args()
+    if args.workload == "serve":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop; "
+                              "its per-request CPU cost is the cpu_baseline of the box workloads"}))
+            return 0
+        return run_serve(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)
