@@ -723,29 +723,50 @@ __global__ void tl_target_kernel(const int32_t *__restrict__ preg, int64_t M,
 
 // Node range checks of sources and targets, and the inner self term of
 // every target (:729-800).
-template <typename R>
-__global__ void tl_setup_kernel(const Members m, const PmHalo *__restrict__ H,
+// Last entry e0 of the ascending array off[0..n] with off[e0] <= idx.
+__device__ __forceinline__ int seg_of(const uint32_t *__restrict__ off, int n, uint32_t idx) {
+  int lo = 0, hi = n;  // off[lo] <= idx < off[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= idx) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Set-up of the refined regions, flat over all their sources and targets:
+// every source must fall inside its region's inner grid, and every target
+// gets its inner self term.
+__global__ void tl_check_kernel(const Members m, const PmHalo *__restrict__ H,
                                 const TlRegion *__restrict__ A, int na,
                                 const uint32_t *__restrict__ src_start, const uint32_t *__restrict__ src,
-                                const uint32_t *__restrict__ tgt_start, const uint32_t *__restrict__ tgt,
-                                const R *__restrict__ self2, const R *__restrict__ self4,
-                                R *__restrict__ self_in, int32_t *flags) {
-  const int a = blockIdx.x;
-  if (a >= na) return;
-  const TlRegion &Rg = A[a];
-  const PmHalo &p = H[Rg.h];
-  for (uint32_t e = src_start[a] + threadIdx.x; e < src_start[a + 1]; e += blockDim.x) {
+                                int32_t *flags) {
+  const uint32_t total = src_start[na];
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const int a = seg_of(src_start, na, e);
+    const TlRegion &Rg = A[a];
     float t[3], w9[9];
     int f[3];
-    tl_t(m, p, src[e], t);
+    tl_t(m, H[Rg.h], src[e], t);
     if (!tl_tsc(Rg, t, f, w9)) atomicCAS(&flags[FLAG_ERR], 0, kInvalid);
   }
-  const R *sp = Rg.r == 2 ? self2 : self4;
-  for (uint32_t e = tgt_start[a] + threadIdx.x; e < tgt_start[a + 1]; e += blockDim.x) {
+}
+
+template <typename R>
+__global__ void tl_self_kernel(const Members m, const PmHalo *__restrict__ H,
+                               const TlRegion *__restrict__ A, int na,
+                               const uint32_t *__restrict__ tgt_start, const uint32_t *__restrict__ tgt,
+                               const R *__restrict__ self2, const R *__restrict__ self4,
+                               R *__restrict__ self_in, int32_t *flags) {
+  const uint32_t total = tgt_start[na];
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const int a = seg_of(tgt_start, na, e);
+    const TlRegion &Rg = A[a];
+    const R *sp = Rg.r == 2 ? self2 : self4;
     const int64_t k = tgt[e];
     float t[3], w9[9];
     int f[3];
-    tl_t(m, p, k, t);
+    tl_t(m, H[Rg.h], k, t);
     if (!tl_tsc(Rg, t, f, w9)) { atomicCAS(&flags[FLAG_ERR], 0, kInvalid); continue; }
     double acc = 0.0;
     for (int sz = 0; sz < 3; ++sz)
@@ -769,15 +790,19 @@ __global__ void tl_setup_kernel(const Members m, const PmHalo *__restrict__ H,
 template <typename R>
 __global__ void tl_deposit_kernel(const Members m, const PmHalo *__restrict__ H,
                                   const TlRegion *__restrict__ A, const int32_t *__restrict__ batch,
+                                  const uint32_t *__restrict__ bpre, int nb,
                                   const uint32_t *__restrict__ src_start, const uint32_t *__restrict__ src,
                                   const uint8_t *__restrict__ keep, int sup, R *__restrict__ rho) {
-  const int a = batch[blockIdx.x];
-  const TlRegion &Rg = A[a];
-  const PmHalo &p = H[Rg.h];
-  R *g = rho + (int64_t)blockIdx.x * sup * sup * sup;
-  for (uint32_t e = src_start[a] + threadIdx.x; e < src_start[a + 1]; e += blockDim.x) {
-    const int64_t k = src[e];
+  // flat over the sources of the batch: bpre[j] = first index of region j
+  const uint32_t total = bpre[nb];
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    const int j = seg_of(bpre, nb, idx);
+    const int a = batch[j];
+    const TlRegion &Rg = A[a];
+    const PmHalo &p = H[Rg.h];
+    const int64_t k = src[src_start[a] + (idx - bpre[j])];
     if (!keep[k]) continue;
+    R *g = rho + (int64_t)j * sup * sup * sup;
     float t[3], w9[9];
     int f[3];
     tl_t(m, p, k, t);
@@ -796,17 +821,20 @@ __global__ void tl_deposit_kernel(const Members m, const PmHalo *__restrict__ H,
 template <typename R>
 __global__ void tl_gather_kernel(const Members m, const PmHalo *__restrict__ H,
                                  const TlRegion *__restrict__ A, const int32_t *__restrict__ batch,
+                                 const uint32_t *__restrict__ bpre, int nb,
                                  const uint32_t *__restrict__ tgt_start, const uint32_t *__restrict__ tgt,
                                  const uint8_t *__restrict__ keep, const R *__restrict__ self_in, int sup,
                                  const R *__restrict__ rho, double a_val, R *__restrict__ phi_in) {
-  const int a = batch[blockIdx.x];
-  const TlRegion &Rg = A[a];
-  const PmHalo &p = H[Rg.h];
-  const R *g = rho + (int64_t)blockIdx.x * sup * sup * sup;
-  const R pref = (R)(a_val * (double)Rg.r / (6.0 * kPi * (double)p.spacing));
-  for (uint32_t e = tgt_start[a] + threadIdx.x; e < tgt_start[a + 1]; e += blockDim.x) {
-    const int64_t k = tgt[e];
+  const uint32_t total = bpre[nb];
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    const int j = seg_of(bpre, nb, idx);
+    const int a = batch[j];
+    const TlRegion &Rg = A[a];
+    const PmHalo &p = H[Rg.h];
+    const int64_t k = tgt[tgt_start[a] + (idx - bpre[j])];
     if (!keep[k]) continue;
+    const R *g = rho + (int64_t)j * sup * sup * sup;
+    const R pref = (R)(a_val * (double)Rg.r / (6.0 * kPi * (double)p.spacing));
     float t[3], w9[9];
     int f[3];
     tl_t(m, p, k, t);
@@ -1312,9 +1340,13 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
       R *self_in = c1;  // reuse: c1 is rewritten every pass, self_in must persist -> own array
       self_in = W.carve<R>(M);
       if (!self_in) { set_error("workspace exhausted (two-level self)"); return kAlloc; }
-      tl_setup_kernel<R><<<na, BLK, 0, s>>>(m, dH, dA, na, src_start, src, tgt_start, tgt,
-                                            g_r2 ? (const R *)g_r2->self : nullptr,
-                                            g_r4 ? (const R *)g_r4->self : nullptr, self_in, ctx.d_flags);
+      const unsigned gs = (unsigned)std::min<int64_t>(ceil_div(std::max<uint32_t>(hsrc[na], 1), BLK), 148 * 16);
+      tl_check_kernel<<<gs, BLK, 0, s>>>(m, dH, dA, na, src_start, src, ctx.d_flags);
+      PYFOF_CHECK_LAUNCH();
+      const unsigned gt = (unsigned)std::min<int64_t>(ceil_div(std::max<uint32_t>(htgt[na], 1), BLK), 148 * 16);
+      tl_self_kernel<R><<<gt, BLK, 0, s>>>(m, dH, dA, na, tgt_start, tgt,
+                                           g_r2 ? (const R *)g_r2->self : nullptr,
+                                           g_r4 ? (const R *)g_r4->self : nullptr, self_in, ctx.d_flags);
       PYFOF_CHECK_LAUNCH();
       tl_self_in = self_in;
     }
@@ -1350,7 +1382,8 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
   unsigned char *scratch = W.carve<unsigned char>(scratch_bytes);
   int32_t *dpend = W.carve<int32_t>(nh), *dslot = W.carve<int32_t>(nh);
   int32_t *dbatch = W.carve<int32_t>(std::max(na, 1));
-  if (!scratch || !dpend || !dslot || !dbatch) { set_error("workspace exhausted (PM grids)"); return kAlloc; }
+  uint32_t *dbpre = W.carve<uint32_t>(2 * (size_t)(std::max(na, 1) + 1));
+  if (!scratch || !dpend || !dslot || !dbatch || !dbpre) { set_error("workspace exhausted (PM grids)"); return kAlloc; }
   for (int pass = 1; pass <= kMaxPasses; ++pass) {
     std::vector<int32_t> pend;
     for (int h = 0; h < nh; ++h) if (H[h].pending) pend.push_back(h);
@@ -1400,19 +1433,30 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
         const int nb = (int)std::min<size_t>(maxb, regs.size() - g0);
         R *rho = reinterpret_cast<R *>(scratch);
         cplx_t<R> *spec = reinterpret_cast<cplx_t<R> *>(scratch + round256(sizeof(R) * (size_t)nb * sup * sup * sup));
+        // prefix counts of the batch's sources and targets (flat launches)
+        std::vector<uint32_t> bp(2 * (size_t)(nb + 1), 0);
+        for (int j = 0; j < nb; ++j) {
+          const int ia = regs[g0 + j];
+          bp[j + 1] = bp[j] + (hsrc[ia + 1] - hsrc[ia]);
+          bp[nb + 1 + j + 1] = bp[nb + 1 + j] + (htgt[ia + 1] - htgt[ia]);
+        }
         PYFOF_CUDA(cudaMemcpyAsync(dbatch, regs.data() + g0, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s));
+        PYFOF_CUDA(cudaMemcpyAsync(dbpre, bp.data(), sizeof(uint32_t) * bp.size(), cudaMemcpyHostToDevice, s));
         const int64_t ng = (int64_t)nb * sup * sup * sup;
         pm_zero_kernel<R><<<(unsigned)std::min<int64_t>(ceil_div(ng, BLK), 148 * 16), BLK, 0, s>>>(rho, ng);
         PYFOF_CHECK_LAUNCH();
-        tl_deposit_kernel<R><<<nb, BLK, 0, s>>>(m, dH, dA, dbatch, src_start, src, keep, sup, rho);
+        const unsigned gd = (unsigned)std::min<int64_t>(ceil_div(std::max<uint32_t>(bp[nb], 1), BLK), 148 * 16);
+        tl_deposit_kernel<R><<<gd, BLK, 0, s>>>(m, dH, dA, dbatch, dbpre, nb, src_start, src, keep, sup, rho);
         PYFOF_CHECK_LAUNCH();
         if (ctx.timing) ctx.conv_timer.begin(s);
         PYFOF_TRY(pm_convolve_batch<R>(rho, spec, gin, nin, sup, nb, s));
         if (ctx.timing) ctx.conv_timer.end(s);
         ctx.last_pm_solves += nb;
         ctx.last_pm_fft_bytes += 16.0 * nb * (nin + 2.0) * nin * nin;
-        tl_gather_kernel<R><<<nb, BLK, 0, s>>>(m, dH, dA, dbatch, tgt_start, tgt, keep, tl_self_in, sup, rho,
-                                               a.a_val, phi_in);
+        const unsigned gg = (unsigned)std::min<int64_t>(
+            ceil_div(std::max<uint32_t>(bp[2 * nb + 1], 1), BLK), 148 * 16);
+        tl_gather_kernel<R><<<gg, BLK, 0, s>>>(m, dH, dA, dbatch, dbpre + nb + 1, nb, tgt_start, tgt, keep,
+                                               tl_self_in, sup, rho, a.a_val, phi_in);
         PYFOF_CHECK_LAUNCH();
       }
     }
