@@ -52,7 +52,9 @@ int32_t pyfof_last_error(char *buf, int64_t len);
 
 /* Library options: "unbind_fp64" (1 = FP64 unbinding, batched; 0 = FP32
  * product path), "unbind_per_halo" (1 = the plain FP64 baseline: one halo per
- * launch sequence), "timing" (1 = record stage times). */
+ * launch sequence), "timing" (1 = record stage times), "unbind_big_np"
+ * (particle-mesh halos above this many members run their removal loop
+ * spread over the whole GPU; 0 = the default of 32768). */
 int32_t pyfof_set_option(const char *key, int64_t value);
 
 /* Issue all later work of the selected device on `stream` (a cudaStream_t;

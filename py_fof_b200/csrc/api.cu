@@ -21,6 +21,7 @@ int g_default_device = 0;
 int g_bound_fp64 = 0;
 int g_bound_per_halo = 0;
 int g_timing = 0;
+int64_t g_big_np = 0;
 }  // namespace
 
 void set_error(const char *fmt, ...) {
@@ -181,6 +182,7 @@ static int32_t run_common(Context &ctx, FofArgs &a) {
   ctx.timing = g_timing != 0;
   a.bound_fp64 = g_bound_fp64;
   a.bound_per_halo = g_bound_per_halo;
+  a.big_np = g_big_np;
   int32_t r = fof_run(ctx, a);
   note_alloc_failure(ctx, r);
   cudaError_t e = cudaStreamSynchronize(ctx.stream);
@@ -226,6 +228,7 @@ int32_t pyfof_set_option(const char *key, int64_t value) {
   if (!std::strcmp(key, "unbind_fp64")) { g_bound_fp64 = value != 0; return kOk; }
   if (!std::strcmp(key, "unbind_per_halo")) { g_bound_per_halo = value != 0; return kOk; }
   if (!std::strcmp(key, "timing")) { g_timing = value != 0; return kOk; }
+  if (!std::strcmp(key, "unbind_big_np")) { g_big_np = value; return kOk; }
   set_error("unknown option %s", key);
   return kInvalid;
 }
@@ -368,6 +371,7 @@ static int32_t run_host(Context &ctx, const double *xp, const double *vp, const 
   ctx.timing = g_timing != 0;
   a.bound_fp64 = g_bound_fp64;
   a.bound_per_halo = g_bound_per_halo;
+  a.big_np = g_big_np;
   int32_t r = fof_run(ctx, a);
   note_alloc_failure(ctx, r);
   if (r == kOk) {

@@ -23,6 +23,7 @@ struct FofArgs {
   double ng_global = 512.0;
   int32_t bound_fp64 = 0;  // 1: plain FP64 unbinding path instead of the FP32 product path
   int32_t bound_per_halo = 0;  // 1: FP64, one halo per launch sequence (the plain baseline)
+  int64_t big_np = 0;          // PM halos above this many members use the chunked removal loop (0: default)
   // recorded when vp and mp are on the device (they may still be copying
   // while the linking runs); null when they are already there
   cudaEvent_t inputs_ready = nullptr;

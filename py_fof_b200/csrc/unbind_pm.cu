@@ -447,6 +447,28 @@ __device__ __forceinline__ T c2_delta(T r, T ht, T hs) {
 // coalesced batches of 32; a source enters the pair loop only if it lies
 // within the chunk's largest cutoff of the chunk's bounding box, so the
 // divergent pair arithmetic runs almost only on pairs that interact.
+// FP32 product path of the short-range kernel: the spline-softened 1/r of
+// depth_c with its divisions replaced by products with per-h reciprocals and
+// 1/r from rsqrtf (a few ulps; the FP64 path keeps the divisions).
+struct DepthConst {
+  float h, two_over_h, inv70h, six_h;
+};
+__device__ __forceinline__ DepthConst depth_const(float h) {
+  return DepthConst{h, 2.0f / h, 1.0f / (70.0f * h), 6.0f * h};
+}
+__device__ __forceinline__ float depth_fast(float r, float rinv, const DepthConst &c) {
+  if (r >= c.h) return rinv;
+  const float e = r * c.two_over_h;
+  if (e <= 1.0f) {
+    const float prim = e * e * (112.0f + e * e * (-56.0f + e * (14.0f + e * (8.0f - 3.0f * e))));
+    return (208.0f - prim) * c.inv70h;
+  }
+  // 12/e = 6 h / r
+  const float prim = e * e * (448.0f + e * (-280.0f + e * (56.0f + e * (14.0f + e * (-8.0f + e))))) -
+                     224.0f * e - c.six_h * rinv;
+  return (128.0f - prim) * c.inv70h;
+}
+
 struct SrChunk {
   uint32_t cell, e0;
 };
@@ -502,6 +524,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) sr_gather_kernel(
     const R eps = (R)(double)(float)app;
     const R fac = (R)(a_val / (6.0 * kPi));
     const bool tl = p.two_level != 0;
+    const DepthConst k_eps = depth_const((float)eps), k_ai = depth_const((float)ai);
     R acc = 0, comp = 0;
     for (int64_t z = cz - kk; z <= cz + kk; ++z) {
       if (z < 0 || z >= n2) continue;
@@ -545,8 +568,14 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) sr_gather_kernel(
                 }
                 const R r2 = dx * dx + dy * dy + dz * dz;
                 if (r2 < a2) {
-                  const R d = sqrt(r2);
-                  const R dphi = -(fac * (depth_c<R>(d, eps) - depth_c<R>(d, ai)));
+                  R dphi;
+                  if constexpr (sizeof(R) == 4) {
+                    const float rinv = rsqrtf(r2), d = r2 * rinv;
+                    dphi = -(fac * (depth_fast(d, rinv, k_eps) - depth_fast(d, rinv, k_ai)));
+                  } else {
+                    const R d = sqrt(r2);
+                    dphi = -(fac * (depth_c<R>(d, eps) - depth_c<R>(d, ai)));
+                  }
                   const R yv = (R)jw * dphi - comp;
                   const R tt = acc + yv;
                   comp = (tt - acc) - yv;
@@ -1033,6 +1062,293 @@ __global__ void __launch_bounds__(IBLK) pm_inner_kernel(const Members m, PmHalo 
   }
 }
 
+// ------------------------------------------------- removal of large halos
+// Halos above kBigNp members run the same removal loop as pm_inner_kernel,
+// but spread over the whole GPU: their members are cut into chunks of
+// kChunk, every sweep is a grid of chunk blocks, and the per-halo decisions
+// (centre, selection, stop conditions) are small kernels between sweeps,
+// driven by a host loop.  The unbound members of an iteration are compacted
+// into a per-halo list, so the radix select runs over that list only.
+
+constexpr int64_t kBigNp = 32768;  // default; option "unbind_big_np" overrides
+constexpr int kChunk = 8192;
+
+struct BigHalo {
+  int32_t h;          // index into the PM halo table
+  int32_t active;     // still in this pass's inner loop
+  int64_t off, np;    // members
+  int64_t uoff;       // first slot of the halo's unbound list
+  int32_t chunk0, nchunk;
+  int32_t np_bound, deleted, n_source, status;
+  int32_t nu, nb;
+  float qc[3], vc[3];
+};
+
+struct BigChunk {
+  int32_t b;          // big halo
+  int64_t start, end; // member range
+};
+
+// phi = (c1 + in) + c2 of the kept members at the start of a pass
+template <typename R>
+__global__ void big_phi_kernel(const BigChunk *__restrict__ ch, int nch, const BigHalo *__restrict__ B,
+                               const uint8_t *__restrict__ keep, const R *__restrict__ c1,
+                               const R *__restrict__ in, const R *__restrict__ c2, float *__restrict__ phi,
+                               int32_t *flags) {
+  const BigChunk c = ch[blockIdx.x];
+  const BigHalo &bh = B[c.b];
+  if (!bh.active) return;
+  bool bad = false;
+  for (int64_t k = c.start + threadIdx.x; k < c.end; k += blockDim.x) {
+    if (!keep[k]) continue;
+    float v = (float)((c1[k] + in[k]) + c2[k]);
+    if (bh.np_bound == 1 || bh.n_source == 1) v = 0.0f;
+    bad |= !isfinite(v);
+    phi[k] = v;
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicCAS(&flags[FLAG_ERR], 0, kNonFinite);
+}
+
+// per-chunk sums of w, w q, w v over the kept members
+__global__ void big_com_kernel(const Members m, const BigChunk *__restrict__ ch, const BigHalo *__restrict__ B,
+                               const uint8_t *__restrict__ keep, double *__restrict__ part) {
+  const BigChunk c = ch[blockIdx.x];
+  if (!B[c.b].active) return;
+  double a7[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int64_t k = c.start + threadIdx.x; k < c.end; k += blockDim.x) {
+    if (!keep[k]) continue;
+    const double wi = (double)m.w[k];
+    a7[0] += wi;
+    for (int d = 0; d < 3; ++d) { a7[1 + d] += wi * (double)m.q[d][k]; a7[4 + d] += wi * (double)m.v[d][k]; }
+  }
+  __shared__ double red[32];
+  for (int j = 0; j < 7; ++j) {
+    const double t = bsum_d(a7[j], red);
+    if (threadIdx.x == 0) part[7 * (int64_t)blockIdx.x + j] = t;
+  }
+}
+
+// per big halo: centre from the chunk sums (in chunk order)
+__global__ void big_center_kernel(BigHalo *__restrict__ B, int nbig, const double *__restrict__ part,
+                                  int32_t *__restrict__ ucount) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbig) return;
+  BigHalo &bh = B[b];
+  ucount[b] = 0;
+  if (!bh.active) return;
+  double a7[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int c = bh.chunk0; c < bh.chunk0 + bh.nchunk; ++c)
+    for (int j = 0; j < 7; ++j) a7[j] += part[7 * (int64_t)c + j];
+  for (int d = 0; d < 3; ++d) {
+    bh.qc[d] = __double2float_rn(a7[1 + d] / a7[0]);
+    bh.vc[d] = __double2float_rn(a7[4 + d] / a7[0]);
+  }
+}
+
+// energies of the kept members; the unbound ones join the halo's list
+__global__ void big_energy_kernel(const Members m, const BigChunk *__restrict__ ch, const BigHalo *__restrict__ B,
+                                  const uint8_t *__restrict__ keep, const float *__restrict__ phi,
+                                  float *__restrict__ en, float b_val, int32_t *__restrict__ ucount,
+                                  uint32_t *__restrict__ ulist, int32_t *flags) {
+  const BigChunk c = ch[blockIdx.x];
+  const BigHalo &bh = B[c.b];
+  if (!bh.active) return;
+  bool bad = false;
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = c.start; base < c.end; base += blockDim.x) {
+    const int64_t k = base + threadIdx.x;
+    bool unb = false;
+    if (k < c.end && keep[k]) {
+      float s = 0.f;
+      for (int d = 0; d < 3; ++d) {
+        const float dv = __fadd_rn(__fsub_rn(m.v[d][k], bh.vc[d]), __fmul_rn(b_val, __fsub_rn(m.q[d][k], bh.qc[d])));
+        s = d == 0 ? __fmul_rn(dv, dv) : __fadd_rn(s, __fmul_rn(dv, dv));
+      }
+      const float e = __fadd_rn(__fdiv_rn(s, 2.0f), phi[k]);
+      bad |= !isfinite(e);
+      en[k] = e;
+      unb = e >= 0.0f;
+    }
+    // warp-aggregated append
+    const unsigned bal = __ballot_sync(0xffffffffu, unb);
+    int basepos = 0;
+    if (lane == 0 && bal) basepos = atomicAdd(&ucount[c.b], __popc(bal));
+    basepos = __shfl_sync(0xffffffffu, basepos, 0);
+    if (unb) ulist[bh.uoff + basepos + __popc(bal & ((1u << lane) - 1u))] = (uint32_t)(k - bh.off);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicCAS(&flags[FLAG_ERR], 0, kInvalid);
+}
+
+// per big halo, one block: the nb most unbound members leave (radix select
+// over the compact list; equal energies: lower index first), then the stop
+// conditions of the inner loop
+__global__ void __launch_bounds__(IBLK) big_select_kernel(BigHalo *__restrict__ B, const int32_t *__restrict__ ucount,
+                                                          const uint32_t *__restrict__ ulist,
+                                                          uint32_t *__restrict__ eqbuf,
+                                                          const float *__restrict__ en,
+                                                          uint8_t *__restrict__ keep, uint8_t *__restrict__ jd,
+                                                          int nmin, int32_t *__restrict__ nactive,
+                                                          const int32_t *flags) {
+  BigHalo &bh = B[blockIdx.x];
+  if (!bh.active) return;
+  __shared__ unsigned hist[IBLK / 32][64];  // per-warp 6-bit digit histograms
+  __shared__ unsigned tot[64];
+  __shared__ int s_digit, s_above, s_neq;
+  if (flags[FLAG_ERR]) {  // a sweep failed: stop, the host reports it
+    if (threadIdx.x == 0) { bh.active = 0; atomicSub(nactive, 1); }
+    return;
+  }
+  const int nu = ucount[blockIdx.x];
+  if (nu == 0) {
+    if (threadIdx.x == 0) {
+      if (bh.deleted == 0) bh.status = 0;
+      bh.active = 0;
+      atomicSub(nactive, 1);
+    }
+    return;
+  }
+  const int nb = min(nu, max(1, (int)ceil(0.02 * (double)bh.np_bound)));
+  const uint32_t *L = ulist + bh.uoff;
+  const float *E = en + bh.off;
+  const int warp = threadIdx.x >> 5;
+  unsigned prefix = 0, mask = 0;
+  int need = nb;
+  // 32-bit keys in digits of 6 bits from the top: 2 + 5 x 6
+  for (int shift = 30; shift >= 0; shift -= 6) {
+    const int bits = shift == 30 ? 2 : 6;
+    const unsigned dm = (1u << bits) - 1u;
+    for (int t = threadIdx.x; t < (IBLK / 32) * 64; t += IBLK) (&hist[0][0])[t] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < nu; i += IBLK) {
+      const unsigned key = __float_as_uint(E[L[i]] + 0.0f);
+      if ((key & mask) != prefix) continue;
+      atomicAdd(&hist[warp][(key >> shift) & dm], 1u);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 64; t += IBLK) {
+      unsigned s = 0;
+      for (int w = 0; w < IBLK / 32; ++w) s += hist[w][t];
+      tot[t] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int digit = (int)dm, above = 0;
+      for (; digit >= 0; --digit) {
+        const int c = (int)tot[digit];
+        if (above + c >= need) break;
+        above += c;
+      }
+      s_digit = digit;
+      s_above = above;
+    }
+    __syncthreads();
+    need -= s_above;
+    prefix |= (unsigned)s_digit << shift;
+    mask |= dm << shift;
+    __syncthreads();
+  }
+  const unsigned thr = prefix;
+  if (threadIdx.x == 0) s_neq = 0;
+  __syncthreads();
+  uint32_t *EQ = eqbuf + bh.uoff;
+  for (int i = threadIdx.x; i < nu; i += IBLK) {
+    const uint32_t li = L[i];
+    const unsigned key = __float_as_uint(E[li] + 0.0f);
+    if (key > thr) {
+      keep[bh.off + li] = 0;
+      jd[bh.off + li] = 1;
+    } else if (key == thr) {
+      EQ[atomicAdd(&s_neq, 1)] = li;
+    }
+  }
+  __syncthreads();
+  const int neq = s_neq;
+  for (int i = threadIdx.x; i < neq; i += IBLK) {
+    const uint32_t li = EQ[i];
+    int rank = 0;
+    for (int j = 0; j < neq; ++j) rank += EQ[j] < li;
+    if (rank < need) {
+      keep[bh.off + li] = 0;
+      jd[bh.off + li] = 1;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bh.np_bound -= nb;
+    bh.deleted += nb;
+    if (bh.np_bound < nmin) {
+      bh.status = 1;
+      bh.active = 0;
+      atomicSub(nactive, 1);
+    } else if ((double)bh.deleted >= 0.2 * (double)bh.np_bound) {
+      bh.active = 0;
+      atomicSub(nactive, 1);
+    }
+  }
+}
+
+// the pass's outcome back into the PM halo table
+__global__ void big_finish_kernel(const BigHalo *__restrict__ B, int nbig, PmHalo *__restrict__ H) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbig) return;
+  const BigHalo &bh = B[b];
+  PmHalo &p = H[bh.h];
+  if (!p.pending) return;
+  p.np_bound = bh.np_bound;
+  p.status = bh.status;
+  if (bh.status >= 0) p.pending = 0;
+}
+
+// start of a pass: the pending big halos enter the inner loop
+__global__ void big_start_kernel(BigHalo *__restrict__ B, int nbig, const PmHalo *__restrict__ H, int phi_only,
+                                 int32_t *__restrict__ nactive) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbig) return;
+  BigHalo &bh = B[b];
+  const PmHalo &p = H[bh.h];
+  bh.active = p.pending ? 1 : 0;
+  bh.np_bound = p.np_bound;
+  bh.n_source = p.np_bound;
+  bh.deleted = 0;
+  bh.status = -1;
+  if (bh.active) atomicAdd(nactive, 1);
+  (void)phi_only;
+}
+
+__global__ void big_phi_only_kernel(BigHalo *__restrict__ B, int nbig) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbig || !B[b].active) return;
+  B[b].status = 0;
+  B[b].active = 0;
+}
+
+// pm_mkeep_kernel of the big halos: chunk sums of the kept mass, then the
+// ordered sum per halo
+__global__ void big_mass_kernel(const Members m, const BigChunk *__restrict__ ch, const BigHalo *__restrict__ B,
+                                const PmHalo *__restrict__ H, const uint8_t *__restrict__ keep,
+                                double *__restrict__ part) {
+  const BigChunk c = ch[blockIdx.x];
+  if (!H[B[c.b].h].pending) return;
+  double s = 0.0;
+  for (int64_t k = c.start + threadIdx.x; k < c.end; k += blockDim.x)
+    if (keep[k]) s += (double)m.w[k];
+  __shared__ double red[32];
+  s = bsum_d(s, red);
+  if (threadIdx.x == 0) part[7 * (int64_t)blockIdx.x] = s;
+}
+
+__global__ void big_mass_sum_kernel(const BigHalo *__restrict__ B, int nbig, const double *__restrict__ part,
+                                    PmHalo *__restrict__ H) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbig) return;
+  const BigHalo &bh = B[b];
+  PmHalo &p = H[bh.h];
+  if (!p.pending) return;
+  double s = 0.0;
+  for (int c = bh.chunk0; c < bh.chunk0 + bh.nchunk; ++c) s += part[7 * (int64_t)c];
+  p.mkeep = s;
+}
+
 __global__ void pm_mkeep_kernel(const Members m, PmHalo *__restrict__ H, const int32_t *list, int nlist,
                                 const uint8_t *__restrict__ keep) {
   const int h = list[blockIdx.x];
@@ -1097,6 +1413,48 @@ int bits_for(uint64_t v) {
   int b = 0;
   while (b < 64 && (v >> b) != 0) ++b;
   return b;
+}
+
+// One pass of the removal loop of the large halos (see BigHalo).
+template <typename R>
+int32_t big_removal(Context &ctx, const Members &m, BigHalo *dB, int nbig, const BigChunk *dCh, int nchb,
+                    PmHalo *dH, uint8_t *keep, uint8_t *jd, const R *c1, const R *phi_in, const R *c2,
+                    float *phi, float *en, double *part, int32_t *ucount, uint32_t *ulist, uint32_t *eqbuf,
+                    int32_t *nactive, float b_val, int nmin, int phi_only) {
+  cudaStream_t s = ctx.stream;
+  const unsigned gb = (unsigned)ceil_div(nbig, 128);
+  PYFOF_CUDA(cudaMemsetAsync(nactive, 0, sizeof(int32_t), s));
+  big_start_kernel<<<gb, 128, 0, s>>>(dB, nbig, dH, phi_only, nactive);
+  PYFOF_CHECK_LAUNCH();
+  big_phi_kernel<R><<<nchb, 256, 0, s>>>(dCh, nchb, dB, keep, c1, phi_in, c2, phi, ctx.d_flags);
+  PYFOF_CHECK_LAUNCH();
+  if (phi_only) {
+    big_phi_only_kernel<<<gb, 128, 0, s>>>(dB, nbig);
+    PYFOF_CHECK_LAUNCH();
+  } else {
+    // iterations until every big halo left the inner loop; the host looks
+    // every few iterations (an iteration removes >= 2 % of a halo, and a pass
+    // ends after 20 %)
+    for (int it = 0; it < 1 << 20; it += 4) {
+      for (int j = 0; j < 4; ++j) {
+        big_com_kernel<<<nchb, 256, 0, s>>>(m, dCh, dB, keep, part);
+        PYFOF_CHECK_LAUNCH();
+        big_center_kernel<<<gb, 128, 0, s>>>(dB, nbig, part, ucount);
+        PYFOF_CHECK_LAUNCH();
+        big_energy_kernel<<<nchb, 256, 0, s>>>(m, dCh, dB, keep, phi, en, b_val, ucount, ulist, ctx.d_flags);
+        PYFOF_CHECK_LAUNCH();
+        big_select_kernel<<<nbig, IBLK, 0, s>>>(dB, ucount, ulist, eqbuf, en, keep, jd, nmin, nactive,
+                                                ctx.d_flags);
+        PYFOF_CHECK_LAUNCH();
+      }
+      PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags + FLAG_COUNT_B, nactive, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      PYFOF_CUDA(cudaStreamSynchronize(s));
+      if (ctx.h_flags[FLAG_COUNT_B] <= 0) break;
+    }
+  }
+  big_finish_kernel<<<gb, 128, 0, s>>>(dB, nbig, dH);
+  PYFOF_CHECK_LAUNCH();
+  return kOk;
 }
 
 template <typename R>
@@ -1384,13 +1742,65 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
   int32_t *dbatch = W.carve<int32_t>(std::max(na, 1));
   uint32_t *dbpre = W.carve<uint32_t>(2 * (size_t)(std::max(na, 1) + 1));
   if (!scratch || !dpend || !dslot || !dbatch || !dbpre) { set_error("workspace exhausted (PM grids)"); return kAlloc; }
+  // halos above kBigNp members: chunked removal loop
+  std::vector<BigHalo> hbig;
+  std::vector<BigChunk> hch;
+  std::vector<char> is_big(nh, 0);
+  int64_t ubig = 0;
+  for (int h = 0; h < nh; ++h) {
+    if (H[h].np <= (a.big_np > 0 ? a.big_np : kBigNp)) continue;
+    is_big[h] = 1;
+    BigHalo bh{};
+    bh.h = h;
+    bh.off = H[h].off;
+    bh.np = H[h].np;
+    bh.uoff = ubig;
+    bh.chunk0 = (int32_t)hch.size();
+    for (int64_t st0 = 0; st0 < bh.np; st0 += kChunk)
+      hch.push_back(BigChunk{(int32_t)hbig.size(), bh.off + st0, bh.off + std::min<int64_t>(bh.np, st0 + kChunk)});
+    bh.nchunk = (int32_t)hch.size() - bh.chunk0;
+    ubig += bh.np;
+    hbig.push_back(bh);
+  }
+  const int nbig = (int)hbig.size(), nchb = (int)hch.size();
+  BigHalo *dB = nullptr;
+  BigChunk *dCh = nullptr;
+  double *bpart = nullptr;
+  int32_t *bucount = nullptr;
+  uint32_t *bulist = nullptr, *beq = nullptr;
+  int32_t *nactive = ctx.d_flags + FLAG_COUNT_B;
+  if (nbig) {
+    dB = W.carve<BigHalo>(nbig);
+    dCh = W.carve<BigChunk>(nchb);
+    bpart = W.carve<double>(7 * (size_t)nchb);
+    bucount = W.carve<int32_t>(nbig);
+    bulist = W.carve<uint32_t>(ubig);
+    beq = W.carve<uint32_t>(ubig);
+    if (!dB || !dCh || !bpart || !bucount || !bulist || !beq) {
+      set_error("workspace exhausted (large halos)");
+      return kAlloc;
+    }
+    PYFOF_CUDA(cudaMemcpyAsync(dB, hbig.data(), sizeof(BigHalo) * nbig, cudaMemcpyHostToDevice, s));
+    PYFOF_CUDA(cudaMemcpyAsync(dCh, hch.data(), sizeof(BigChunk) * nchb, cudaMemcpyHostToDevice, s));
+  }
   for (int pass = 1; pass <= kMaxPasses; ++pass) {
     std::vector<int32_t> pend;
     for (int h = 0; h < nh; ++h) if (H[h].pending) pend.push_back(h);
     if (pend.empty()) break;
-    PYFOF_CUDA(cudaMemcpyAsync(dpend, pend.data(), sizeof(int32_t) * pend.size(), cudaMemcpyHostToDevice, s));
-    pm_mkeep_kernel<<<(unsigned)pend.size(), 256, 0, s>>>(m, dH, dpend, (int)pend.size(), keep);
-    PYFOF_CHECK_LAUNCH();
+    std::vector<int32_t> pend_small;
+    for (int h : pend) if (!is_big[h]) pend_small.push_back(h);
+    if (!pend_small.empty()) {
+      PYFOF_CUDA(cudaMemcpyAsync(dpend, pend_small.data(), sizeof(int32_t) * pend_small.size(),
+                                 cudaMemcpyHostToDevice, s));
+      pm_mkeep_kernel<<<(unsigned)pend_small.size(), 256, 0, s>>>(m, dH, dpend, (int)pend_small.size(), keep);
+      PYFOF_CHECK_LAUNCH();
+    }
+    if (nbig) {
+      big_mass_kernel<<<nchb, 256, 0, s>>>(m, dCh, dB, dH, keep, bpart);
+      PYFOF_CHECK_LAUNCH();
+      big_mass_sum_kernel<<<(unsigned)ceil_div(nbig, 128), 128, 0, s>>>(dB, nbig, bpart, dH);
+      PYFOF_CHECK_LAUNCH();
+    }
     for (int n : {48, 64, 128, 256}) {
       std::vector<int32_t> grp;
       for (int h : pend) if (H[h].n == n) grp.push_back(h);
@@ -1474,10 +1884,16 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
                                                    rpos, rsrc, a.a_val, a.softening, c2);
       PYFOF_CHECK_LAUNCH();
     }
-    pm_inner_kernel<R><<<(unsigned)pend.size(), IBLK, 0, s>>>(m, dH, dpend, (int)pend.size(), keep, jd, c1, phi_in, c2, phi,
-                                                           en, (float)a.b_val, a.np_halo_min, phi_only,
-                                                           ctx.d_flags);
-    PYFOF_CHECK_LAUNCH();
+    if (!pend_small.empty()) {
+      pm_inner_kernel<R><<<(unsigned)pend_small.size(), IBLK, 0, s>>>(m, dH, dpend, (int)pend_small.size(), keep,
+                                                                     jd, c1, phi_in, c2, phi, en,
+                                                                     (float)a.b_val, a.np_halo_min, phi_only,
+                                                                     ctx.d_flags);
+      PYFOF_CHECK_LAUNCH();
+    }
+    if (nbig) PYFOF_TRY(big_removal<R>(ctx, m, dB, nbig, dCh, nchb, dH, keep, jd, c1, phi_in, c2, phi, en, bpart,
+                                       bucount, bulist, beq, nactive, (float)a.b_val, a.np_halo_min,
+                                       phi_only));
     PYFOF_CUDA(cudaMemcpyAsync(H.data(), dH, sizeof(PmHalo) * nh, cudaMemcpyDeviceToHost, s));
     PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     PYFOF_CUDA(cudaStreamSynchronize(s));

@@ -109,3 +109,43 @@ def test_pm_unbinding_end_to_end(fp64):
     assert n_in > 1000
     assert mism <= max(3, n_in // 1000), (mism, n_in)
     assert int(g[1].max()) == int(o[1].max())
+
+
+@pytest.mark.parametrize("fp64", [True, False])
+def test_large_halo_removal_loop(fp64):
+    """A halo above the chunked-loop threshold (32768 members): the removal
+    loop spread over the GPU against the oracle."""
+    xs, vs, ms = _pm_halos(21, [40000, 3000, 1500])
+    kw = dict(vp_list=vs, mp_list=ms, L_Box=512.0, linking_length=0.3, np_halo_min=10,
+              bound_check=True)
+    _native.set_option("unbind_fp64", int(fp64))
+    try:
+        g = P._fof_core(xs, **kw)
+    finally:
+        _native.set_option("unbind_fp64", 0)
+    o = oracle_core(xs, **kw)
+    n_in = int(o[0].sum())
+    assert n_in > 30000
+    mism = int((g[0] != o[0]).sum())
+    assert mism <= max(3, n_in // 1000), (mism, n_in)
+    assert int(g[1].max()) == int(o[1].max())
+
+
+def test_chunked_loop_equals_block_loop():
+    """Every PM halo through the chunked removal loop (threshold lowered)
+    against the one-block loop: the same algorithm, centre sums in another
+    order, so only marginally bound members may differ."""
+    xs, vs, ms = _pm_halos(7, [1200, 2500, 4000, 9000, 1100, 600, 300])
+    kw = dict(vp_list=vs, mp_list=ms, L_Box=512.0, linking_length=0.3, np_halo_min=10,
+              bound_check=True, return_ang_mom=True)
+    _native.set_option("unbind_fp64", 1)
+    try:
+        a = P._fof_core(xs, **kw)
+        _native.set_option("unbind_big_np", 1000)
+        b = P._fof_core(xs, **kw)
+    finally:
+        _native.set_option("unbind_big_np", 0)
+        _native.set_option("unbind_fp64", 0)
+    n_in = int(a[0].sum())
+    assert int((a[0] != b[0]).sum()) <= max(2, n_in // 2000)
+    assert int(a[1].max()) == int(b[1].max())
