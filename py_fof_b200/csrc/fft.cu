@@ -201,6 +201,22 @@ constexpr size_t smem_bytes() {
   return sizeof(cplx_t<R>) * (size_t)(N + 2 * (kW<R> + 1) * N);
 }
 
+// Shared memory of the fused z pass: the tiles plus two staging buffers of
+// N/2+1 rows for the next halo's input.
+template <typename R, int N>
+constexpr size_t smem_conv_bytes() {
+  return smem_bytes<R, N>() + sizeof(cplx_t<R>) * (size_t)(2 * (N / 2 + 1) * kW<R>);
+}
+
+// 16-byte asynchronous copy global -> shared (completion by wait_group)
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int K>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
+
 // tw[j] = exp(-2 pi i j / N), from double-precision sincospi
 template <typename R, int N, int T>
 __device__ __forceinline__ void load_twiddles(cplx_t<R> *tw) {
@@ -413,10 +429,38 @@ __global__ void __launch_bounds__(Cfg<R, N>::T) k_lines(cplx_t<R> *__restrict__ 
   }
   __syncthreads();
   int parity = 0;
-  for (int b = b0; b < b1; ++b) {
+  // CONV: the input rows of the next halo are copied into a staging buffer
+  // while the current one is transformed (two buffers of N/2+1 rows of W
+  // complex; in_lim <= N/2+1 there)
+  constexpr int SROWS = N / 2 + 1, CPR = (int)(W * sizeof(C) / 16);
+  C *const stage0 = buf0 + 2 * WP * N;
+  auto prefetch = [&](int bb, int slot) {
+    const C *src = spec + (int64_t)bb * bstride + (int64_t)other * ostride + kx0;
+    C *dst = stage0 + slot * (SROWS * W);
+    for (int c = threadIdx.x; c < in_lim * CPR; c += T) {
+      const int e = c / CPR, part = c - e * CPR;
+      cp_async16(reinterpret_cast<char *>(dst + e * W) + 16 * part,
+                 reinterpret_cast<const char *>(src + (int64_t)e * estride) + 16 * part);
+    }
+    cp_async_commit();
+  };
+  if constexpr (CONV) {
+    if (b0 < b1) prefetch(b0, 0);
+  }
+  for (int b = b0, i = 0; b < b1; ++b, ++i) {
     C *base = spec + (int64_t)b * bstride + (int64_t)other * ostride + kx0;
     C *bA = buf0 + parity * (WP * N);
-    // stage A: global -> registers -> DFT over q -> twiddle -> shared
+    const C *stg = stage0 + (i & 1) * (SROWS * W);
+    if constexpr (CONV) {
+      if (b + 1 < b1) {
+        prefetch(b + 1, (i + 1) & 1);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncthreads();
+    }
+    // stage A: input -> registers -> DFT over q -> twiddle -> shared
 #pragma unroll
     for (int it = 0; it < IA; ++it) {
       const int u = threadIdx.x + it * T;
@@ -427,7 +471,8 @@ __global__ void __launch_bounds__(Cfg<R, N>::T) k_lines(cplx_t<R> *__restrict__ 
 #pragma unroll
         for (int q = 0; q < N1; ++q) {
           const int e = s + N2 * q;
-          v[q] = (col && e < in_lim) ? base[(int64_t)e * estride + li] : mk<C>(0, 0);
+          if constexpr (CONV) v[q] = (col && e < in_lim) ? stg[e * W + li] : mk<C>(0, 0);
+          else v[q] = (col && e < in_lim) ? base[(int64_t)e * estride + li] : mk<C>(0, 0);
         }
         dft<N1, CONV ? -1 : SIGN>(v);
 #pragma unroll
@@ -529,7 +574,7 @@ int32_t prepare() {
     if (r == kOk) r = allow_smem(k_x_c2r<R, N, N>, sm);
     if (r == kOk) r = allow_smem(k_lines<R, N, -1, false>, sm);
     if (r == kOk) r = allow_smem(k_lines<R, N, +1, false>, sm);
-    if (r == kOk) r = allow_smem(k_lines<R, N, -1, true>, sm);
+    if (r == kOk) r = allow_smem(k_lines<R, N, -1, true>, smem_conv_bytes<R, N>());
     status = r;
   });
   return status;
@@ -556,7 +601,8 @@ int32_t convolve_n(R *rho, cplx_t<R> *spec, const R *green, int sup, int batch, 
   static int conv_blocks_per_sm = 0;
   if (!conv_blocks_per_sm) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_lines<R, N, -1, true>, T, sm) != cudaSuccess || b < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_lines<R, N, -1, true>, T,
+                                                      smem_conv_bytes<R, N>()) != cudaSuccess || b < 1)
       b = 1;
     conv_blocks_per_sm = b;
   }
@@ -564,7 +610,7 @@ int32_t convolve_n(R *rho, cplx_t<R> *spec, const R *green, int sup, int batch, 
   const int nchunk = (int)std::max<int64_t>(1, std::min<int64_t>(batch, ceil_div(4 * slots, per)));
   const int nbb = (int)ceil_div(batch, nchunk);
   const int nchunk_used = (int)ceil_div(batch, nbb);
-  k_lines<R, N, -1, true><<<(unsigned)(per * nchunk_used), T, sm, s>>>(
+  k_lines<R, N, -1, true><<<(unsigned)(per * nchunk_used), T, smem_conv_bytes<R, N>(), s>>>(
       spec, green, bstride, nhp, (int64_t)N * nhp, N, ntiles, nbb, batch, sup, sup);
   PYFOF_CHECK_LAUNCH();
   // y inverse: lines (kx, z < sup), input all y, output y < sup
