@@ -59,6 +59,10 @@ WORKLOADS = {
     "fof_64": ("box", 64, False),
     "unbind_nfw_20k": ("nfw", 20000, 2_000_000),
     "unbind_nfw_2k": ("nfw", 2000, 200_000),
+    # lognormal field boxes: name -> (n_side, mesh); L = n_side, np_halo_min 20
+    "fof_lognormal_1024": ("lognormal", 1024, 512),
+    "fof_lognormal_512": ("lognormal", 512, 256),
+    "fof_lognormal_128": ("lognormal", 128, 64),
 }
 # CPU sample of each workload: a sub-volume with the same recipe and density,
 # or the first halos of the same list
@@ -70,6 +74,9 @@ CPU_SAMPLE = {
     "fof_64": "fof_64",
     "unbind_nfw_20k": "unbind_nfw_20k:300",
     "unbind_nfw_2k": "unbind_nfw_2k:300",
+    "fof_lognormal_1024": "fof_lognormal_128",
+    "fof_lognormal_512": "fof_lognormal_128",
+    "fof_lognormal_128": "fof_lognormal_128",
 }
 LINK = 0.2
 NP_MIN = 10
@@ -156,13 +163,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_workload(name, seed=0):
+def make_workload(name, seed=0, device=None):
     """Synthetic input of a workload: dict(xp (3,N), vp, mp (None = unit
-    masses), np_halo, L, bound, s15, regions (the per-region arrays of a
-    list input, else None)).  "name:K" keeps the first K regions of a list."""
+    masses), np_halo, L, bound, s15, np_min, regions (the per-region arrays
+    of a list input, else None)).  "name:K" keeps the first K regions of a
+    list.  Lognormal boxes above 128^3 are generated on `device` (xp is then
+    a torch tensor there)."""
     from py_fof_b200 import workloads as W
     base, _, keep = name.partition(":")
     kind, a, b = WORKLOADS[base]
+    if kind == "lognormal":
+        side, mesh = a, b
+        dev = device if side > 128 else None
+        xp = W.lognormal_box(side ** 3, float(side), mesh, seed=seed, device=dev)
+        return dict(xp=xp, vp=None, mp=None, np_halo=[side ** 3], L=float(side), bound=False,
+                    s15=15.0 * 0.67 * side / 300.0, ng_global=float(side), regions=None, np_min=20,
+                    on_device=dev is not None)
     if kind == "box":
         side, bound = a, b
         halos = max(1, int(round(4096 * (side / 256.0) ** 3)))
@@ -170,13 +186,15 @@ def make_workload(name, seed=0):
                           lognormal_mass=0.3 if bound else None)
         # a sub-volume keeps the 256-box s_15 (the same physical scales)
         return dict(xp=d["xp"], vp=d["vp"], mp=d["mp"], np_halo=[side ** 3], L=float(side),
-                    bound=bound, s15=15.0 * 0.67 * 256.0 / 300.0, ng_global=256.0, regions=None)
+                    bound=bound, s15=15.0 * 0.67 * 256.0 / 300.0, ng_global=256.0, regions=None,
+                    np_min=NP_MIN, on_device=False)
     xs, vs = W.nfw_halos(a, seed=seed, mmax=b)
     if keep:
         xs, vs = xs[:int(keep)], vs[:int(keep)]
     return dict(xp=np.ascontiguousarray(np.hstack(xs)), vp=np.ascontiguousarray(np.hstack(vs)), mp=None,
                 np_halo=[x.shape[1] for x in xs], L=512.0, bound=True,
-                s15=15.0 * 0.67 * 512.0 / 300.0, ng_global=512.0, regions=(xs, vs))
+                s15=15.0 * 0.67 * 512.0 / 300.0, ng_global=512.0, regions=(xs, vs), np_min=NP_MIN,
+                on_device=False)
 
 
 def cpu_port_run(wl, threads):
@@ -188,7 +206,7 @@ def cpu_port_run(wl, threads):
     mp = wl["mp"] if wl["mp"] is not None else np.ones(n)
     nph = np.asarray(wl["np_halo"], np.int32)
     t0 = time.perf_counter()
-    _, hid, _, ierr = O.fof_fortran(xp, vp, mp, nph, len(nph), wl["L"], LINK, NP_MIN,
+    _, hid, _, ierr = O.fof_fortran(xp, vp, mp, nph, len(nph), wl["L"], LINK, wl["np_min"],
                                     int(wl["bound"]), 0, SOFTENING, 1.0, 0.0, wl["s15"], threads, n)
     dt = time.perf_counter() - t0
     if ierr:
@@ -247,7 +265,7 @@ def run_reference(args):
         "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "particles": n, "L_Box": L, "link": LINK,
-                   "np_halo_min": NP_MIN, "bound_check": bound, "softening": SOFTENING},
+                   "np_halo_min": wl["np_min"], "bound_check": bound, "softening": SOFTENING},
         "cpu_baseline": {"value": v, "unit": "Mpart/s", "cores": used, "kind": "port",
                          "sample": f"{name}: {n} particles per step, "
                                    f"{_sample_kind(name, args.workload)}, reference thread policy"},
@@ -276,7 +294,10 @@ def run_b200(args):
     L_ = _native.load()
     if L_.pyfof_init(local) != 0:
         raise RuntimeError(_native.last_error())
-    d = make_workload(args.workload, args.seed)
+    dev = torch.device("cuda", local)
+    d = make_workload(args.workload, args.seed, device=dev)
+    if d["on_device"]:
+        torch.cuda.empty_cache()  # the generator's temporaries go back to the driver
     Lbox, bound, s15 = d["L"], d["bound"], d["s15"]
     nph = list(d["np_halo"])
     n = d["xp"].shape[1]
@@ -298,7 +319,7 @@ def run_b200(args):
         n = d["xp"].shape[1]
         scaling = "strong"
     dev = torch.device("cuda", local)
-    xp = torch.from_numpy(d["xp"]).to(dev)
+    xp = d["xp"] if d["on_device"] else torch.from_numpy(d["xp"]).to(dev)
     vp = torch.from_numpy(d["vp"]).to(dev) if d["vp"] is not None else None
     mp = torch.from_numpy(d["mp"]).to(dev) if d["mp"] is not None else None
     ih = torch.zeros(n, dtype=torch.int32, device=dev)
@@ -311,7 +332,7 @@ def run_b200(args):
         _, ierr = _native.run_device(
             xp.data_ptr(), vp.data_ptr() if vp is not None else 0,
             mp.data_ptr() if mp is not None else 0, _native.LAYOUT_SOA, nph, len(nph), n, Lbox, LINK,
-            NP_MIN, int(bound), 0, SOFTENING, 1.0, 0.0, s15, 0, ih.data_ptr(), hid.data_ptr())
+            d["np_min"], int(bound), 0, SOFTENING, 1.0, 0.0, s15, 0, ih.data_ptr(), hid.data_ptr())
         if ierr:
             raise RuntimeError(f"ierr={ierr}: {_native.last_error()}")
         return {k: _native.last_stage_ms(k) for k in ("link", "fof", "unbind", "call", "pm_fft")} | {
@@ -396,26 +417,36 @@ def run_b200(args):
         p.copy_(torch.from_numpy(a))
         return p.numpy()
 
-    if d["regions"] is None:
-        xp_h, vp_h, mp_h = pinned(d["xp"]), pinned(d["vp"]), pinned(d["mp"])
-    else:  # list input, as the reference API takes it
-        xp_h, vp_h, mp_h = list(d["regions"][0]), list(d["regions"][1]), None
-    _native.set_stream(0)
-    kw = dict(vp_list=vp_h, mp_list=mp_h, L_Box=Lbox, linking_length=LINK, np_halo_min=NP_MIN,
-              bound_check=bound, softening=SOFTENING, ng_global=d["ng_global"])
-    for _ in range(max(1, min(args.warmup, 2))):
-        P.fof(xp_h, **kw)
-    e2e_t = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        P.fof(xp_h, **kw)
-        e2e_t.append(time.perf_counter() - t0)
-    e2e_s = torch.tensor([sum(e2e_t) / len(e2e_t)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
-    e2e_value = n_job / float(e2e_s.item()) / 1e6
-    h2d = 24 * n + (24 * n if vp_h is not None else 0) + (8 * n if mp_h is not None else 0)
-    d2h = 8 * n + 24
+    e2e_note = None
+    if d["on_device"] and 24 * n > (8 << 30):
+        # a host copy of the input would exceed what the host can pin
+        e2e_value, h2d, d2h = None, 0, 0
+        e2e_note = f"not measured: {24 * n / 1e9:.1f} GB of positions generated on the device"
+    else:
+        if d["on_device"]:
+            xp_h = torch.empty(tuple(xp.shape), dtype=torch.float64, pin_memory=True)
+            xp_h.copy_(xp)
+            xp_h, vp_h, mp_h = xp_h.numpy(), None, None
+        elif d["regions"] is None:
+            xp_h, vp_h, mp_h = pinned(d["xp"]), pinned(d["vp"]), pinned(d["mp"])
+        else:  # list input, as the reference API takes it
+            xp_h, vp_h, mp_h = list(d["regions"][0]), list(d["regions"][1]), None
+        _native.set_stream(0)
+        kw = dict(vp_list=vp_h, mp_list=mp_h, L_Box=Lbox, linking_length=LINK, np_halo_min=d["np_min"],
+                  bound_check=bound, softening=SOFTENING, ng_global=d["ng_global"])
+        for _ in range(max(1, min(args.warmup, 2))):
+            P.fof(xp_h, **kw)
+        e2e_t = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            P.fof(xp_h, **kw)
+            e2e_t.append(time.perf_counter() - t0)
+        e2e_s = torch.tensor([sum(e2e_t) / len(e2e_t)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
+        e2e_value = n_job / float(e2e_s.item()) / 1e6
+        h2d = 24 * n + (24 * n if vp_h is not None else 0) + (8 * n if mp_h is not None else 0)
+        d2h = 8 * n + 24
 
     peak, peak_kind = _peaks()
     if bound:
@@ -451,7 +482,7 @@ def run_b200(args):
         "dtype": "f64 linking; f32 unbinding" if bound else "f64",
         "data": "synthetic",
         "config": {"workload": args.workload, "particles": n_job if scaling == "strong" else n, "L_Box": Lbox, "link": LINK,
-                   "np_halo_min": NP_MIN, "bound_check": bound, "softening": SOFTENING,
+                   "np_halo_min": d["np_min"], "bound_check": bound, "softening": SOFTENING,
                    "s_15": s15, "regions": len(nph), "groups": ngroups, "unbinding": "fp32 batched" if bound else None,
                    "l2": "inputs larger than L2 (402 MB positions)" if n >= 2 ** 24 else
                          "inputs smaller than L2",
@@ -461,7 +492,7 @@ def run_b200(args):
                       "unbind": mean(st, "unbind"), "pm_fft": mean(st, "pm_fft")},
         "unbind": unbind,
         "e2e": {"value": e2e_value, "unit": "Mpart/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
+                "d2h_bytes_per_step": d2h, **({"note": e2e_note} if e2e_note else {})},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "kernel": kname, "peak_kind": peak_kind,

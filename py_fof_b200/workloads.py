@@ -162,3 +162,105 @@ def nfw_halos(n_halos, seed=0, mmin=20, mmax=2_000_000, s15=17.152, link=0.2, ki
             v[:, k] += 3.0 * sig[k] * kd
         vs.append(v)
     return xs, vs
+
+
+def lognormal_box(n_total, L, mesh, sigma=1.5, seed=0, device=None, slope=-2.0):
+    """Poisson-like sample of a lognormal density field in a periodic box
+    (the large-FoF configuration: 1024^3 particles, L = 1024, a 512^3 mesh,
+    sigma_G = 1.5, P(k) ~ k^-2).
+
+    A Gaussian field with power spectrum P(k) ~ k^slope on a mesh^3 grid,
+    normalised to standard deviation sigma; weights exp(G - sigma^2/2) per
+    mesh cell; cell counts drawn so that they sum to exactly n_total
+    (Poisson counts of the expected numbers, then the difference spread over
+    randomly chosen cells by weight); positions uniform inside their cell.
+
+    With `device` (a torch device) the field, counts and positions are made
+    there and a (3, n_total) float64 torch tensor is returned; otherwise a
+    numpy array.  Both follow the same recipe but not the same random stream.
+    """
+    if device is None:
+        rng = np.random.default_rng(seed)
+        g = rng.standard_normal((mesh, mesh, mesh))
+        gk = np.fft.rfftn(g)
+        kx = np.fft.fftfreq(mesh)[:, None, None]
+        ky = np.fft.fftfreq(mesh)[None, :, None]
+        kz = np.fft.rfftfreq(mesh)[None, None, :]
+        k2 = kx * kx + ky * ky + kz * kz
+        k2[0, 0, 0] = np.inf
+        gk *= np.power(k2, slope / 4.0)  # amplitude ~ sqrt(P) = k^(slope/2)
+        g = np.fft.irfftn(gk, s=(mesh, mesh, mesh))
+        g *= sigma / g.std()
+        w = np.exp(g - 0.5 * sigma * sigma).ravel()
+        lam = w * (n_total / w.sum())
+        counts = rng.poisson(lam).astype(np.int64)
+        diff = n_total - int(counts.sum())
+        while diff != 0:
+            idx = rng.choice(counts.size, size=abs(diff), p=w / w.sum())
+            if diff > 0:
+                np.add.at(counts, idx, 1)
+            else:
+                sub = np.bincount(idx, minlength=counts.size)
+                counts = np.maximum(counts - sub, 0)
+            diff = n_total - int(counts.sum())
+        cells = np.repeat(np.arange(counts.size, dtype=np.int64), counts)
+        cz, rem = np.divmod(cells, mesh * mesh)
+        cy, cx = np.divmod(rem, mesh)
+        h = L / mesh
+        xp = np.empty((3, n_total))
+        xp[0] = (cx + rng.random(n_total)) * h
+        xp[1] = (cy + rng.random(n_total)) * h
+        xp[2] = (cz + rng.random(n_total)) * h
+        return np.mod(xp, L)
+    import torch
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    g = torch.randn((mesh, mesh, mesh), generator=gen, device=device, dtype=torch.float32)
+    gk = torch.fft.rfftn(g)
+    del g
+    kx = torch.fft.fftfreq(mesh, device=device)[:, None, None]
+    ky = torch.fft.fftfreq(mesh, device=device)[None, :, None]
+    kz = torch.fft.rfftfreq(mesh, device=device)[None, None, :]
+    k2 = kx * kx + ky * ky + kz * kz
+    k2[0, 0, 0] = float("inf")
+    gk *= torch.pow(k2, slope / 4.0)
+    del k2
+    g = torch.fft.irfftn(gk, s=(mesh, mesh, mesh))
+    del gk
+    g = g.double()
+    g *= sigma / g.std()
+    w = torch.exp(g - 0.5 * sigma * sigma).reshape(-1)
+    del g
+    lam = w * (n_total / w.sum())
+    counts = torch.poisson(lam, generator=gen).long()
+    diff = n_total - int(counts.sum().item())
+    cdf = torch.cumsum(w, 0)
+    while diff != 0:
+        # cells drawn by weight (inverse of the cumulative weights)
+        u = torch.rand(abs(diff), generator=gen, device=device, dtype=torch.float64) * cdf[-1]
+        idx = torch.clamp(torch.searchsorted(cdf, u), max=counts.numel() - 1)
+        sub = torch.bincount(idx, minlength=counts.numel())
+        counts = counts + sub if diff > 0 else torch.clamp(counts - sub, min=0)
+        diff = n_total - int(counts.sum().item())
+    del lam, cdf, w
+    # positions cell by cell, in slices of cells to bound the temporaries
+    h = L / mesh
+    xp = torch.empty((3, n_total), dtype=torch.float64, device=device)
+    ends = torch.cumsum(counts, 0)
+    starts = ends - counts
+    ncell = counts.numel()
+    step = 1 << 22
+    for c0 in range(0, ncell, step):
+        c1 = min(ncell, c0 + step)
+        p0, p1 = int(starts[c0].item()), int(ends[c1 - 1].item())
+        if p1 <= p0:
+            continue
+        cells = torch.repeat_interleave(torch.arange(c0, c1, device=device), counts[c0:c1])
+        cz = torch.div(cells, mesh * mesh, rounding_mode="floor")
+        rem = cells - cz * (mesh * mesh)
+        cy = torch.div(rem, mesh, rounding_mode="floor")
+        cx = rem - cy * mesh
+        for d, c in enumerate((cx, cy, cz)):
+            u = torch.rand(p1 - p0, generator=gen, device=device, dtype=torch.float64)
+            xp[d, p0:p1] = torch.remainder((c.double() + u) * h, L)
+    return xp

@@ -200,3 +200,16 @@ def test_invalid_masses_rejected_on_device(bad_mass, bound):
     # the library stays usable and a valid call afterwards is unaffected
     kw["mp_list"] = d["mp"]
     assert np.array_equal(P._fof_core(d["xp"], **kw)[1], oracle_core(d["xp"], **kw)[1])
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_lognormal_field_partition(seed):
+    """The large-FoF configuration's recipe at reduced size (lognormal field,
+    sigma_G = 1.5, P(k) ~ k^-2, np_halo_min 20): dense clumps next to voids,
+    groups that span many cells; bit-exact with the oracle."""
+    x = W.lognormal_box(96 ** 3, 96.0, 48, seed=seed)
+    kw = dict(L_Box=96.0, linking_length=0.2, np_halo_min=20)
+    g, o = _both(x, **kw)
+    assert o[1].max() > 20
+    assert np.array_equal(g[0], o[0])
+    assert np.array_equal(g[1], o[1])
