@@ -120,7 +120,8 @@ int32_t pyfof_halo_potential_direct_static(const float *q, const float *w, int32
  *   np_halo   (nhalo) particle count of every input region
  *   in_halo, halo_id  (total_np) int32 outputs; ang_mom (3,nhalo) float64
  *             Fortran order (ang_mom[3*h+d]) output; all three are written
- *             in full on success and zeroed on failure
+ *             in full on success and zeroed on failure.  in_halo may be
+ *             NULL: it equals halo_id > 0, so a caller can save its copy
  * Returns ierr: the reference codes (0 ok, 1 invalid input, 2 span above
  * s_15, 3 allocation, 4 non-finite, 10 n_threads > 256), plus 5 when a mass
  * is not positive and finite (the reference raises that in Python before

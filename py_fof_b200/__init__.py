@@ -242,7 +242,9 @@ def _finish(call: FofCall, in_halo_out, halo_id_out, ang_mom_out, ierr):
             raise RuntimeError(f"FOF Fortran computation failed with error code ierr={ierr}"
                                + (f" ({detail})" if detail else ""))
     ang_mom_scaled = ang_mom_out * call.ang_mom_scale
-    return in_halo_out.astype(bool), halo_id_out, ang_mom_scaled
+    if in_halo_out.dtype != np.bool_:
+        in_halo_out = in_halo_out.astype(bool)
+    return in_halo_out, halo_id_out, ang_mom_scaled
 
 
 def _native_call(call: FofCall):

@@ -163,16 +163,18 @@ def run(xp, vp, mp, np_halo, nhalo, L_Box, link, np_halo_min, bound_check, verbo
     if mp is not None:
         mp = np.ascontiguousarray(mp, dtype=np.float64)
     nph = np.ascontiguousarray(np_halo, dtype=np.int32)
-    # written in full by the library (zeros on every failure path)
-    in_halo = np.empty(n, dtype=np.int32)
+    # written in full by the library (zeros on every failure path); in_halo
+    # is halo_id > 0, so only halo_id crosses back to the host
+    in_halo = None
     halo_id = np.empty(n, dtype=np.int32)
     ang_mom = np.zeros((3, max(int(nhalo), 0)), dtype=np.float64, order="F")
     args = (_ptr(xp), _ptr(vp), _ptr(mp), layout, nph.ctypes.data_as(_i32p),
             int(nhalo), n, float(L_Box), float(link), int(np_halo_min),
             int(bound_check), int(verbose), float(softening), float(a_val),
             float(b_val), float(s_15_val), int(n_threads), int(ng_val),
-            float(ng_global_val), _ptr(in_halo), _ptr(halo_id), ang_mom.ctypes.data_as(_dp))
+            float(ng_global_val), None, _ptr(halo_id), ang_mom.ctypes.data_as(_dp))
     ierr = L.pyfof_run(*args) if slot is None else L.pyfof_slot_run(ctypes.c_void_p(slot), *args)
+    in_halo = halo_id > 0
     return in_halo, halo_id, ang_mom, int(ierr)
 
 

@@ -375,7 +375,7 @@ static int32_t run_host(Context &ctx, const double *xp, const double *vp, const 
   int32_t r = fof_run(ctx, a);
   note_alloc_failure(ctx, r);
   if (r == kOk) {
-    cudaMemcpyAsync(in_halo, a.in_halo, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);
+    if (in_halo) cudaMemcpyAsync(in_halo, a.in_halo, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(halo_id, a.halo_id, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);
   }
   // an early failure may leave the side copies in flight: their buffers are
@@ -416,7 +416,7 @@ static int32_t run_host_checked(Context *ctx, const double *xp, const double *vp
     zero();
     return kOk;
   }
-  if (r == kOk && (!xp || !in_halo || !halo_id || !ang_mom)) {
+  if (r == kOk && (!xp || !halo_id || !ang_mom)) {
     set_error("null argument");
     r = kInvalid;
   }

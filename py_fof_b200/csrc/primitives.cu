@@ -92,6 +92,24 @@ __global__ void __launch_bounds__(SCAN_THREADS) scan_apply_kernel(const uint32_t
 
 // ------------------------------------------------------------ radix sort
 
+// exclusive scan over the 256 threads of a block (one value each)
+__device__ __forceinline__ uint32_t block_excl_scan_256(uint32_t v, uint32_t *total) {
+  __shared__ uint32_t ws[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t inc = warp_incl_scan(v);
+  if (lane == 31) ws[warp] = inc;
+  __syncthreads();
+  uint32_t before = 0, all = 0;
+#pragma unroll
+  for (int w = 0; w < 8; ++w) {
+    const uint32_t s = ws[w];
+    before += w < warp ? s : 0u;
+    all += s;
+  }
+  *total = all;
+  return before + inc - v;
+}
+
 constexpr int RS_THREADS = 256;
 constexpr int RS_WARPS = RS_THREADS / 32;
 constexpr int RS_ROUNDS = 16;                          // items per lane
@@ -115,6 +133,10 @@ __global__ void __launch_bounds__(RS_THREADS) rs_upsweep(const uint32_t *__restr
   hist[(int64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
 }
 
+// Stable scatter of one tile: warp ranks by digit (__match_any_sync, in
+// input order), then the tile is reordered by digit in shared memory and
+// written out in that order, so consecutive threads store consecutive
+// positions of the same digit run.
 __global__ void __launch_bounds__(RS_THREADS) rs_downsweep(const uint32_t *__restrict__ kin,
                                                            const uint32_t *__restrict__ vin,
                                                            uint32_t *__restrict__ kout,
@@ -123,10 +145,13 @@ __global__ void __launch_bounds__(RS_THREADS) rs_downsweep(const uint32_t *__res
                                                            const uint32_t *__restrict__ offs,
                                                            int64_t ntiles) {
   __shared__ uint32_t wh[RS_WARPS][RS_BINS];
+  __shared__ uint32_t tstart[RS_BINS], glob[RS_BINS];
+  __shared__ uint32_t sk[RS_TILE], sv[RS_TILE];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int d = lane; d < RS_BINS; d += 32) wh[warp][d] = 0;
   __syncwarp();
-  const int64_t wbase = (int64_t)blockIdx.x * RS_TILE + (int64_t)warp * (32 * RS_ROUNDS);
+  const int64_t tbase = (int64_t)blockIdx.x * RS_TILE;
+  const int64_t wbase = tbase + (int64_t)warp * (32 * RS_ROUNDS);
   uint32_t key[RS_ROUNDS], val[RS_ROUNDS], rank[RS_ROUNDS];
   const unsigned lt = lanemask_lt();
 #pragma unroll
@@ -146,25 +171,39 @@ __global__ void __launch_bounds__(RS_THREADS) rs_downsweep(const uint32_t *__res
   }
   __syncthreads();
   {
+    // per digit: offsets of the warps inside the tile's run, the run's
+    // start in the tile (block scan) and its global start
     const int d = threadIdx.x;  // RS_THREADS == RS_BINS
-    uint32_t run = offs[(int64_t)d * ntiles + blockIdx.x];
+    uint32_t run = 0;
 #pragma unroll
     for (int w = 0; w < RS_WARPS; ++w) {
-      uint32_t c = wh[w][d];
+      const uint32_t c = wh[w][d];
       wh[w][d] = run;
       run += c;
     }
+    uint32_t tot;
+    tstart[d] = block_excl_scan_256(run, &tot);
+    glob[d] = offs[(int64_t)d * ntiles + blockIdx.x];
   }
   __syncthreads();
 #pragma unroll
   for (int r = 0; r < RS_ROUNDS; ++r) {
     int64_t i = wbase + r * 32 + lane;
     if (i < n) {
-      uint32_t d = (key[r] >> shift) & 0xffu;
-      uint32_t pos = wh[warp][d] + rank[r];
-      kout[pos] = key[r];
-      vout[pos] = val[r];
+      const uint32_t d = (key[r] >> shift) & 0xffu;
+      const uint32_t loc = tstart[d] + wh[warp][d] + rank[r];
+      sk[loc] = key[r];
+      sv[loc] = val[r];
     }
+  }
+  __syncthreads();
+  const int tn = (int)min((int64_t)RS_TILE, n - tbase);
+  for (int i = threadIdx.x; i < tn; i += RS_THREADS) {
+    const uint32_t k = sk[i];
+    const uint32_t d = (k >> shift) & 0xffu;
+    const uint32_t pos = glob[d] + ((uint32_t)i - tstart[d]);
+    kout[pos] = k;
+    vout[pos] = sv[i];
   }
 }
 
