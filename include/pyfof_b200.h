@@ -146,6 +146,22 @@ int32_t pyfof_run_device(const double *d_xp, const double *d_vp, const double *d
                          double ng_global_val, int32_t *d_in_halo, int32_t *d_halo_id,
                          double *ang_mom);
 
+/* fof_with_info on the device (py_fof/__init__.py:481-518): pyfof_run
+ * (without in_halo, which is halo_id > 0) that also returns the halo
+ * catalogue: members[0 .. offsets[n]) holds the particle indices of every
+ * valid halo, ascending within a halo, halos in id order, and
+ * offsets[h] .. offsets[h+1] delimits halo h+1 (n = *nhalo_found halos;
+ * members needs total_np entries, offsets n+1, at most total_np /
+ * max(1, np_halo_min) + 1).  slot: a slot handle or NULL (default context).
+ * Returns ierr like pyfof_run. */
+int32_t pyfof_run_catalogue(void *slot, const double *xp, const double *vp, const double *mp,
+                            int32_t layout, const int32_t *np_halo, int32_t nhalo, int64_t total_np,
+                            double L_Box, double linking_length, int32_t np_halo_min, int32_t bound_check,
+                            int32_t verbose, double softening, double a_val, double b_val, double s_15_val,
+                            int32_t n_threads, int64_t ng_val, double ng_global_val, int32_t *halo_id,
+                            double *ang_mom, int32_t *members, int64_t *offsets, int64_t offsets_cap,
+                            int32_t *nhalo_found);
+
 /* Slots: contexts of their own (CUDA streams, device scratch, status
  * words) on one device, for callers that run several calls at once — the
  * serving loop of py_fof_b200.serve runs one host thread per slot, so the

@@ -346,12 +346,43 @@ def fof_with_info(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2,
     'halo_indices' (ascending particle indices per halo, ordered by halo id),
     'bound_status' (zeros) and, if requested, 'ang_mom'.
     """
-    in_halo, halo_id, ang_mom = _fof_core(
-        xp_list=xp_list, vp_list=vp_list, L_Box=L_Box, linking_length=linking_length,
-        np_halo_min=np_halo_min, bound_check=bound_check, verbose=verbose,
-        return_ang_mom=return_ang_mom, n_threads=n_threads, mp_list=mp_list,
-        softening=softening, z=z, box=box, h0=h0, omega_m=omega_m, omega_l=omega_l,
-        n_sim=n_sim, units=units, include_hubble_flow=include_hubble_flow,
-        ng=ng, ng_global=ng_global
-    )
-    return catalogue_from_ids(in_halo, halo_id, ang_mom, return_ang_mom)
+    call = _prepare(xp_list, vp_list=vp_list, L_Box=L_Box, linking_length=linking_length,
+                    np_halo_min=np_halo_min, bound_check=bound_check, verbose=verbose,
+                    return_ang_mom=return_ang_mom, n_threads=n_threads, mp_list=mp_list,
+                    softening=softening, z=z, box=box, h0=h0, omega_m=omega_m,
+                    omega_l=omega_l, n_sim=n_sim, units=units,
+                    include_hubble_flow=include_hubble_flow, ng=ng, ng_global=ng_global,
+                    check_masses=False)
+    if not isinstance(call, FofCall):
+        return catalogue_from_ids(*call, return_ang_mom=return_ang_mom)
+    return _catalogue_call(call, return_ang_mom)
+
+
+def _catalogue_call(call: FofCall, return_ang_mom, slot=None):
+    """One native call with the catalogue sorted on the device; the result
+    dict of fof_with_info (py_fof/__init__.py:481-518)."""
+    ih, hid, am, ierr, members, offsets = _native.run_catalogue(
+        call.xp, call.vp, call.mp, call.np_halo, call.nhalo, call.L_Box, call.link, call.np_halo_min,
+        call.bound_check, call.verbose, call.softening, call.a_val, call.b_val, call.s_15_val,
+        call.n_threads, call.total_np, ng_val=call.ng_val, ng_global_val=call.ng_global_val, slot=slot)
+    in_halo, _, ang_mom = _finish(call, ih, hid, am, ierr)
+    counts = np.diff(offsets)
+    if counts.size == 0:
+        halo_indices, np_per_halo = [], np.array([], dtype=int)
+    else:
+        halo_indices = np.split(members.astype(np.int64), offsets[1:-1])
+        np_per_halo = counts
+        if not np.all(counts > 0):  # ids without members are not listed
+            halo_indices = [h for h, c in zip(halo_indices, counts) if c > 0]
+            np_per_halo = counts[counts > 0]
+    nfound = len(halo_indices)
+    res = {
+        'in_halo': in_halo,
+        'nhalo_found': nfound,
+        'np_per_halo': np_per_halo,
+        'halo_indices': halo_indices,
+        'bound_status': np.zeros(nfound, dtype=np.int32)
+    }
+    if return_ang_mom:
+        res['ang_mom'] = ang_mom
+    return res

@@ -35,7 +35,7 @@ EXPORTED = ("pyfof_version", "pyfof_init", "pyfof_shutdown", "pyfof_last_error",
             "pyfof_set_option", "pyfof_set_stream", "pyfof_get_stat", "pyfof_last_link_ms", "pyfof_last_stage_ms",
             "pyfof_halo_potential", "pyfof_halo_potential_direct_static", "pyfof_run",
             "pyfof_run_device", "pyfof_slot_create", "pyfof_slot_destroy", "pyfof_slot_run",
-            "pyfof_slot_stat")
+            "pyfof_slot_stat", "pyfof_run_catalogue")
 
 
 class NativeLibraryError(RuntimeError):
@@ -87,6 +87,10 @@ def load():
         L.pyfof_slot_destroy.argtypes = [ctypes.c_void_p]
         L.pyfof_slot_run.restype = ctypes.c_int32
         L.pyfof_slot_run.argtypes = [ctypes.c_void_p] + list(_RUN_ARGS)
+        L.pyfof_run_catalogue.restype = ctypes.c_int32
+        L.pyfof_run_catalogue.argtypes = ([ctypes.c_void_p] + list(_RUN_ARGS[:19]) +
+                                          [_RUN_ARGS[20], _RUN_ARGS[21], ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32)])
         L.pyfof_slot_stat.restype = ctypes.c_int32
         L.pyfof_slot_stat.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
         v = L.pyfof_version()
@@ -176,6 +180,45 @@ def run(xp, vp, mp, np_halo, nhalo, L_Box, link, np_halo_min, bound_check, verbo
     ierr = L.pyfof_run(*args) if slot is None else L.pyfof_slot_run(ctypes.c_void_p(slot), *args)
     in_halo = halo_id > 0
     return in_halo, halo_id, ang_mom, int(ierr)
+
+
+def run_catalogue(xp, vp, mp, np_halo, nhalo, L_Box, link, np_halo_min, bound_check, verbose,
+                  softening, a_val, b_val, s_15_val, n_threads, total_np, ng_val=256,
+                  ng_global_val=512.0, slot=None):
+    """run() plus the halo catalogue built on the device.  Returns
+    (in_halo, halo_id, ang_mom, ierr, members, offsets): members (int32)
+    lists each valid halo's particle indices, ascending, halos in id order;
+    offsets[h]:offsets[h+1] delimits halo h+1."""
+    L = load()
+    n = int(total_np)
+    if xp.flags.c_contiguous:
+        layout = LAYOUT_SOA
+    elif xp.flags.f_contiguous:
+        layout = LAYOUT_AOS
+    else:
+        xp = np.ascontiguousarray(xp)
+        layout = LAYOUT_SOA
+    if vp is not None:
+        vp = np.asarray(vp, dtype=np.float64)
+        vp = np.ascontiguousarray(vp) if layout == LAYOUT_SOA else np.asfortranarray(vp)
+    if mp is not None:
+        mp = np.ascontiguousarray(mp, dtype=np.float64)
+    nph = np.ascontiguousarray(np_halo, dtype=np.int32)
+    halo_id = np.empty(n, dtype=np.int32)
+    ang_mom = np.zeros((3, max(int(nhalo), 0)), dtype=np.float64, order="F")
+    members = np.empty(max(n, 1), dtype=np.int32)
+    cap = n // max(1, int(np_halo_min)) + 2
+    offsets = np.empty(cap, dtype=np.int64)
+    nfound = ctypes.c_int32(0)
+    ierr = L.pyfof_run_catalogue(
+        ctypes.c_void_p(slot) if slot else None, _ptr(xp), _ptr(vp), _ptr(mp), layout,
+        nph.ctypes.data_as(_i32p), int(nhalo), n, float(L_Box), float(link), int(np_halo_min),
+        int(bound_check), int(verbose), float(softening), float(a_val), float(b_val), float(s_15_val),
+        int(n_threads), int(ng_val), float(ng_global_val), _ptr(halo_id), ang_mom.ctypes.data_as(_dp),
+        _ptr(members), _ptr(offsets), cap, ctypes.byref(nfound))
+    k = int(nfound.value) if ierr == 0 else 0
+    offsets = offsets[:k + 1] if k else np.zeros(1, dtype=np.int64)
+    return halo_id > 0, halo_id, ang_mom, int(ierr), members[:int(offsets[-1])], offsets
 
 
 def slot_create(device=0, pm_budget_bytes=0):

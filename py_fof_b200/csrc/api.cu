@@ -3,6 +3,7 @@
 #include <cstdarg>
 #include <cstring>
 
+#include "catalogue.cuh"
 #include "context.cuh"
 #include "fof.cuh"
 #include "fof_internal.cuh"
@@ -313,12 +314,19 @@ int32_t pyfof_halo_potential(const float *q, const float *w, int32_t np, double 
 // Host-memory call.  Positions are copied first on the call's stream; the
 // velocities and masses follow on the context's second stream and are
 // waited for only after the linking, so their copies overlap with it.
+struct CatalogueOut {
+  int32_t *members;
+  int64_t *offsets;
+  int64_t cap;
+  int32_t *nfound;
+};
+
 static int32_t run_host(Context &ctx, const double *xp, const double *vp, const double *mp,
                         int32_t layout, const int32_t *np_halo, int32_t nhalo, int64_t total_np,
                         double L_Box, double linking_length, int32_t np_halo_min, int32_t bound_check,
                         int32_t verbose, double softening, double a_val, double b_val,
                         double s_15_val, int32_t n_threads, int64_t ng_val, double ng_global_val,
-                        int32_t *in_halo, int32_t *halo_id, double *ang_mom) {
+                        int32_t *in_halo, int32_t *halo_id, double *ang_mom, CatalogueOut *cat) {
   PYFOF_CUDA(cudaSetDevice(ctx.device));
   cudaStream_t s = ctx.stream;
   const size_t n = (size_t)total_np;
@@ -373,6 +381,8 @@ static int32_t run_host(Context &ctx, const double *xp, const double *vp, const 
   a.bound_per_halo = g_bound_per_halo;
   a.big_np = g_big_np;
   int32_t r = fof_run(ctx, a);
+  if (r == kOk && cat) r = build_catalogue(ctx, a.halo_id, (int64_t)n, cat->members, cat->offsets, cat->cap,
+                                           cat->nfound);
   note_alloc_failure(ctx, r);
   if (r == kOk) {
     if (in_halo) cudaMemcpyAsync(in_halo, a.in_halo, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);
@@ -402,7 +412,7 @@ static int32_t run_host_checked(Context *ctx, const double *xp, const double *vp
                                 int32_t bound_check, int32_t verbose, double softening, double a_val,
                                 double b_val, double s_15_val, int32_t n_threads, int64_t ng_val,
                                 double ng_global_val, int32_t *in_halo, int32_t *halo_id,
-                                double *ang_mom) {
+                                double *ang_mom, CatalogueOut *cat = nullptr) {
   // outputs are written in full on success and zeroed on every other path
   auto zero = [&]() {
     if (total_np > 0) {
@@ -414,6 +424,10 @@ static int32_t run_host_checked(Context *ctx, const double *xp, const double *vp
   int32_t r = validate(nhalo, total_np, np_halo, n_threads);
   if (r == kOk && (nhalo <= 0 || total_np <= 0)) {
     zero();
+    if (cat) {
+      *cat->nfound = 0;
+      if (cat->cap >= 1) cat->offsets[0] = 0;
+    }
     return kOk;
   }
   if (r == kOk && (!xp || !halo_id || !ang_mom)) {
@@ -430,7 +444,7 @@ static int32_t run_host_checked(Context *ctx, const double *xp, const double *vp
     std::lock_guard<std::mutex> lk(ctx->mu);
     r = run_host(*ctx, xp, vp, mp, layout, np_halo, nhalo, total_np, L_Box, linking_length,
                  np_halo_min, bound_check, verbose, softening, a_val, b_val, s_15_val, n_threads,
-                 ng_val, ng_global_val, in_halo, halo_id, ang_mom);
+                 ng_val, ng_global_val, in_halo, halo_id, ang_mom, cat);
   }
   if (r != kOk) zero();
   return r;
@@ -505,6 +519,28 @@ int32_t pyfof_run_device(const double *d_xp, const double *d_vp, const double *d
     std::memset(ang_mom, 0, sizeof(double) * 3 * (size_t)nhalo);
   }
   return r;
+}
+
+int32_t pyfof_run_catalogue(void *slot, const double *xp, const double *vp, const double *mp,
+                            int32_t layout, const int32_t *np_halo, int32_t nhalo, int64_t total_np,
+                            double L_Box, double linking_length, int32_t np_halo_min, int32_t bound_check,
+                            int32_t verbose, double softening, double a_val, double b_val, double s_15_val,
+                            int32_t n_threads, int64_t ng_val, double ng_global_val, int32_t *halo_id,
+                            double *ang_mom, int32_t *members, int64_t *offsets, int64_t offsets_cap,
+                            int32_t *nhalo_found) {
+  if (!members || !offsets || !nhalo_found || offsets_cap < 1) {
+    set_error("pyfof_run_catalogue: null catalogue output");
+    return kInvalid;
+  }
+  if (slot && static_cast<Context *>(slot)->magic != Context::kMagic) {
+    set_error("pyfof_run_catalogue: not a slot");
+    return kInvalid;
+  }
+  CatalogueOut cat{members, offsets, offsets_cap, nhalo_found};
+  *nhalo_found = 0;
+  return run_host_checked(static_cast<Context *>(slot), xp, vp, mp, layout, np_halo, nhalo, total_np, L_Box,
+                          linking_length, np_halo_min, bound_check, verbose, softening, a_val, b_val,
+                          s_15_val, n_threads, ng_val, ng_global_val, nullptr, halo_id, ang_mom, &cat);
 }
 
 // ---------------------------------------------------------------- slots

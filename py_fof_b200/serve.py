@@ -29,7 +29,7 @@ import time
 
 import numpy as np
 
-from . import FofCall, _finish, _native, _prepare, catalogue_from_ids
+from . import FofCall, _catalogue_call, _finish, _native, _prepare, catalogue_from_ids
 
 __all__ = ["Server"]
 
@@ -57,17 +57,20 @@ def native_executor(device=0, pm_budget_bytes=2 << 30):
     made = []
     lock = threading.Lock()
 
-    def run(call: FofCall):
+    def run(call: FofCall, ret_am=False):
+        """The fof_with_info result of one request (catalogue sorted on the
+        device) and the slot's peak device memory."""
         if not hasattr(local, "slot"):
             local.slot = _native.slot_create(device, pm_budget_bytes)
             with lock:
                 made.append(local.slot)
-        out = _native.run(call.xp, call.vp, call.mp, call.np_halo, call.nhalo, call.L_Box, call.link,
-                          call.np_halo_min, call.bound_check, call.verbose, call.softening,
-                          call.a_val, call.b_val, call.s_15_val, call.n_threads, call.total_np,
-                          ng_val=call.ng_val, ng_global_val=call.ng_global_val, slot=local.slot)
-        peak = _native.slot_stat(local.slot, "peak_bytes")
+        try:
+            out = _catalogue_call(call, ret_am, slot=local.slot)
+        finally:
+            peak = _native.slot_stat(local.slot, "peak_bytes")
         return out, peak
+
+    run.returns_result = True
 
     def close():
         with lock:
@@ -86,7 +89,8 @@ class Server:
     hbm_budget:  device bytes the running requests may hold together
                  (default: 80 % of the free device memory at start)
     executor:    callable(FofCall) -> ((in_halo, halo_id, ang_mom, ierr),
-                 peak_bytes); the native slots by default
+                 peak_bytes); the native slots by default (those return the
+                 finished result, its catalogue sorted on the device)
     """
 
     FOF_BYTES = 200.0    # initial per-particle estimates (device bytes)
@@ -212,9 +216,12 @@ class Server:
                 req.start = time.perf_counter()
             peak = 0
             try:
-                (ih, hid, am, ierr), peak = self._exec(req.call)
-                res = _finish(req.call, ih, hid, am, ierr)
-                out = catalogue_from_ids(*res, return_ang_mom=req.ret_am)
+                if getattr(self._exec, "returns_result", False):
+                    out, peak = self._exec(req.call, req.ret_am)
+                else:
+                    (ih, hid, am, ierr), peak = self._exec(req.call)
+                    res = _finish(req.call, ih, hid, am, ierr)
+                    out = catalogue_from_ids(*res, return_ang_mom=req.ret_am)
                 err = None
             except Exception as exc:  # delivered through the future
                 out, err = None, exc
