@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define PYFOF_B200_ABI_VERSION 1
+#define PYFOF_B200_ABI_VERSION 2
 
 /* Memory layout of the (3,N) float64 coordinate/velocity arrays. */
 #define PYFOF_LAYOUT_AOS 0 /* Fortran order, x[3*i+d]: the f2py xp_halo layout */
@@ -146,15 +146,41 @@ int32_t pyfof_run_device(const double *d_xp, const double *d_vp, const double *d
                          double ng_global_val, int32_t *d_in_halo, int32_t *d_halo_id,
                          double *ang_mom);
 
+/* Conversion of the inputs to code units, applied on the device after the
+ * host-to-device copy.  The reference converts on the host before its call
+ * (py_fof/__init__.py:266-326, units='physical'): positions / dx,
+ * velocities * v_scale, masses / m_grid, or the constant mass
+ * ng_eff^3 / n_sim when only n_sim is given.  The same IEEE operations on
+ * the device give the same bits.  Masses are checked (positive, finite)
+ * before the division, as the reference checks mp_list before converting.
+ * {1, 1, 1, 1} converts nothing. */
+typedef struct pyfof_units {
+  double x_div;   /* positions are divided by x_div */
+  double v_mul;   /* velocities are multiplied by v_mul */
+  double m_div;   /* masses (mp != NULL) are divided by m_div */
+  double m_const; /* the mass of every particle when mp is NULL */
+} pyfof_units_t;
+
+/* pyfof_run with the inputs in the caller's units, converted on the device
+ * (`units` may be NULL: none).  slot: a slot handle or NULL (default
+ * context); in_halo may be NULL (it is halo_id > 0). */
+int32_t pyfof_run_units(void *slot, const pyfof_units_t *units, const double *xp, const double *vp,
+                        const double *mp, int32_t layout, const int32_t *np_halo, int32_t nhalo,
+                        int64_t total_np, double L_Box, double linking_length, int32_t np_halo_min,
+                        int32_t bound_check, int32_t verbose, double softening, double a_val,
+                        double b_val, double s_15_val, int32_t n_threads, int64_t ng_val,
+                        double ng_global_val, int32_t *in_halo, int32_t *halo_id, double *ang_mom);
+
 /* fof_with_info on the device (py_fof/__init__.py:481-518): pyfof_run
  * (without in_halo, which is halo_id > 0) that also returns the halo
  * catalogue: members[0 .. offsets[n]) holds the particle indices of every
  * valid halo, ascending within a halo, halos in id order, and
  * offsets[h] .. offsets[h+1] delimits halo h+1 (n = *nhalo_found halos;
  * members needs total_np entries, offsets n+1, at most total_np /
- * max(1, np_halo_min) + 1).  slot: a slot handle or NULL (default context).
- * Returns ierr like pyfof_run. */
-int32_t pyfof_run_catalogue(void *slot, const double *xp, const double *vp, const double *mp,
+ * max(1, np_halo_min) + 1).  slot: a slot handle or NULL (default context);
+ * units: as in pyfof_run_units, or NULL.  Returns ierr like pyfof_run. */
+int32_t pyfof_run_catalogue(void *slot, const pyfof_units_t *units, const double *xp, const double *vp,
+                            const double *mp,
                             int32_t layout, const int32_t *np_halo, int32_t nhalo, int64_t total_np,
                             double L_Box, double linking_length, int32_t np_halo_min, int32_t bound_check,
                             int32_t verbose, double softening, double a_val, double b_val, double s_15_val,

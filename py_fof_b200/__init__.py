@@ -9,7 +9,7 @@ replaced by the C-ABI library ``libpyfof_b200.so`` (include/pyfof_b200.h).
 """
 from __future__ import annotations
 
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 
 import numpy as np
 
@@ -41,11 +41,30 @@ class FofCall:
     ng_val: int
     ng_global_val: float
     ang_mom_scale: float
+    # (x_div, v_mul, m_div, m_const): the conversion of xp/vp/mp to code
+    # units that the device applies after the copy (pyfof_units_t); None
+    # when the arrays above are in code units already
+    units: tuple | None = None
+
+    def on_host(self):
+        """The same call with the unit conversion done here, in NumPy, as the
+        reference does it (py_fof/__init__.py:302-321)."""
+        if self.units is None:
+            return self
+        x_div, v_mul, m_div, m_const = self.units
+        xp = self.xp if x_div == 1.0 else np.ascontiguousarray(self.xp / x_div, dtype=np.float64)
+        vp = self.vp if (self.vp is None or v_mul == 1.0) else np.ascontiguousarray(self.vp * v_mul)
+        if self.mp is not None:
+            mp = self.mp if m_div == 1.0 else np.ascontiguousarray(self.mp / m_div, dtype=np.float64)
+        else:
+            mp = None if m_const == 1.0 else np.full(self.total_np, m_const, dtype=np.float64)
+        return replace(self, xp=xp, vp=vp, mp=mp, units=None)
 
     def dense(self):
-        """vp/mp materialised exactly as the reference passes them."""
-        vp = self.vp if self.vp is not None else np.zeros((3, self.total_np), dtype=np.float64)
-        mp = self.mp if self.mp is not None else np.ones(self.total_np, dtype=np.float64)
+        """vp/mp in code units, materialised exactly as the reference passes them."""
+        c = self.on_host()
+        vp = c.vp if c.vp is not None else np.zeros((3, c.total_np), dtype=np.float64)
+        mp = c.mp if c.mp is not None else np.ones(c.total_np, dtype=np.float64)
         return vp, mp
 
 
@@ -65,13 +84,17 @@ def _prepare(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2, np_halo_min
              bound_check=False, verbose=0, return_ang_mom=False, n_threads=None, mp_list=None,
              softening=None, z=0.0, box=300.0, h0=0.67, omega_m=0.3, omega_l=0.7, n_sim=None,
              units='cube', include_hubble_flow=False, ng=None, ng_global=None,
-             check_masses=True):
+             check_masses=True, device_units=False):
     """Validation and unit conversion of _fof_core (py_fof/__init__.py:168-329).
 
     Returns either a FofCall or, for total_np == 0, the final empty result.
     With check_masses=False the per-particle mass check (positive and
     finite) is left to the native library, which runs it on the device and
     reports it as ierr 5; _finish raises the same ValueError for it.
+    With device_units=True the arrays stay in the caller's units and the
+    call carries their conversion (FofCall.units), which the library applies
+    on the device; a scalar mass then travels as that constant instead of
+    an array of N copies.
     """
     if units not in ('cube', 'physical'):
         raise ValueError(f"units must be 'cube' or 'physical', got '{units}'")
@@ -127,12 +150,16 @@ def _prepare(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2, np_halo_min
         vp_halo = None  # the reference passes zeros (py_fof/__init__.py:233)
 
     mp_raw = None
+    mp_scalar = None  # a scalar mass kept as such (device_units only)
     if mp_list is not None:
         if np.isscalar(mp_list) or (isinstance(mp_list, np.ndarray) and mp_list.ndim == 0):
             val = float(mp_list)
             if val <= 0 or not np.isfinite(val):
                 raise ValueError("mp_list scalar must be positive and finite")
-            mp_raw = np.full(total_np, val, dtype=np.float64)
+            if device_units:
+                mp_scalar = val
+            else:
+                mp_raw = np.full(total_np, val, dtype=np.float64)
         elif isinstance(mp_list, np.ndarray):
             if mp_list.ndim == 1 and len(mp_list) == total_np:
                 mp_raw = np.ascontiguousarray(mp_list, dtype=np.float64)
@@ -153,7 +180,7 @@ def _prepare(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2, np_halo_min
         else:
             raise ValueError("Unsupported mp_list type")
 
-        if check_masses and (not np.all(np.isfinite(mp_raw)) or not np.all(mp_raw > 0)):
+        if check_masses and mp_raw is not None and (not np.all(np.isfinite(mp_raw)) or not np.all(mp_raw > 0)):
             raise ValueError(_MASS_ERROR)
 
     z_val = float(z)
@@ -180,36 +207,51 @@ def _prepare(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2, np_halo_min
         vp_code = vp_halo
         mp_code = mp_raw  # None means unit masses (py_fof/__init__.py:290-291)
         ang_mom_scale = 1.0
+        conv = None if mp_scalar is None else (1.0, 1.0, 1.0, mp_scalar)
     else:
         if bound_check:
             if softening is None or float(softening) <= 0:
                 raise ValueError("softening must be explicitly provided and > 0 when units='physical' and bound_check=True")
-            if mp_raw is None and n_sim is None:
+            if mp_raw is None and mp_scalar is None and n_sim is None:
                 raise ValueError("Either mp_list or n_sim must be provided when units='physical' and bound_check=True")
 
         ng_eff = float(round(float(n_sim) ** (1.0 / 3.0))) if (n_sim is not None and float(n_sim) > 0) else (float(ng_global) if ng_global is not None else 512.0)
         box_mpc_h = float(L_Box)
         dx = box_mpc_h / ng_eff
 
-        xp_code = np.ascontiguousarray(xp_halo / dx, dtype=np.float64)
         L_Box_code = ng_eff
         link_code = float(linking_length) / dx
         softening_grid = 0.1 if softening is None else (float(softening) / dx)
         s_15_val = 15.0 * float(h0) * ng_eff / box_mpc_h
 
         v_scale = (a_val * ng_eff) / (150.0 * np.sqrt(float(omega_m)) * box_mpc_h)
-        vp_code = None if vp_halo is None else np.ascontiguousarray(vp_halo * v_scale, dtype=np.float64)
 
         rho_crit_0 = 2.77536627e11
         m_grid = float(omega_m) * rho_crit_0 * (box_mpc_h ** 3) / (ng_eff ** 3)
 
-        if mp_raw is not None:
-            mp_code = np.ascontiguousarray(mp_raw / m_grid, dtype=np.float64)
-        elif n_sim is not None:
-            mp_code = np.full(total_np, (ng_eff ** 3) / float(n_sim), dtype=np.float64)
+        if device_units:
+            # the device divides/multiplies with the same IEEE operations
+            xp_code, vp_code, mp_code = xp_halo, vp_halo, mp_raw
+            if mp_raw is not None:
+                conv = (dx, v_scale, m_grid, 1.0)
+            elif mp_scalar is not None:
+                conv = (dx, v_scale, 1.0, mp_scalar / m_grid)
+            elif n_sim is not None:
+                conv = (dx, v_scale, 1.0, (ng_eff ** 3) / float(n_sim))
+            else:
+                conv = (dx, v_scale, 1.0, 1.0)
+                m_grid = 1.0
         else:
-            mp_code = None
-            m_grid = 1.0
+            conv = None
+            xp_code = np.ascontiguousarray(xp_halo / dx, dtype=np.float64)
+            vp_code = None if vp_halo is None else np.ascontiguousarray(vp_halo * v_scale, dtype=np.float64)
+            if mp_raw is not None:
+                mp_code = np.ascontiguousarray(mp_raw / m_grid, dtype=np.float64)
+            elif n_sim is not None:
+                mp_code = np.full(total_np, (ng_eff ** 3) / float(n_sim), dtype=np.float64)
+            else:
+                mp_code = None
+                m_grid = 1.0
 
         ang_mom_scale = m_grid * dx / v_scale
 
@@ -221,7 +263,7 @@ def _prepare(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2, np_halo_min
                    bound_check=int(bound_check), verbose=int(verbose), softening=softening_grid,
                    a_val=a_val, b_val=b_val, s_15_val=s_15_val, n_threads=n_threads_val,
                    total_np=total_np, ng_val=ng_val, ng_global_val=ng_global_val,
-                   ang_mom_scale=ang_mom_scale)
+                   ang_mom_scale=ang_mom_scale, units=conv)
 
 
 def _finish(call: FofCall, in_halo_out, halo_id_out, ang_mom_out, ierr):
@@ -251,7 +293,8 @@ def _native_call(call: FofCall):
     return _native.run(call.xp, call.vp, call.mp, call.np_halo, call.nhalo, call.L_Box,
                        call.link, call.np_halo_min, call.bound_check, call.verbose,
                        call.softening, call.a_val, call.b_val, call.s_15_val, call.n_threads,
-                       call.total_np, ng_val=call.ng_val, ng_global_val=call.ng_global_val)
+                       call.total_np, ng_val=call.ng_val, ng_global_val=call.ng_global_val,
+                       units=call.units)
 
 
 def _fof_core(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2,
@@ -268,7 +311,7 @@ def _fof_core(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2,
                     softening=softening, z=z, box=box, h0=h0, omega_m=omega_m,
                     omega_l=omega_l, n_sim=n_sim, units=units,
                     include_hubble_flow=include_hubble_flow, ng=ng, ng_global=ng_global,
-                    check_masses=False)
+                    check_masses=False, device_units=True)
     if not isinstance(call, FofCall):
         return call
     in_halo, halo_id, ang_mom, ierr = _native_call(call)
@@ -352,7 +395,7 @@ def fof_with_info(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2,
                     softening=softening, z=z, box=box, h0=h0, omega_m=omega_m,
                     omega_l=omega_l, n_sim=n_sim, units=units,
                     include_hubble_flow=include_hubble_flow, ng=ng, ng_global=ng_global,
-                    check_masses=False)
+                    check_masses=False, device_units=True)
     if not isinstance(call, FofCall):
         return catalogue_from_ids(*call, return_ang_mom=return_ang_mom)
     return _catalogue_call(call, return_ang_mom)
@@ -364,7 +407,8 @@ def _catalogue_call(call: FofCall, return_ang_mom, slot=None):
     ih, hid, am, ierr, members, offsets = _native.run_catalogue(
         call.xp, call.vp, call.mp, call.np_halo, call.nhalo, call.L_Box, call.link, call.np_halo_min,
         call.bound_check, call.verbose, call.softening, call.a_val, call.b_val, call.s_15_val,
-        call.n_threads, call.total_np, ng_val=call.ng_val, ng_global_val=call.ng_global_val, slot=slot)
+        call.n_threads, call.total_np, ng_val=call.ng_val, ng_global_val=call.ng_global_val, slot=slot,
+        units=call.units)
     in_halo, _, ang_mom = _finish(call, ih, hid, am, ierr)
     counts = np.diff(offsets)
     if counts.size == 0:

@@ -14,7 +14,7 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpyfof_b200.so")
-ABI_VERSION = 1
+ABI_VERSION = 2
 LAYOUT_AOS = 0
 LAYOUT_SOA = 1
 
@@ -30,12 +30,24 @@ _RUN_ARGS = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, 
              ctypes.c_double, ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p,
              ctypes.c_void_p, _dp]
 
+class Units(ctypes.Structure):
+    """pyfof_units_t: conversion of the inputs to code units on the device
+    (positions / x_div, velocities * v_mul, masses / m_div, or m_const for
+    every particle when there is no mass array)."""
+    _fields_ = [("x_div", ctypes.c_double), ("v_mul", ctypes.c_double),
+                ("m_div", ctypes.c_double), ("m_const", ctypes.c_double)]
+
+
+def _units_ptr(units):
+    return None if units is None else ctypes.byref(Units(*[float(v) for v in units]))
+
+
 # every symbol include/pyfof_b200.h declares
 EXPORTED = ("pyfof_version", "pyfof_init", "pyfof_shutdown", "pyfof_last_error",
             "pyfof_set_option", "pyfof_set_stream", "pyfof_get_stat", "pyfof_last_link_ms", "pyfof_last_stage_ms",
             "pyfof_halo_potential", "pyfof_halo_potential_direct_static", "pyfof_run",
             "pyfof_run_device", "pyfof_slot_create", "pyfof_slot_destroy", "pyfof_slot_run",
-            "pyfof_slot_stat", "pyfof_run_catalogue")
+            "pyfof_slot_stat", "pyfof_run_catalogue", "pyfof_run_units")
 
 
 class NativeLibraryError(RuntimeError):
@@ -88,7 +100,9 @@ def load():
         L.pyfof_slot_run.restype = ctypes.c_int32
         L.pyfof_slot_run.argtypes = [ctypes.c_void_p] + list(_RUN_ARGS)
         L.pyfof_run_catalogue.restype = ctypes.c_int32
-        L.pyfof_run_catalogue.argtypes = ([ctypes.c_void_p] + list(_RUN_ARGS[:19]) +
+        L.pyfof_run_units.restype = ctypes.c_int32
+        L.pyfof_run_units.argtypes = [ctypes.c_void_p, ctypes.POINTER(Units)] + list(_RUN_ARGS)
+        L.pyfof_run_catalogue.argtypes = ([ctypes.c_void_p, ctypes.POINTER(Units)] + list(_RUN_ARGS[:19]) +
                                           [_RUN_ARGS[20], _RUN_ARGS[21], ctypes.c_void_p,
                                            ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32)])
         L.pyfof_slot_stat.restype = ctypes.c_int32
@@ -145,12 +159,15 @@ def _ptr(a):
 
 
 def run(xp, vp, mp, np_halo, nhalo, L_Box, link, np_halo_min, bound_check, verbose, softening,
-        a_val, b_val, s_15_val, n_threads, total_np, ng_val=256, ng_global_val=512.0, slot=None):
+        a_val, b_val, s_15_val, n_threads, total_np, ng_val=256, ng_global_val=512.0, slot=None,
+        units=None):
     """Host-memory call with the f2py argument order of fof_fortran.fof_fortran.
 
     xp, vp: (3,N) float64 arrays, C- or Fortran-contiguous (vp may be None);
     mp: (N,) float64 or None.  `slot`: a handle of slot_create, else the
-    default context.  Returns (in_halo, halo_id, ang_mom, ierr).
+    default context.  `units`: (x_div, v_mul, m_div, m_const), the inputs'
+    conversion to code units done on the device, or None.  Returns
+    (in_halo, halo_id, ang_mom, ierr).
     """
     L = load()
     n = int(total_np)
@@ -177,14 +194,19 @@ def run(xp, vp, mp, np_halo, nhalo, L_Box, link, np_halo_min, bound_check, verbo
             int(bound_check), int(verbose), float(softening), float(a_val),
             float(b_val), float(s_15_val), int(n_threads), int(ng_val),
             float(ng_global_val), None, _ptr(halo_id), ang_mom.ctypes.data_as(_dp))
-    ierr = L.pyfof_run(*args) if slot is None else L.pyfof_slot_run(ctypes.c_void_p(slot), *args)
+    if units is not None:
+        ierr = L.pyfof_run_units(ctypes.c_void_p(slot) if slot else None, _units_ptr(units), *args)
+    elif slot is None:
+        ierr = L.pyfof_run(*args)
+    else:
+        ierr = L.pyfof_slot_run(ctypes.c_void_p(slot), *args)
     in_halo = halo_id > 0
     return in_halo, halo_id, ang_mom, int(ierr)
 
 
 def run_catalogue(xp, vp, mp, np_halo, nhalo, L_Box, link, np_halo_min, bound_check, verbose,
                   softening, a_val, b_val, s_15_val, n_threads, total_np, ng_val=256,
-                  ng_global_val=512.0, slot=None):
+                  ng_global_val=512.0, slot=None, units=None):
     """run() plus the halo catalogue built on the device.  Returns
     (in_halo, halo_id, ang_mom, ierr, members, offsets): members (int32)
     lists each valid halo's particle indices, ascending, halos in id order;
@@ -211,7 +233,7 @@ def run_catalogue(xp, vp, mp, np_halo, nhalo, L_Box, link, np_halo_min, bound_ch
     offsets = np.empty(cap, dtype=np.int64)
     nfound = ctypes.c_int32(0)
     ierr = L.pyfof_run_catalogue(
-        ctypes.c_void_p(slot) if slot else None, _ptr(xp), _ptr(vp), _ptr(mp), layout,
+        ctypes.c_void_p(slot) if slot else None, _units_ptr(units), _ptr(xp), _ptr(vp), _ptr(mp), layout,
         nph.ctypes.data_as(_i32p), int(nhalo), n, float(L_Box), float(link), int(np_halo_min),
         int(bound_check), int(verbose), float(softening), float(a_val), float(b_val), float(s_15_val),
         int(n_threads), int(ng_val), float(ng_global_val), _ptr(halo_id), ang_mom.ctypes.data_as(_dp),

@@ -326,33 +326,47 @@ static int32_t run_host(Context &ctx, const double *xp, const double *vp, const 
                         double L_Box, double linking_length, int32_t np_halo_min, int32_t bound_check,
                         int32_t verbose, double softening, double a_val, double b_val,
                         double s_15_val, int32_t n_threads, int64_t ng_val, double ng_global_val,
-                        int32_t *in_halo, int32_t *halo_id, double *ang_mom, CatalogueOut *cat) {
+                        int32_t *in_halo, int32_t *halo_id, double *ang_mom, CatalogueOut *cat,
+                        const pyfof_units_t *units) {
   PYFOF_CUDA(cudaSetDevice(ctx.device));
   cudaStream_t s = ctx.stream;
   const size_t n = (size_t)total_np;
+  const pyfof_units_t u = units ? *units : pyfof_units_t{1.0, 1.0, 1.0, 1.0};
+  const bool fill_m = !mp && u.m_const != 1.0;  // a constant mass other than the unit one
   FofArgs a;
-  a.xp = ctx.work.carve<double>(3 * n);
-  a.vp = vp ? ctx.work.carve<double>(3 * n) : nullptr;
-  a.mp = mp ? ctx.work.carve<double>(n) : nullptr;
+  double *xd = ctx.work.carve<double>(3 * n);
+  double *vd = vp ? ctx.work.carve<double>(3 * n) : nullptr;
+  double *md = (mp || fill_m) ? ctx.work.carve<double>(n) : nullptr;
+  a.xp = xd;
+  a.vp = vd;
+  a.mp = md;
   a.in_halo = ctx.work.carve<int32_t>(n);
   a.halo_id = ctx.work.carve<int32_t>(n);
-  if (!a.xp || (vp && !a.vp) || (mp && !a.mp) || !a.in_halo || !a.halo_id) {
+  if (!xd || (vp && !vd) || ((mp || fill_m) && !md) || !a.in_halo || !a.halo_id) {
     ctx.work.release();
     set_error("device allocation failed for %zu particles", n);
     return kAlloc;
   }
-  const bool side = vp || mp;
+  const bool side = vp || mp || fill_m;
   if (side) {
     // the buffers were allocated in the order of stream s
     PYFOF_CUDA(cudaEventRecord(ctx.ev_alloc, s));
     PYFOF_CUDA(cudaStreamWaitEvent(ctx.aux_stream, ctx.ev_alloc, 0));
   }
-  PYFOF_CUDA(cudaMemcpyAsync((void *)a.xp, xp, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
-  if (vp)
-    PYFOF_CUDA(cudaMemcpyAsync((void *)a.vp, vp, sizeof(double) * 3 * n, cudaMemcpyHostToDevice,
-                               ctx.aux_stream));
-  if (mp)
-    PYFOF_CUDA(cudaMemcpyAsync((void *)a.mp, mp, sizeof(double) * n, cudaMemcpyHostToDevice, ctx.aux_stream));
+  // conversions to code units run on the stream of their copy; the masses
+  // are converted after their check, inside the call
+  PYFOF_CUDA(cudaMemcpyAsync(xd, xp, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
+  if (u.x_div != 1.0) PYFOF_TRY(divide_inplace(xd, (int64_t)(3 * n), u.x_div, s));
+  if (vp) {
+    PYFOF_CUDA(cudaMemcpyAsync(vd, vp, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx.aux_stream));
+    if (u.v_mul != 1.0) PYFOF_TRY(multiply_inplace(vd, (int64_t)(3 * n), u.v_mul, ctx.aux_stream));
+  }
+  if (mp) {
+    PYFOF_CUDA(cudaMemcpyAsync(md, mp, sizeof(double) * n, cudaMemcpyHostToDevice, ctx.aux_stream));
+    a.m_div = u.m_div;
+  } else if (fill_m) {
+    PYFOF_TRY(fill_value(md, (int64_t)n, u.m_const, ctx.aux_stream));
+  }
   if (side) {
     PYFOF_CUDA(cudaEventRecord(ctx.ev_inputs, ctx.aux_stream));
     a.inputs_ready = ctx.ev_inputs;
@@ -412,7 +426,8 @@ static int32_t run_host_checked(Context *ctx, const double *xp, const double *vp
                                 int32_t bound_check, int32_t verbose, double softening, double a_val,
                                 double b_val, double s_15_val, int32_t n_threads, int64_t ng_val,
                                 double ng_global_val, int32_t *in_halo, int32_t *halo_id,
-                                double *ang_mom, CatalogueOut *cat = nullptr) {
+                                double *ang_mom, CatalogueOut *cat = nullptr,
+                                const pyfof_units_t *units = nullptr) {
   // outputs are written in full on success and zeroed on every other path
   auto zero = [&]() {
     if (total_np > 0) {
@@ -444,7 +459,7 @@ static int32_t run_host_checked(Context *ctx, const double *xp, const double *vp
     std::lock_guard<std::mutex> lk(ctx->mu);
     r = run_host(*ctx, xp, vp, mp, layout, np_halo, nhalo, total_np, L_Box, linking_length,
                  np_halo_min, bound_check, verbose, softening, a_val, b_val, s_15_val, n_threads,
-                 ng_val, ng_global_val, in_halo, halo_id, ang_mom, cat);
+                 ng_val, ng_global_val, in_halo, halo_id, ang_mom, cat, units);
   }
   if (r != kOk) zero();
   return r;
@@ -521,8 +536,24 @@ int32_t pyfof_run_device(const double *d_xp, const double *d_vp, const double *d
   return r;
 }
 
-int32_t pyfof_run_catalogue(void *slot, const double *xp, const double *vp, const double *mp,
-                            int32_t layout, const int32_t *np_halo, int32_t nhalo, int64_t total_np,
+int32_t pyfof_run_units(void *slot, const pyfof_units_t *units, const double *xp, const double *vp,
+                        const double *mp, int32_t layout, const int32_t *np_halo, int32_t nhalo,
+                        int64_t total_np, double L_Box, double linking_length, int32_t np_halo_min,
+                        int32_t bound_check, int32_t verbose, double softening, double a_val,
+                        double b_val, double s_15_val, int32_t n_threads, int64_t ng_val,
+                        double ng_global_val, int32_t *in_halo, int32_t *halo_id, double *ang_mom) {
+  if (slot && static_cast<Context *>(slot)->magic != Context::kMagic) {
+    set_error("pyfof_run_units: not a slot");
+    return kInvalid;
+  }
+  return run_host_checked(static_cast<Context *>(slot), xp, vp, mp, layout, np_halo, nhalo, total_np, L_Box,
+                          linking_length, np_halo_min, bound_check, verbose, softening, a_val, b_val,
+                          s_15_val, n_threads, ng_val, ng_global_val, in_halo, halo_id, ang_mom, nullptr,
+                          units);
+}
+
+int32_t pyfof_run_catalogue(void *slot, const pyfof_units_t *units, const double *xp, const double *vp,
+                            const double *mp, int32_t layout, const int32_t *np_halo, int32_t nhalo, int64_t total_np,
                             double L_Box, double linking_length, int32_t np_halo_min, int32_t bound_check,
                             int32_t verbose, double softening, double a_val, double b_val, double s_15_val,
                             int32_t n_threads, int64_t ng_val, double ng_global_val, int32_t *halo_id,
@@ -540,7 +571,8 @@ int32_t pyfof_run_catalogue(void *slot, const double *xp, const double *vp, cons
   *nhalo_found = 0;
   return run_host_checked(static_cast<Context *>(slot), xp, vp, mp, layout, np_halo, nhalo, total_np, L_Box,
                           linking_length, np_halo_min, bound_check, verbose, softening, a_val, b_val,
-                          s_15_val, n_threads, ng_val, ng_global_val, nullptr, halo_id, ang_mom, &cat);
+                          s_15_val, n_threads, ng_val, ng_global_val, nullptr, halo_id, ang_mom, &cat,
+                          units);
 }
 
 // ---------------------------------------------------------------- slots

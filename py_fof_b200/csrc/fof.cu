@@ -1162,23 +1162,68 @@ int32_t fof_plain_angmom(Context &ctx, const FofArgs &a, FofState &st) {
   return kOk;
 }
 
-// Every mass positive and finite (py_fof/__init__.py:259-260).
-__global__ void check_mass_kernel(const double *__restrict__ mp, int64_t n, int32_t *__restrict__ bad) {
+// Every mass positive and finite (py_fof/__init__.py:259-260); with
+// m_div != 1 each checked mass is then converted to code units, mp / m_grid
+// (py_fof/__init__.py:318-319), in the same pass.
+__global__ void check_mass_kernel(double *__restrict__ mp, int64_t n, int32_t *__restrict__ bad, double m_div) {
   int found = 0;
+  const bool conv = m_div != 1.0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const double m = mp[i];
     found |= !(m > 0.0 && m <= 1.7976931348623157e308);
+    if (conv) mp[i] = m / m_div;
   }
   if (__syncthreads_or(found) && threadIdx.x == 0) atomicExch(bad, 1);
 }
 
-int32_t check_masses(Context &ctx, const double *mp, int64_t n) {
+__global__ void divide_kernel(double *__restrict__ x, int64_t n, double d) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = x[i] / d;
+}
+
+__global__ void multiply_kernel(double *__restrict__ x, int64_t n, double f) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = x[i] * f;
+}
+
+__global__ void fill_kernel(double *__restrict__ x, int64_t n, double v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = v;
+}
+
+static unsigned stream_grid(int64_t n) {
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, BLK), (int64_t)kNumSMs * 8));
+}
+
+int32_t divide_inplace(double *x, int64_t n, double d, cudaStream_t s) {
+  if (n <= 0) return kOk;
+  divide_kernel<<<stream_grid(n), BLK, 0, s>>>(x, n, d);
+  PYFOF_CHECK_LAUNCH();
+  return kOk;
+}
+
+int32_t multiply_inplace(double *x, int64_t n, double f, cudaStream_t s) {
+  if (n <= 0) return kOk;
+  multiply_kernel<<<stream_grid(n), BLK, 0, s>>>(x, n, f);
+  PYFOF_CHECK_LAUNCH();
+  return kOk;
+}
+
+int32_t fill_value(double *x, int64_t n, double v, cudaStream_t s) {
+  if (n <= 0) return kOk;
+  fill_kernel<<<stream_grid(n), BLK, 0, s>>>(x, n, v);
+  PYFOF_CHECK_LAUNCH();
+  return kOk;
+}
+
+int32_t check_masses(Context &ctx, const double *mp, int64_t n, double m_div) {
   cudaStream_t s = ctx.stream;
   int32_t *bad = ctx.d_flags + FLAG_COUNT_C;
   PYFOF_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t), s));
-  const unsigned grid = (unsigned)std::min<int64_t>(ceil_div(n, BLK), (int64_t)kNumSMs * 8);
-  check_mass_kernel<<<grid, BLK, 0, s>>>(mp, n, bad);
+  // the mass array is only written when m_div != 1, and then it is the
+  // library's own copy of the caller's masses
+  check_mass_kernel<<<stream_grid(n), BLK, 0, s>>>(const_cast<double *>(mp), n, bad, m_div);
   PYFOF_CHECK_LAUNCH();
   PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags + FLAG_COUNT_C, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   PYFOF_CUDA(cudaStreamSynchronize(s));
@@ -1198,7 +1243,7 @@ int32_t fof_run(Context &ctx, const FofArgs &a) {
   PYFOF_TRY(fof_link_stage(ctx, a, st));
   PYFOF_TRY(fof_candidates_stage(ctx, a, st, !a.bound_check));
   if (a.inputs_ready) PYFOF_CUDA(cudaStreamWaitEvent(ctx.stream, a.inputs_ready, 0));
-  if (a.mp) PYFOF_TRY(check_masses(ctx, a.mp, a.total_np));
+  if (a.mp) PYFOF_TRY(check_masses(ctx, a.mp, a.total_np, a.m_div));
   if (ctx.timing) cudaEventRecord(ctx.ev[3], ctx.stream);
   if (!a.bound_check) PYFOF_TRY(fof_plain_angmom(ctx, a, st));
   else PYFOF_TRY(unbind_stage(ctx, a, st));

@@ -24,6 +24,9 @@ struct FofArgs {
   int32_t bound_fp64 = 0;  // 1: plain FP64 unbinding path instead of the FP32 product path
   int32_t bound_per_halo = 0;  // 1: FP64, one halo per launch sequence (the plain baseline)
   int64_t big_np = 0;          // PM halos above this many members use the chunked removal loop (0: default)
+  // masses are divided by m_div right after their check (code units); only
+  // with mp in the library's own scratch, which the check then rewrites
+  double m_div = 1.0;
   // recorded when vp and mp are on the device (they may still be copying
   // while the linking runs); null when they are already there
   cudaEvent_t inputs_ready = nullptr;
@@ -33,6 +36,13 @@ struct FofArgs {
 };
 
 struct Context;
+
+// In-place conversions of device arrays to code units, ordered on stream s:
+// x[i] / d, x[i] * f, and x[i] = v.  IEEE double operations, so the results
+// equal the host's.
+int32_t divide_inplace(double *x, int64_t n, double d, cudaStream_t s);
+int32_t multiply_inplace(double *x, int64_t n, double f, cudaStream_t s);
+int32_t fill_value(double *x, int64_t n, double v, cudaStream_t s);
 
 // Runs the whole call on ctx's stream; returns a reference ierr code (or
 // kCuda).  Synchronises the stream before returning.

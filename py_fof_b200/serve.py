@@ -132,7 +132,7 @@ class Server:
         yields its result dict (or raises its error)."""
         ret_am = bool(kw.get("return_ang_mom", False))
         try:
-            call = _prepare(xp_list, check_masses=False, **kw)
+            call = _prepare(xp_list, check_masses=False, device_units=True, **kw)
         except (ValueError, TypeError) as exc:
             f = cf.Future()
             f.set_exception(exc)

@@ -25,11 +25,12 @@ def _same_catalogue(a, b):
 def _device_and_host(xp_list, **kw):
     """Both catalogues of ONE native call: the device's and the one the host
     derives from that call's halo ids."""
-    call = P._prepare(xp_list, check_masses=False, **kw)
+    call = P._prepare(xp_list, check_masses=False, device_units=True, **kw)
     ih, hid, am, ierr, members, offsets = _native.run_catalogue(
         call.xp, call.vp, call.mp, call.np_halo, call.nhalo, call.L_Box, call.link, call.np_halo_min,
         call.bound_check, call.verbose, call.softening, call.a_val, call.b_val, call.s_15_val,
-        call.n_threads, call.total_np, ng_val=call.ng_val, ng_global_val=call.ng_global_val)
+        call.n_threads, call.total_np, ng_val=call.ng_val, ng_global_val=call.ng_global_val,
+        units=call.units)
     assert ierr == 0
     assert offsets[0] == 0 and np.all(np.diff(offsets) > 0) and offsets[-1] == members.size
     host = P.catalogue_from_ids(ih, hid)

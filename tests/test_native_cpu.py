@@ -66,6 +66,41 @@ def test_prepare_units():
     assert np.isclose(c.s_15_val, 15 * 0.67 * 256.0 / 300.0)
 
 
+@pytest.mark.parametrize("mass", ["array", "scalar", "n_sim", "none", "per_region"])
+@pytest.mark.parametrize("units", ["physical", "cube"])
+def test_device_units_carry_the_host_conversion(mass, units):
+    """_prepare(device_units=True) leaves the arrays in the caller's units and
+    carries the conversion; applying it (FofCall.on_host, the operations the
+    device performs) gives the host-converted call bit for bit."""
+    rng = np.random.default_rng(4)
+    xs = [rng.uniform(0, 300.0, (3, 40)), rng.uniform(0, 300.0, (3, 25))]
+    vs = [rng.normal(0, 300.0, (3, 40)), rng.normal(0, 300.0, (3, 25))]
+    kw = dict(vp_list=vs, L_Box=300.0, linking_length=0.3, units=units, z=0.7, softening=0.02,
+              bound_check=True, include_hubble_flow=True)
+    if mass == "array":
+        kw["mp_list"] = rng.uniform(1e9, 1e11, 65)
+    elif mass == "scalar":
+        kw["mp_list"] = 3.7e10
+    elif mass == "n_sim":
+        kw["n_sim"] = 256 ** 3
+    elif mass == "per_region":
+        kw["mp_list"] = [2e10, 5e9]
+    elif units == "physical":
+        kw["n_sim"] = 200 ** 3
+    host = P._prepare(xs, **kw)
+    dev = P._prepare(xs, device_units=True, **kw)
+    if units == "physical":
+        assert dev.units is not None and dev.units[0] != 1.0
+        assert np.array_equal(dev.xp, np.hstack(xs))  # unconverted
+    conv = dev.on_host()
+    assert conv.units is None
+    assert conv.xp.dtype == host.xp.dtype and np.array_equal(conv.xp, host.xp)
+    # vp/mp may be absent on one side where the other holds zeros / ones
+    for f in ("L_Box", "link", "softening", "a_val", "b_val", "s_15_val", "ang_mom_scale"):
+        assert getattr(conv, f) == getattr(host, f), f
+    assert all(x.dtype == y.dtype and np.array_equal(x, y) for x, y in zip(dev.dense(), host.dense()))
+
+
 def test_catalogue_from_ids():
     hid = np.array([0, 2, 1, 2, 0, 1, 3], np.int32)
     res = P.catalogue_from_ids(hid > 0, hid)

@@ -28,11 +28,12 @@ class OracleExec:
             self.most = max(self.most, self.now)
         try:
             time.sleep(self.delay)
-            vp, mp = call.dense()
-            if call.mp is not None and not np.all(np.isfinite(mp) & (mp > 0)):
+            if call.mp is not None and not np.all(np.isfinite(call.mp) & (call.mp > 0)):
                 n = call.total_np
                 return (np.zeros(n, np.int32), np.zeros(n, np.int32),
                         np.zeros((3, call.nhalo)), 5), self.peak
+            call = call.on_host()
+            vp, mp = call.dense()
             out = O.fof_fortran(np.asfortranarray(call.xp), np.asfortranarray(vp), mp, call.np_halo,
                                 call.nhalo, call.L_Box, call.link, call.np_halo_min, call.bound_check,
                                 call.verbose, call.softening, call.a_val, call.b_val, call.s_15_val,
