@@ -62,6 +62,7 @@ WORKLOADS = {
     # lognormal field boxes: name -> (n_side, mesh); L = n_side, np_halo_min 20
     "fof_lognormal_1024": ("lognormal", 1024, 512),
     "fof_lognormal_512": ("lognormal", 512, 256),
+    "fof_lognormal_256": ("lognormal", 256, 128),
     "fof_lognormal_128": ("lognormal", 128, 64),
 }
 # CPU sample of each workload: a sub-volume with the same recipe and density,
@@ -76,6 +77,7 @@ CPU_SAMPLE = {
     "unbind_nfw_2k": "unbind_nfw_2k:300",
     "fof_lognormal_1024": "fof_lognormal_128",
     "fof_lognormal_512": "fof_lognormal_128",
+    "fof_lognormal_256": "fof_lognormal_128",
     "fof_lognormal_128": "fof_lognormal_128",
 }
 LINK = 0.2

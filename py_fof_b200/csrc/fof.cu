@@ -9,13 +9,17 @@
 //   3. fof_key_kernel     global cell key per particle + cell histogram
 //   4. stable radix sort  (cell key, particle index): the reference CRS order
 //   5. fof_gather_kernel  FP32 sorted coordinates (real(x_rel,4))
-//   6. fof_link_kernel    pair tests over the reference's neighbour cells,
+//   6. link kernels       pair tests over the reference's neighbour cells
+//                         (fof_link_dense_kernel for cells with more than
+//                         DENSE_T particles and their pairs with sparse
+//                         cells, fof_link_kernel for sparse-cell pairs),
 //                         lock-free atomicCAS union (lower index wins)
 //   7. fof_root_kernel    full compression + warp-aggregated group sizes
 //   8. scan of root flags -> candidate ranks (region order, then root CRS
 //                         position: the reference halo numbering)
 //   9. outputs, FP64 centre-of-mass / angular momentum per candidate
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 
@@ -216,8 +220,9 @@ __device__ __forceinline__ bool linked_pbc(float4 a, float4 b, const LinkParams 
 // are listed by sub-cell in dpos[], sub_tab holds the offsets.  A pair test
 // against such a cell only visits the sub-cells that overlap the cube of
 // half-width `reach` around the particle, which contains every partner the
-// exact distance test can accept.  Their particles are linked by the
-// warp-cooperative kernel.
+// exact distance test can accept.  Their particles, and every pair between
+// a dense and a sparse cell, are linked by the dense-cell kernel; pairs of
+// sparse cells by the per-particle kernel.
 constexpr int DENSE_T = 12;
 constexpr int SUB_MAX = 216;
 
@@ -240,6 +245,29 @@ __device__ __forceinline__ int sub_of(float x, float lo, float inv_sub, int s) {
   return (int)t;
 }
 
+// Sub-cell layout of a dense cell with n particles: about SUB_OCC particles
+// per sub-cell (floor(cbrt(n / SUB_OCC)) slabs per axis), at most the
+// region's sub[d] (slabs at least one linking length wide).  Few, well
+// filled sub-cells keep the number of source ranges a query walks small.
+// Build and queries use this one function, so they agree on every cell.
+constexpr float SUB_OCC = 6.0f;
+
+struct SubGrid {
+  int s[3];
+  float inv[3];  // sub-cells per unit length
+};
+
+__device__ __forceinline__ SubGrid dense_sub(const RegionDev &r, int64_t n) {
+  SubGrid g;
+  const int k = max(1, (int)cbrtf(__fdiv_rn((float)n, SUB_OCC)));
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    g.s[d] = min(k, r.sub[d]);
+    g.inv[d] = g.s[d] == r.sub[d] ? r.inv_sub[d] : __double2float_rn((double)g.s[d] / r.size[d]);
+  }
+  return g;
+}
+
 __device__ __forceinline__ float cell_lower(const RegionDev &r, int d, int64_t i) {
   return __double2float_rn(__dadd_rn(r.origin[d], __dmul_rn((double)i, r.size[d])));
 }
@@ -256,7 +284,14 @@ __device__ __forceinline__ void link_pair(int *parent, int p, int q, int &rp, in
   }
 }
 
-__global__ void __launch_bounds__(BLK, 3) fof_link_kernel(
+// Ordered-integer image of a float (monotone: a < b  <=>  key(a) < key(b)
+// for non-NaN values), so warp min/max reductions of coordinates can use the
+// integer reduction instructions.  The map is its own inverse.
+// Sparse-cell particles, one thread each: pair tests against the sparse
+// cells among the neighbour cells the cube of half-width `reach` around the
+// particle touches, from the lower cell (in one cell, from the lower sorted
+// position).  Pairs with dense-cell particles are the dense kernel's.
+__global__ void __launch_bounds__(BLK, 4) fof_link_kernel(
     const float4 *__restrict__ pos, const uint32_t *__restrict__ skey,
     const uint32_t *__restrict__ prid, const RegionDev *__restrict__ R,
     const uint32_t *__restrict__ cell_start, int *parent, int64_t w0, int64_t w1, LinkParams P,
@@ -266,25 +301,19 @@ __global__ void __launch_bounds__(BLK, 3) fof_link_kernel(
     const int64_t p = D.order[w];
     const float4 me = pos[p];
     const RegionDev &r = R[prid[p]];
-    const int64_t local = (int64_t)skey[p] - (int64_t)r.cell_off;
+    const uint32_t local = skey[p] - (uint32_t)r.cell_off;
     const int64_t N0 = r.N[0], N1 = r.N[1], N2 = r.N[2];
     int64_t ixyz[3];
-    if (r.ncell <= 0xffffffffll) {
-      const uint32_t l32 = (uint32_t)local, n0 = (uint32_t)N0, n1 = (uint32_t)N1;
-      const uint32_t q0 = l32 / n0;
-      ixyz[0] = l32 - q0 * n0;
+    {
+      const uint32_t n0 = (uint32_t)N0, n1 = (uint32_t)N1;
+      const uint32_t q0 = local / n0;
+      ixyz[0] = local - q0 * n0;
       ixyz[1] = q0 % n1;
       ixyz[2] = q0 / n1;
-    } else {
-      ixyz[0] = local % N0;
-      ixyz[1] = (local / N0) % N1;
-      ixyz[2] = local / (N0 * N1);
     }
     const int64_t Nd[3] = {N0, N1, N2};
     const bool per = r.periodic != 0;
     const float mexyz[3] = {me.x, me.y, me.z};
-    // neighbour offsets per axis: only cells the cube of half-width `reach`
-    // around p can touch (any linked partner lies inside that cube)
     int lo[3], hi[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -299,60 +328,34 @@ __global__ void __launch_bounds__(BLK, 3) fof_link_kernel(
     }
     const int ip = (int)p;
     int rp = -1;  // cached root of p
+    // (the distance test takes the minimum image itself: a wrapped cell
+    // needs no coordinate shift)
     for (int dz = lo[2]; dz <= hi[2]; ++dz) {
       int64_t jz = ixyz[2] + dz;
-      double shz = 0.0;
       if ((r.pdim >> 2) & 1) {
-        if (jz < 0) { jz += N2; shz = P.L; } else if (jz >= N2) { jz -= N2; shz = -P.L; }
+        if (jz < 0) jz += N2; else if (jz >= N2) jz -= N2;
       } else if (jz < 0 || jz >= N2) continue;
       for (int dy = lo[1]; dy <= hi[1]; ++dy) {
         int64_t jy = ixyz[1] + dy;
-        double shy = 0.0;
         if ((r.pdim >> 1) & 1) {
-          if (jy < 0) { jy += N1; shy = P.L; } else if (jy >= N1) { jy -= N1; shy = -P.L; }
+          if (jy < 0) jy += N1; else if (jy >= N1) jy -= N1;
         } else if (jy < 0 || jy >= N1) continue;
         for (int dx = lo[0]; dx <= hi[0]; ++dx) {
           int64_t jx = ixyz[0] + dx;
-          double shx = 0.0;
           if (r.pdim & 1) {
-            if (jx < 0) { jx += N0; shx = P.L; } else if (jx >= N0) { jx -= N0; shx = -P.L; }
+            if (jx < 0) jx += N0; else if (jx >= N0) jx -= N0;
           } else if (jx < 0 || jx >= N0) continue;
           const int64_t jl = jx + N0 * (jy + N1 * jz);
-          if (jl < local) continue;
+          if (jl < (int64_t)local) continue;
           const uint64_t jc = r.cell_off + (uint64_t)jl;
           const int64_t b = cell_start[jc];
           const int64_t e = cell_start[jc + 1];
-          const bool own = (jl == local);
-          if (e - b > DENSE_T) {
-            const uint32_t *tab = D.tab + (int64_t)D.rank[jc] * D.stride;
-            const int64_t jcoord[3] = {jx, jy, jz};
-            const double sh[3] = {shx, shy, shz};
-            int slo[3], shi[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              const float clo = cell_lower(r, d, jcoord[d]);
-              const float xs = __fadd_rn(mexyz[d], (float)sh[d]);
-              slo[d] = sub_of(__fsub_rn(xs, D.reach), clo, r.inv_sub[d], r.sub[d]);
-              shi[d] = sub_of(__fadd_rn(xs, D.reach), clo, r.inv_sub[d], r.sub[d]);
-            }
-            for (int sz = slo[2]; sz <= shi[2]; ++sz)
-              for (int sy = slo[1]; sy <= shi[1]; ++sy) {
-                const int s0 = slo[0] + r.sub[0] * (sy + r.sub[1] * sz);
-                const int64_t k0 = tab[s0], k1 = tab[s0 + (shi[0] - slo[0]) + 1];
-                for (int64_t k = k0; k < k1; ++k) {
-                  const float4 o = D.dpos[b + k];
-                  const int q = __float_as_int(o.w);
-                  if (own && q <= ip) continue;
-                  const bool lk = per ? linked_pbc(me, o, P) : linked_open(me, o, P.rp2_open);
-                  if (lk) link_pair(parent, ip, q, rp, flags);
-                }
-              }
-          } else {
-            for (int64_t q = own ? p + 1 : b; q < e; ++q) {
-              const float4 o = pos[q];
-              const bool lk = per ? linked_pbc(me, o, P) : linked_open(me, o, P.rp2_open);
-              if (lk) link_pair(parent, ip, (int)q, rp, flags);
-            }
+          if (e - b > DENSE_T) continue;  // pairs with a dense cell: the dense kernel
+          const bool own = (jl == (int64_t)local);
+          for (int64_t q = own ? p + 1 : b; q < e; ++q) {
+            const float4 o = pos[q];
+            const bool lk = per ? linked_pbc(me, o, P) : linked_open(me, o, P.rp2_open);
+            if (lk) link_pair(parent, ip, (int)q, rp, flags);
           }
         }
       }
@@ -366,10 +369,15 @@ __global__ void __launch_bounds__(BLK, 3) fof_link_kernel(
 // bounding box widened by `reach` can touch.  Sources come in coalesced
 // batches of 32; a source enters the pair loop only if it lies inside the
 // widened box, and then every lane tests it against its own particle with
-// the exact reference test.  Each pair is tested from the same side as in
-// the per-particle kernel (lower cell; in the own cell the lower sorted
-// position), so the set of linked pairs, and with it the partition, is the
-// same.
+// the exact reference test.
+//
+// Which side tests a pair: two dense cells, this kernel from the lower cell
+// (in one cell, from the lower sorted position); a dense and a sparse cell,
+// this kernel from the dense cell, whichever key is lower; two sparse cells,
+// the per-particle kernel.  Every pair within reach is tested once, and the
+// reference test is symmetric (|a - b| = |b - a| in IEEE arithmetic), so
+// the set of linked pairs, and with it the partition, equals the
+// reference's.
 struct DenseChunk {
   uint32_t cell, e0;  // dense cell (global cell index), first index in its dpos list
 };
@@ -438,10 +446,11 @@ __global__ void __launch_bounds__(BLK, 2) fof_link_dense_kernel(
             if (jx < 0) { jx += N0; shx = (float)P.L; } else if (jx >= N0) { jx -= N0; shx = -(float)P.L; }
           } else if (jx < 0 || jx >= N0) continue;
           const int64_t jl = jx + N0 * (jy + N1 * jz);
-          if (jl < local) continue;
           const uint64_t jc = r.cell_off + (uint64_t)jl;
           const int64_t b = cell_start[jc];
           const int64_t e = cell_start[jc + 1];
+          const bool dense = e - b > DENSE_T;
+          if ((dense && jl < local) || e == b) continue;
           const bool own = (jl == local);
           const float sh[3] = {shx, shy, shz};
           // the widened box in the neighbour cell's frame
@@ -460,24 +469,27 @@ __global__ void __launch_bounds__(BLK, 2) fof_link_dense_kernel(
           }
           // source ranges: one range for a plain cell, one per sub-cell row
           // for a dense cell
-          const bool dense = e - b > DENSE_T;
           int slo[3] = {0, 0, 0}, shi[3] = {0, 0, 0};
+          int gs0 = 1, gs1 = 1;
           const uint32_t *tab = nullptr;
           if (dense) {
             tab = D.tab + (int64_t)D.rank[jc] * D.stride;
+            const SubGrid g = dense_sub(r, e - b);
+            gs0 = g.s[0];
+            gs1 = g.s[1];
             const int64_t jcoord[3] = {jx, jy, jz};
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
               const float clo = cell_lower(r, d, jcoord[d]);
-              slo[d] = sub_of(wl[d], clo, r.inv_sub[d], r.sub[d]);
-              shi[d] = sub_of(wh[d], clo, r.inv_sub[d], r.sub[d]);
+              slo[d] = sub_of(wl[d], clo, g.inv[d], g.s[d]);
+              shi[d] = sub_of(wh[d], clo, g.inv[d], g.s[d]);
             }
           }
           for (int sz = slo[2]; sz <= shi[2]; ++sz)
             for (int sy = slo[1]; sy <= shi[1]; ++sy) {
               int64_t k0, k1;
               if (dense) {
-                const int s0 = slo[0] + r.sub[0] * (sy + r.sub[1] * sz);
+                const int s0 = slo[0] + gs0 * (sy + gs1 * sz);
                 k0 = tab[s0];
                 k1 = tab[s0 + (shi[0] - slo[0]) + 1];
               } else {
@@ -598,17 +610,18 @@ __global__ void __launch_bounds__(BLK) fof_dense_build_kernel(
   const int64_t ic[3] = {local % N0, (local / N0) % N1, local / (N0 * N1)};
   float clo[3];
   for (int d = 0; d < 3; ++d) clo[d] = cell_lower(r, d, ic[d]);
-  const int S = r.sub[0] * r.sub[1] * r.sub[2];
   for (int k = threadIdx.x; k <= SUB_MAX; k += BLK) hist[k] = 0;
   __syncthreads();
   const int64_t base = cs[c];
   const int64_t n = (int64_t)cs[c + 1] - base;
+  const SubGrid g = dense_sub(r, n);
+  const int S = g.s[0] * g.s[1] * g.s[2];
   for (int64_t k = threadIdx.x; k < n; k += BLK) {
     const float4 v = pos[base + k];
-    const int sx = sub_of(v.x, clo[0], r.inv_sub[0], r.sub[0]);
-    const int sy = sub_of(v.y, clo[1], r.inv_sub[1], r.sub[1]);
-    const int sz = sub_of(v.z, clo[2], r.inv_sub[2], r.sub[2]);
-    atomicAdd(&hist[sx + r.sub[0] * (sy + r.sub[1] * sz)], 1u);
+    const int sx = sub_of(v.x, clo[0], g.inv[0], g.s[0]);
+    const int sy = sub_of(v.y, clo[1], g.inv[1], g.s[1]);
+    const int sz = sub_of(v.z, clo[2], g.inv[2], g.s[2]);
+    atomicAdd(&hist[sx + g.s[0] * (sy + g.s[1] * sz)], 1u);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -626,10 +639,10 @@ __global__ void __launch_bounds__(BLK) fof_dense_build_kernel(
   __syncthreads();
   for (int64_t k = threadIdx.x; k < n; k += BLK) {
     const float4 v = pos[base + k];
-    const int sx = sub_of(v.x, clo[0], r.inv_sub[0], r.sub[0]);
-    const int sy = sub_of(v.y, clo[1], r.inv_sub[1], r.sub[1]);
-    const int sz = sub_of(v.z, clo[2], r.inv_sub[2], r.sub[2]);
-    const uint32_t slot = atomicAdd(&cur[sx + r.sub[0] * (sy + r.sub[1] * sz)], 1u);
+    const int sx = sub_of(v.x, clo[0], g.inv[0], g.s[0]);
+    const int sy = sub_of(v.y, clo[1], g.inv[1], g.s[1]);
+    const int sz = sub_of(v.z, clo[2], g.inv[2], g.s[2]);
+    const uint32_t slot = atomicAdd(&cur[sx + g.s[0] * (sy + g.s[1] * sz)], 1u);
     dpos[base + slot] = make_float4(v.x, v.y, v.z, __int_as_float((int)(base + k)));
   }
 }

@@ -78,6 +78,36 @@ def test_small_periodic_boxes(L, link):
     _assert_same(g, o)
 
 
+@pytest.mark.parametrize("L,link,n", [(3.0, 0.5, 40), (2.0, 0.6, 12), (1.2, 0.5, 20), (1.5, 0.45, 30),
+                                      (5.0, 0.6, 200), (7.0, 1.1, 150)])
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_sparse_small_periodic_boxes(L, link, n, seed):
+    """Few particles per cell in boxes of 2 to 6 cells per axis: the row
+    kernel's wrapped ranges, shifted boxes and skipped rows."""
+    rng = np.random.default_rng(seed + int(10 * L))
+    xp = rng.uniform(0, L, (3, n))
+    g, o = _both(xp, L_Box=L, linking_length=link, np_halo_min=2)
+    _assert_same(g, o)
+
+
+def test_sparse_rows_with_dense_cells():
+    """Sparse rows interleaved with dense cells, in a periodic box and in an
+    open region: pairs between sparse and dense cells from both sides."""
+    rng = np.random.default_rng(11)
+    for L, open_region in ((24.0, False), (1000.0, True)):
+        lo = 0.0 if not open_region else 400.0
+        span = L if not open_region else 24.0
+        back = rng.uniform(lo, lo + span, (3, int(2.5 * span ** 3)))
+        cents = rng.uniform(lo, lo + span, (3, 40))
+        clumps = np.concatenate([c[:, None] + rng.normal(0, 0.15, (3, 60)) for c in cents.T], axis=1)
+        xp = np.concatenate([back, clumps], axis=1)
+        if not open_region:
+            xp = np.mod(xp, L)
+        g, o = _both(xp, L_Box=L, linking_length=0.2, np_halo_min=5)
+        assert o[1].max() > 10
+        _assert_same(g, o)
+
+
 def test_partially_periodic_filament():
     rng = np.random.default_rng(5)
     n = 6000
