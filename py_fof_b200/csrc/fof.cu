@@ -287,79 +287,153 @@ __device__ __forceinline__ void link_pair(int *parent, int p, int q, int &rp, in
 // Ordered-integer image of a float (monotone: a < b  <=>  key(a) < key(b)
 // for non-NaN values), so warp min/max reductions of coordinates can use the
 // integer reduction instructions.  The map is its own inverse.
-// Sparse-cell particles, one thread each: pair tests against the sparse
-// cells among the neighbour cells the cube of half-width `reach` around the
-// particle touches, from the lower cell (in one cell, from the lower sorted
-// position).  Pairs with dense-cell particles are the dense kernel's.
+// Sparse-cell particles, a warp per 32 consecutive entries of the sparse
+// work order.  Each lane lists the source ranges of its particle: the
+// sparse cells among the neighbour cells that the cube of half-width
+// `reach` around it touches, from its own cell on (higher keys; in the own
+// cell, the higher sorted positions).  That is at most 8 cells where cells
+// are wider than two linking lengths; narrower cells, and the key order of
+// wrapped periodic neighbours, allow up to all 27, and a lane tests the
+// ranges beyond the first MAX_RANGES itself, right away.  The warp then
+// runs all pairs of all lanes in rounds of 32, one pair per lane (a lane
+// finds its pair's particle by a binary search over the lanes' pair
+// offsets and its source by walking that particle's ranges), so the lanes
+// stay busy however unevenly the pairs are spread over the particles.
+// Pairs with dense-cell particles are the dense kernel's.
+constexpr int MAX_RANGES = 8;
+
 __global__ void __launch_bounds__(BLK, 4) fof_link_kernel(
     const float4 *__restrict__ pos, const uint32_t *__restrict__ skey,
     const uint32_t *__restrict__ prid, const RegionDev *__restrict__ R,
     const uint32_t *__restrict__ cell_start, int *parent, int64_t w0, int64_t w1, LinkParams P,
     DenseIndex D, int32_t *flags) {
-  for (int64_t w = w0 + (int64_t)blockIdx.x * BLK + threadIdx.x; w < w1;
-       w += (int64_t)gridDim.x * BLK) {
-    const int64_t p = D.order[w];
-    const float4 me = pos[p];
-    const RegionDev &r = R[prid[p]];
-    const uint32_t local = skey[p] - (uint32_t)r.cell_off;
-    const int64_t N0 = r.N[0], N1 = r.N[1], N2 = r.N[2];
-    int64_t ixyz[3];
-    {
-      const uint32_t n0 = (uint32_t)N0, n1 = (uint32_t)N1;
-      const uint32_t q0 = local / n0;
-      ixyz[0] = local - q0 * n0;
-      ixyz[1] = q0 % n1;
-      ixyz[2] = q0 / n1;
-    }
-    const int64_t Nd[3] = {N0, N1, N2};
-    const bool per = r.periodic != 0;
-    const float mexyz[3] = {me.x, me.y, me.z};
-    int lo[3], hi[3];
+  constexpr unsigned FULL = 0xffffffffu;
+  __shared__ uint2 ranges[BLK][MAX_RANGES];  // (first source, count)
+  const int lane = threadIdx.x & 31;
+  const int wbase_t = threadIdx.x & ~31;
+  const int64_t nw = ((int64_t)gridDim.x * BLK) >> 5;
+  for (int64_t wb = w0 + (((int64_t)blockIdx.x * BLK + threadIdx.x) >> 5) * 32; wb < w1; wb += nw * 32) {
+    const int64_t w = wb + lane;
+    const bool valid = w < w1;
+    const int ip = valid ? (int)D.order[w] : 0;
+    const float4 me = valid ? pos[ip] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const RegionDev &r = R[valid ? prid[ip] : 0];
+    uint32_t total = 0;
+    int nr = 0;
+    if (valid) {
+      const uint32_t local = skey[ip] - (uint32_t)r.cell_off;
+      const int64_t N0 = r.N[0], N1 = r.N[1], N2 = r.N[2];
+      int64_t ixyz[3];
+      {
+        const uint32_t n0 = (uint32_t)N0, n1 = (uint32_t)N1;
+        const uint32_t q0 = local / n0;
+        ixyz[0] = local - q0 * n0;
+        ixyz[1] = q0 % n1;
+        ixyz[2] = q0 / n1;
+      }
+      const int64_t Nd[3] = {N0, N1, N2};
+      const float mexyz[3] = {me.x, me.y, me.z};
+      int lo[3], hi[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const bool pd = (r.pdim >> d) & 1;
-      if (Nd[d] == 1) { lo[d] = 0; hi[d] = 0; continue; }
-      const float clo = cell_lower(r, d, ixyz[d]);
-      const float chi = cell_lower(r, d, ixyz[d] + 1);
-      const bool below = __fsub_rn(mexyz[d], D.reach) < clo;
-      const bool above = __fadd_rn(mexyz[d], D.reach) >= chi;
-      if (pd && Nd[d] == 2) { lo[d] = 0; hi[d] = (below || above) ? 1 : 0; }
-      else { lo[d] = below ? -1 : 0; hi[d] = above ? 1 : 0; }
-    }
-    const int ip = (int)p;
-    int rp = -1;  // cached root of p
-    // (the distance test takes the minimum image itself: a wrapped cell
-    // needs no coordinate shift)
-    for (int dz = lo[2]; dz <= hi[2]; ++dz) {
-      int64_t jz = ixyz[2] + dz;
-      if ((r.pdim >> 2) & 1) {
-        if (jz < 0) jz += N2; else if (jz >= N2) jz -= N2;
-      } else if (jz < 0 || jz >= N2) continue;
-      for (int dy = lo[1]; dy <= hi[1]; ++dy) {
-        int64_t jy = ixyz[1] + dy;
-        if ((r.pdim >> 1) & 1) {
-          if (jy < 0) jy += N1; else if (jy >= N1) jy -= N1;
-        } else if (jy < 0 || jy >= N1) continue;
-        for (int dx = lo[0]; dx <= hi[0]; ++dx) {
-          int64_t jx = ixyz[0] + dx;
-          if (r.pdim & 1) {
-            if (jx < 0) jx += N0; else if (jx >= N0) jx -= N0;
-          } else if (jx < 0 || jx >= N0) continue;
-          const int64_t jl = jx + N0 * (jy + N1 * jz);
-          if (jl < (int64_t)local) continue;
-          const uint64_t jc = r.cell_off + (uint64_t)jl;
-          const int64_t b = cell_start[jc];
-          const int64_t e = cell_start[jc + 1];
-          if (e - b > DENSE_T) continue;  // pairs with a dense cell: the dense kernel
-          const bool own = (jl == (int64_t)local);
-          for (int64_t q = own ? p + 1 : b; q < e; ++q) {
-            const float4 o = pos[q];
-            const bool lk = per ? linked_pbc(me, o, P) : linked_open(me, o, P.rp2_open);
-            if (lk) link_pair(parent, ip, (int)q, rp, flags);
+      for (int d = 0; d < 3; ++d) {
+        const bool pd = (r.pdim >> d) & 1;
+        if (Nd[d] == 1) { lo[d] = 0; hi[d] = 0; continue; }
+        const float clo = cell_lower(r, d, ixyz[d]);
+        const float chi = cell_lower(r, d, ixyz[d] + 1);
+        const bool below = __fsub_rn(mexyz[d], D.reach) < clo;
+        const bool above = __fadd_rn(mexyz[d], D.reach) >= chi;
+        if (pd && Nd[d] == 2) { lo[d] = 0; hi[d] = (below || above) ? 1 : 0; }
+        else { lo[d] = below ? -1 : 0; hi[d] = above ? 1 : 0; }
+      }
+      // (the distance test takes the minimum image itself: a wrapped cell
+      // needs no coordinate shift)
+      for (int dz = lo[2]; dz <= hi[2]; ++dz) {
+        int64_t jz = ixyz[2] + dz;
+        if ((r.pdim >> 2) & 1) {
+          if (jz < 0) jz += N2; else if (jz >= N2) jz -= N2;
+        } else if (jz < 0 || jz >= N2) continue;
+        for (int dy = lo[1]; dy <= hi[1]; ++dy) {
+          int64_t jy = ixyz[1] + dy;
+          if ((r.pdim >> 1) & 1) {
+            if (jy < 0) jy += N1; else if (jy >= N1) jy -= N1;
+          } else if (jy < 0 || jy >= N1) continue;
+          for (int dx = lo[0]; dx <= hi[0]; ++dx) {
+            int64_t jx = ixyz[0] + dx;
+            if (r.pdim & 1) {
+              if (jx < 0) jx += N0; else if (jx >= N0) jx -= N0;
+            } else if (jx < 0 || jx >= N0) continue;
+            const int64_t jl = jx + N0 * (jy + N1 * jz);
+            if (jl < (int64_t)local) continue;
+            const uint64_t jc = r.cell_off + (uint64_t)jl;
+            uint32_t b = cell_start[jc];
+            const uint32_t e = cell_start[jc + 1];
+            if (e - b > (uint32_t)DENSE_T) continue;  // pairs with a dense cell: the dense kernel
+            if (jl == (int64_t)local) b = (uint32_t)ip + 1;
+            if (e <= b) continue;
+            if (nr < MAX_RANGES) {
+              ranges[threadIdx.x][nr++] = make_uint2(b, e - b);
+              total += e - b;
+            } else {
+              const bool per = r.periodic != 0;
+              for (uint32_t q = b; q < e; ++q) {
+                const float4 o = pos[q];
+                const bool lk = per ? linked_pbc(me, o, P) : linked_open(me, o, P.rp2_open);
+                if (lk) {
+                  int rp = -1;
+                  link_pair(parent, ip, (int)q, rp, flags);
+                }
+              }
+            }
           }
         }
       }
     }
+    // pair offsets of the lanes
+    uint32_t incl = total;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const uint32_t excl = incl - total;
+    const uint32_t T = __shfl_sync(FULL, incl, 31);
+    __syncwarp();
+    for (uint32_t g0 = 0; g0 < T; g0 += 32) {
+      const uint32_t g = g0 + (uint32_t)lane;
+      // owner lane of pair g: the number of lanes whose pairs end at or before g
+      int owner = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const uint32_t v = __shfl_sync(FULL, incl, owner + step - 1);
+        if (v <= g) owner += step;
+      }
+      owner &= 31;
+      const uint32_t oexcl = __shfl_sync(FULL, excl, owner);
+      const int po = __shfl_sync(FULL, ip, owner);
+      float4 pm;
+      pm.x = __shfl_sync(FULL, me.x, owner);
+      pm.y = __shfl_sync(FULL, me.y, owner);
+      pm.z = __shfl_sync(FULL, me.z, owner);
+      pm.w = 0.f;
+      const bool per = __shfl_sync(FULL, r.periodic, owner) != 0;
+      if (g < T) {
+        uint32_t j = g - oexcl;
+        const uint2 *rg = ranges[wbase_t + owner];
+        int k = 0;
+        while (j >= rg[k].y) {
+          j -= rg[k].y;
+          ++k;
+        }
+        const int q = (int)(rg[k].x + j);
+        const float4 o = pos[q];
+        const bool lk = per ? linked_pbc(pm, o, P) : linked_open(pm, o, P.rp2_open);
+        if (lk) {
+          int rp = -1;
+          link_pair(parent, po, q, rp, flags);
+        }
+      }
+    }
+    __syncwarp();
   }
 }
 
