@@ -461,7 +461,9 @@ __global__ void __launch_bounds__(BLK, 2) fof_link_dense_kernel(
     const uint32_t *__restrict__ cell_start, int *parent, const DenseChunk *__restrict__ chunks,
     int64_t nchunks, LinkParams P, DenseIndex D, int32_t *flags) {
   constexpr unsigned FULL = 0xffffffffu;
+  __shared__ float4 sbuf[BLK];
   const int lane = threadIdx.x & 31;
+  float4 *wbuf = sbuf + (threadIdx.x & ~31);
   const int64_t nw = ((int64_t)gridDim.x * BLK) >> 5;
   for (int64_t ch = ((int64_t)blockIdx.x * BLK + threadIdx.x) >> 5; ch < nchunks; ch += nw) {
     const DenseChunk C = chunks[ch];
@@ -489,9 +491,11 @@ __global__ void __launch_bounds__(BLK, 2) fof_link_dense_kernel(
         bh[d] = fmaxf(bh[d], __shfl_xor_sync(FULL, bh[d], o));
       }
     int lo[3], hi[3];
+    bool open_ax[3];  // periodic axes of one or two cells: no box along them
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const bool pd = (r.pdim >> d) & 1;
+      open_ax[d] = pd && Nd[d] <= 2;
       if (Nd[d] == 1) { lo[d] = 0; hi[d] = 0; continue; }
       const float clo = cell_lower(r, d, ixyz[d]);
       const float chi = cell_lower(r, d, ixyz[d] + 1);
@@ -500,111 +504,174 @@ __global__ void __launch_bounds__(BLK, 2) fof_link_dense_kernel(
       if (pd && Nd[d] == 2) { lo[d] = 0; hi[d] = (below || above) ? 1 : 0; }
       else { lo[d] = below ? -1 : 0; hi[d] = above ? 1 : 0; }
     }
-    int rp = -1;  // cached root of this lane's particle
-    for (int dz = lo[2]; dz <= hi[2]; ++dz) {
-      int64_t jz = ixyz[2] + dz;
-      float shz = 0.f;
-      if ((r.pdim >> 2) & 1) {
-        if (jz < 0) { jz += N2; shz = (float)P.L; } else if (jz >= N2) { jz -= N2; shz = -(float)P.L; }
-      } else if (jz < 0 || jz >= N2) continue;
-      for (int dy = lo[1]; dy <= hi[1]; ++dy) {
-        int64_t jy = ixyz[1] + dy;
-        float shy = 0.f;
-        if ((r.pdim >> 1) & 1) {
-          if (jy < 0) { jy += N1; shy = (float)P.L; } else if (jy >= N1) { jy -= N1; shy = -(float)P.L; }
-        } else if (jy < 0 || jy >= N1) continue;
-        for (int dx = lo[0]; dx <= hi[0]; ++dx) {
-          int64_t jx = ixyz[0] + dx;
-          float shx = 0.f;
-          if (r.pdim & 1) {
-            if (jx < 0) { jx += N0; shx = (float)P.L; } else if (jx >= N0) { jx -= N0; shx = -(float)P.L; }
-          } else if (jx < 0 || jx >= N0) continue;
-          const int64_t jl = jx + N0 * (jy + N1 * jz);
-          const uint64_t jc = r.cell_off + (uint64_t)jl;
-          const int64_t b = cell_start[jc];
-          const int64_t e = cell_start[jc + 1];
-          const bool dense = e - b > DENSE_T;
-          if ((dense && jl < local) || e == b) continue;
-          const bool own = (jl == local);
-          const float sh[3] = {shx, shy, shz};
-          // the widened box in the neighbour cell's frame
-          // (no bound along periodic axes of one or two cells: a partner may
-          // sit across either face there, through the minimum image)
-          float wl[3], wh[3];
+    // --- neighbour cells, one per lane (lane = 9 (dz+1) + 3 (dy+1) + dx+1)
+    bool use = false, dense = false, own = false, single = false;
+    int64_t nb_b = 0, nb_e = 0, jcoord[3] = {0, 0, 0};
+    uint64_t jc = 0;
+    float sh[3] = {0.f, 0.f, 0.f};
+    if (lane < 27) {
+      const int off[3] = {lane % 3 - 1, (lane / 3) % 3 - 1, lane / 9 - 1};
+      use = true;
 #pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            if (((r.pdim >> d) & 1) && Nd[d] <= 2) {
-              wl[d] = -3e38f;
-              wh[d] = 3e38f;
-            } else {
-              wl[d] = __fsub_rn(__fadd_rn(bl[d], sh[d]), D.reach);
-              wh[d] = __fadd_rn(__fadd_rn(bh[d], sh[d]), D.reach);
-            }
-          }
-          // source ranges: one range for a plain cell, one per sub-cell row
-          // for a dense cell
-          int slo[3] = {0, 0, 0}, shi[3] = {0, 0, 0};
-          int gs0 = 1, gs1 = 1;
-          const uint32_t *tab = nullptr;
-          if (dense) {
-            tab = D.tab + (int64_t)D.rank[jc] * D.stride;
-            const SubGrid g = dense_sub(r, e - b);
-            gs0 = g.s[0];
-            gs1 = g.s[1];
-            const int64_t jcoord[3] = {jx, jy, jz};
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              const float clo = cell_lower(r, d, jcoord[d]);
-              slo[d] = sub_of(wl[d], clo, g.inv[d], g.s[d]);
-              shi[d] = sub_of(wh[d], clo, g.inv[d], g.s[d]);
-            }
-          }
-          for (int sz = slo[2]; sz <= shi[2]; ++sz)
-            for (int sy = slo[1]; sy <= shi[1]; ++sy) {
-              int64_t k0, k1;
-              if (dense) {
-                const int s0 = slo[0] + gs0 * (sy + gs1 * sz);
-                k0 = tab[s0];
-                k1 = tab[s0 + (shi[0] - slo[0]) + 1];
-              } else {
-                k0 = 0;
-                k1 = e - b;
-              }
-              for (int64_t base = k0; base < k1; base += 32) {
-                const int64_t t = base + lane;
-                float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
-                int q = -1;
-                bool cand = false;
-                if (t < k1) {
-                  if (dense) {
-                    o = D.dpos[b + t];
-                    q = __float_as_int(o.w);
-                  } else {
-                    o = pos[b + t];
-                    q = (int)(b + t);
-                  }
-                  cand = o.x >= wl[0] && o.x <= wh[0] && o.y >= wl[1] && o.y <= wh[1] && o.z >= wl[2] &&
-                         o.z <= wh[2];
-                }
-                unsigned mask = __ballot_sync(FULL, cand);
-                while (mask) {
-                  const int src = __ffs(mask) - 1;
-                  mask &= mask - 1;
-                  float4 so;
-                  so.x = __shfl_sync(FULL, o.x, src);
-                  so.y = __shfl_sync(FULL, o.y, src);
-                  so.z = __shfl_sync(FULL, o.z, src);
-                  so.w = 0.f;
-                  const int qs = __shfl_sync(FULL, q, src);
-                  if (valid && !(own && qs <= ip)) {
-                    const bool lk = per ? linked_pbc(me, so, P) : linked_open(me, so, P.rp2_open);
-                    if (lk) link_pair(parent, ip, qs, rp, flags);
-                  }
-                }
-              }
-            }
+      for (int d = 0; d < 3; ++d) {
+        if (off[d] < lo[d] || off[d] > hi[d]) use = false;
+        int64_t j = ixyz[d] + off[d];
+        if ((r.pdim >> d) & 1) {
+          if (j < 0) { j += Nd[d]; sh[d] = (float)P.L; } else if (j >= Nd[d]) { j -= Nd[d]; sh[d] = -(float)P.L; }
+        } else if (j < 0 || j >= Nd[d]) use = false;
+        jcoord[d] = j;
+      }
+      if (use) {
+        const int64_t jl = jcoord[0] + N0 * (jcoord[1] + N1 * jcoord[2]);
+        jc = r.cell_off + (uint64_t)jl;
+        nb_b = cell_start[jc];
+        nb_e = cell_start[jc + 1];
+        dense = nb_e - nb_b > DENSE_T;
+        // pairs with a lower dense cell are that cell's; pairs with sparse
+        // cells are all tested here
+        if ((dense && jl < local) || nb_e == nb_b) use = false;
+        own = jl == local;
+        if (use) {
+          const SubGrid g = dense ? dense_sub(r, nb_e - nb_b) : SubGrid{{1, 1, 1}, {0.f, 0.f, 0.f}};
+          single = g.s[0] * g.s[1] * g.s[2] == 1;
         }
       }
+    }
+    int rp = -1;  // cached root of this lane's particle
+    // --- cells that are one source range (sparse cells, dense cells of one
+    // sub-cell): their sources packed into shared batches of 32
+    {
+      const uint32_t cnt = (use && single) ? (uint32_t)(nb_e - nb_b) : 0u;
+      uint32_t incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const uint32_t excl = incl - cnt;
+      const uint32_t T = __shfl_sync(FULL, incl, 31);
+      for (uint32_t g0 = 0; g0 < T; g0 += 32) {
+        const uint32_t g = g0 + (uint32_t)lane;
+        int owner = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const uint32_t v = __shfl_sync(FULL, incl, owner + step - 1);
+          if (v <= g) owner += step;
+        }
+        owner &= 31;
+        const uint32_t ob = (uint32_t)__shfl_sync(FULL, (unsigned)nb_b, owner);
+        const uint32_t oex = __shfl_sync(FULL, excl, owner);
+        const bool od = __shfl_sync(FULL, (int)dense, owner) != 0;
+        const bool oown = __shfl_sync(FULL, (int)own, owner) != 0;
+        const float osh0 = __shfl_sync(FULL, sh[0], owner), osh1 = __shfl_sync(FULL, sh[1], owner),
+                    osh2 = __shfl_sync(FULL, sh[2], owner);
+        bool cand = false;
+        if (g < T) {
+          const uint32_t t = ob + (g - oex);
+          float4 o;
+          int q;
+          if (od) {
+            o = D.dpos[t];
+            q = __float_as_int(o.w);
+          } else {
+            o = pos[t];
+            q = (int)t;
+          }
+          const float osh[3] = {osh0, osh1, osh2};
+          const float oc[3] = {o.x, o.y, o.z};
+          cand = true;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            if (open_ax[d]) continue;
+            const float wl = __fsub_rn(__fadd_rn(bl[d], osh[d]), D.reach);
+            const float wh = __fadd_rn(__fadd_rn(bh[d], osh[d]), D.reach);
+            cand = cand && oc[d] >= wl && oc[d] <= wh;
+          }
+          o.w = __int_as_float(oown ? ~q : q);  // own-cell sources carry their flag
+          wbuf[lane] = o;
+        }
+        __syncwarp();
+        unsigned mask = __ballot_sync(FULL, cand);
+        while (mask) {
+          const int src = __ffs(mask) - 1;
+          mask &= mask - 1;
+          const float4 so = wbuf[src];
+          const int qw = __float_as_int(so.w);
+          const bool sown = qw < 0;
+          const int qs = sown ? ~qw : qw;
+          if (valid && !(sown && qs <= ip)) {
+            const bool lk = per ? linked_pbc(me, so, P) : linked_open(me, so, P.rp2_open);
+            if (lk) link_pair(parent, ip, qs, rp, flags);
+          }
+        }
+        __syncwarp();
+      }
+    }
+    // --- dense cells of several sub-cells: one after the other, a source
+    // range per sub-cell row the widened box overlaps
+    unsigned multi = __ballot_sync(FULL, use && !single);
+    while (multi) {
+      const int nl = __ffs(multi) - 1;
+      multi &= multi - 1;
+      const int64_t b = (int64_t)__shfl_sync(FULL, (unsigned long long)nb_b, nl);
+      const int64_t e = (int64_t)__shfl_sync(FULL, (unsigned long long)nb_e, nl);
+      const uint64_t jcn = __shfl_sync(FULL, (unsigned long long)jc, nl);
+      const bool own_n = __shfl_sync(FULL, (int)own, nl) != 0;
+      int64_t jcn3[3];
+      float wl[3], wh[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        jcn3[d] = (int64_t)__shfl_sync(FULL, (unsigned long long)jcoord[d], nl);
+        const float s = __shfl_sync(FULL, sh[d], nl);
+        if (open_ax[d]) {
+          wl[d] = -3e38f;
+          wh[d] = 3e38f;
+        } else {
+          wl[d] = __fsub_rn(__fadd_rn(bl[d], s), D.reach);
+          wh[d] = __fadd_rn(__fadd_rn(bh[d], s), D.reach);
+        }
+      }
+      const uint32_t *tab = D.tab + (int64_t)D.rank[jcn] * D.stride;
+      const SubGrid g = dense_sub(r, e - b);
+      int slo[3], shi[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float clo = cell_lower(r, d, jcn3[d]);
+        slo[d] = sub_of(wl[d], clo, g.inv[d], g.s[d]);
+        shi[d] = sub_of(wh[d], clo, g.inv[d], g.s[d]);
+      }
+      for (int sz = slo[2]; sz <= shi[2]; ++sz)
+        for (int sy = slo[1]; sy <= shi[1]; ++sy) {
+          const int s0 = slo[0] + g.s[0] * (sy + g.s[1] * sz);
+          const int64_t k0 = tab[s0], k1 = tab[s0 + (shi[0] - slo[0]) + 1];
+          for (int64_t base = k0; base < k1; base += 32) {
+            const int64_t t = base + lane;
+            float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+            int q = -1;
+            bool cand = false;
+            if (t < k1) {
+              o = D.dpos[b + t];
+              q = __float_as_int(o.w);
+              cand = o.x >= wl[0] && o.x <= wh[0] && o.y >= wl[1] && o.y <= wh[1] && o.z >= wl[2] &&
+                     o.z <= wh[2];
+            }
+            unsigned mask = __ballot_sync(FULL, cand);
+            while (mask) {
+              const int src = __ffs(mask) - 1;
+              mask &= mask - 1;
+              float4 so;
+              so.x = __shfl_sync(FULL, o.x, src);
+              so.y = __shfl_sync(FULL, o.y, src);
+              so.z = __shfl_sync(FULL, o.z, src);
+              so.w = 0.f;
+              const int qs = __shfl_sync(FULL, q, src);
+              if (valid && !(own_n && qs <= ip)) {
+                const bool lk = per ? linked_pbc(me, so, P) : linked_open(me, so, P.rp2_open);
+                if (lk) link_pair(parent, ip, qs, rp, flags);
+              }
+            }
+          }
+        }
     }
   }
 }
