@@ -456,7 +456,7 @@ struct DenseChunk {
   uint32_t cell, e0;  // dense cell (global cell index), first index in its dpos list
 };
 
-__global__ void __launch_bounds__(BLK, 2) fof_link_dense_kernel(
+__global__ void __launch_bounds__(BLK, 3) fof_link_dense_kernel(
     const float4 *__restrict__ pos, const uint32_t *__restrict__ prid, const RegionDev *__restrict__ R,
     const uint32_t *__restrict__ cell_start, int *parent, const DenseChunk *__restrict__ chunks,
     int64_t nchunks, LinkParams P, DenseIndex D, int32_t *flags) {
