@@ -54,7 +54,11 @@ int32_t pyfof_last_error(char *buf, int64_t len);
  * product path), "unbind_per_halo" (1 = the plain FP64 baseline: one halo per
  * launch sequence), "timing" (1 = record stage times), "unbind_big_np"
  * (particle-mesh halos above this many members run their removal loop
- * spread over the whole GPU; 0 = the default of 32768). */
+ * spread over the whole GPU; 0 = the default of 32768), "cell_order" (how
+ * the particles are put in cell order: 0 = per-cell sorts when cell keys
+ * need more than 24 bits and no cell holds more than 8192 particles, else a
+ * radix sort; 1 = per-cell sorts whenever no cell holds more than 8192; 2 =
+ * always the radix sort; all give the same order). */
 int32_t pyfof_set_option(const char *key, int64_t value);
 
 /* Issue all later work of the selected device on `stream` (a cudaStream_t;
@@ -66,6 +70,8 @@ int32_t pyfof_set_stream(void *stream);
  * the last call on the selected device "cells" (reference cell grid size),
  * "active" (particles in linked regions), "candidates" (FoF groups with at
  * least np_halo_min members), "dense_cells" (cells given a sub-cell index),
+ * "max_cell" (particles in the fullest cell), "cell_sorts" (1 when the
+ * cell order came from per-cell sorts, 0 from the radix sort),
  * "direct_halos" / "pm_halos" (candidates unbound by direct summation / the
  * particle mesh), "valid_halos" (halos written to the output),
  * "refined_regions" (two-level inner regions), "pm_solves" (halo-grid

@@ -23,6 +23,7 @@ int g_bound_fp64 = 0;
 int g_bound_per_halo = 0;
 int g_timing = 0;
 int64_t g_big_np = 0;
+int g_cell_order = 0;
 }  // namespace
 
 void set_error(const char *fmt, ...) {
@@ -184,6 +185,7 @@ static int32_t run_common(Context &ctx, FofArgs &a) {
   a.bound_fp64 = g_bound_fp64;
   a.bound_per_halo = g_bound_per_halo;
   a.big_np = g_big_np;
+  a.cell_order = g_cell_order;
   int32_t r = fof_run(ctx, a);
   note_alloc_failure(ctx, r);
   cudaError_t e = cudaStreamSynchronize(ctx.stream);
@@ -230,6 +232,14 @@ int32_t pyfof_set_option(const char *key, int64_t value) {
   if (!std::strcmp(key, "unbind_per_halo")) { g_bound_per_halo = value != 0; return kOk; }
   if (!std::strcmp(key, "timing")) { g_timing = value != 0; return kOk; }
   if (!std::strcmp(key, "unbind_big_np")) { g_big_np = value; return kOk; }
+  if (!std::strcmp(key, "cell_order")) {
+    if (value < 0 || value > 2) {
+      set_error("cell_order must be 0, 1 or 2");
+      return kInvalid;
+    }
+    g_cell_order = (int)value;
+    return kOk;
+  }
   set_error("unknown option %s", key);
   return kInvalid;
 }
@@ -250,6 +260,8 @@ static int32_t context_stat(const Context *c, const char *key, int64_t *value) {
   if (!std::strcmp(key, "active")) { *value = c->last_active; return kOk; }
   if (!std::strcmp(key, "candidates")) { *value = c->last_candidates; return kOk; }
   if (!std::strcmp(key, "dense_cells")) { *value = c->last_dense; return kOk; }
+  if (!std::strcmp(key, "max_cell")) { *value = c->last_max_cell; return kOk; }
+  if (!std::strcmp(key, "cell_sorts")) { *value = c->last_cell_sorts; return kOk; }
   if (!std::strcmp(key, "direct_halos")) { *value = c->last_direct; return kOk; }
   if (!std::strcmp(key, "pm_halos")) { *value = c->last_pm; return kOk; }
   if (!std::strcmp(key, "valid_halos")) { *value = c->last_valid; return kOk; }
@@ -394,6 +406,7 @@ static int32_t run_host(Context &ctx, const double *xp, const double *vp, const 
   a.bound_fp64 = g_bound_fp64;
   a.bound_per_halo = g_bound_per_halo;
   a.big_np = g_big_np;
+  a.cell_order = g_cell_order;
   int32_t r = fof_run(ctx, a);
   if (r == kOk && cat) r = build_catalogue(ctx, a.halo_id, (int64_t)n, cat->members, cat->offsets, cat->cap,
                                            cat->nfound);

@@ -76,6 +76,8 @@ struct Context {
   double last_pm_fft_bytes = 0.0;
   // statistics of the last call
   int64_t last_cells = 0, last_active = 0, last_candidates = 0, last_dense = 0;
+  int64_t last_max_cell = 0;    // particles in the fullest cell
+  int64_t last_cell_sorts = 0;  // 1: cell order by per-cell sorts, 0: by the radix sort
   int64_t last_direct = 0, last_pm = 0, last_valid = 0, last_tl_regions = 0;
   ~Context();
 };

@@ -7,7 +7,9 @@
 //   2. host               reference cell geometry per region (same formulas,
 //                         same libm pow) -> region table
 //   3. fof_key_kernel     global cell key per particle + cell histogram
-//   4. stable radix sort  (cell key, particle index): the reference CRS order
+//   4. stable cell order  (cell key, particle index): the reference CRS order,
+//                         by a scatter to per-cell slots and a sort of each
+//                         cell (a stable radix sort when a cell is large)
 //   5. fof_gather_kernel  FP32 sorted coordinates (real(x_rel,4))
 //   6. link kernels       pair tests over the reference's neighbour cells
 //                         (fof_link_dense_kernel for cells with more than
@@ -108,11 +110,15 @@ __global__ void __launch_bounds__(BLK) fof_key_kernel(Coords xp, const RegionDev
                                                       const Tile *__restrict__ T, double L,
                                                       double half, uint32_t sentinel,
                                                       uint32_t *__restrict__ keys,
-                                                      uint32_t *__restrict__ counts) {
+                                                      uint32_t *__restrict__ counts,
+                                                      uint32_t *__restrict__ rank) {
   const Tile t = T[blockIdx.x];
   const RegionDev &r = R[t.region];
   if (!r.active) {
-    for (int64_t i = t.begin + threadIdx.x; i < t.end; i += BLK) keys[i] = sentinel;
+    for (int64_t i = t.begin + threadIdx.x; i < t.end; i += BLK) {
+      keys[i] = sentinel;
+      rank[i] = atomicAdd(&counts[sentinel], 1u);
+    }
     return;
   }
   double anc[3];
@@ -124,7 +130,92 @@ __global__ void __launch_bounds__(BLK) fof_key_kernel(Coords xp, const RegionDev
       c[d] = cell_coord(unwrap(xp.get(i, d), anc[d], half, L), r.origin[d], r.size[d], r.N[d]);
     uint64_t key = r.cell_off + (uint64_t)(c[0] + (int64_t)r.N[0] * (c[1] + (int64_t)r.N[1] * c[2]));
     keys[i] = (uint32_t)key;
-    atomicAdd(&counts[key], 1u);
+    rank[i] = atomicAdd(&counts[key], 1u);  // a slot in the cell, in no particular order
+  }
+}
+
+// ---- cell order without a radix sort ---------------------------------------
+// The key kernel's counters give every particle a distinct slot in its
+// cell; scattering to cell start + slot groups the particles by cell, and
+// sorting each cell's original indices restores the stable order of the
+// reference's counting sort (ascending original index within a cell).
+
+__global__ void fof_max_count_kernel(const uint32_t *__restrict__ counts, int64_t ncell,
+                                     uint32_t *__restrict__ out) {
+  uint32_t m = 0;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (int64_t)gridDim.x * blockDim.x)
+    m = max(m, counts[c]);
+  m = __reduce_max_sync(0xffffffffu, m);
+  if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(out, m);
+}
+
+__global__ void fof_cell_scatter_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ rank,
+                                        const uint32_t *__restrict__ cstart, int64_t n,
+                                        uint32_t *__restrict__ skey, uint32_t *__restrict__ sidx) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = keys[i];
+    const uint32_t p = cstart[k] + rank[i];
+    skey[p] = k;
+    sidx[p] = (uint32_t)i;
+  }
+}
+
+constexpr int CELL_SORT_SMALL = 32;   // cells up to this size: one thread, insertion sort
+constexpr int CELL_SORT_MAX = 8192;   // cells up to this size: one block, bitonic sort
+
+__global__ void fof_cell_sort_small_kernel(const uint32_t *__restrict__ cstart, int64_t ncell,
+                                           uint32_t *__restrict__ sidx, uint32_t *__restrict__ big,
+                                           uint32_t *__restrict__ nbig) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t b = cstart[c], m = cstart[c + 1] - b;
+    if (m < 2) continue;
+    if (m > (uint32_t)CELL_SORT_SMALL) {
+      big[atomicAdd(nbig, 1u)] = (uint32_t)c;
+      continue;
+    }
+    uint32_t *a = sidx + b;
+    for (uint32_t i = 1; i < m; ++i) {
+      const uint32_t v = a[i];
+      uint32_t j = i;
+      while (j > 0 && a[j - 1] > v) {
+        a[j] = a[j - 1];
+        --j;
+      }
+      a[j] = v;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(1024) fof_cell_sort_big_kernel(const uint32_t *__restrict__ cstart,
+                                                               const uint32_t *__restrict__ big,
+                                                               const uint32_t *__restrict__ nbig,
+                                                               uint32_t *__restrict__ sidx) {
+  __shared__ uint32_t v[CELL_SORT_MAX];
+  const uint32_t nb = *nbig;
+  for (uint32_t j = blockIdx.x; j < nb; j += gridDim.x) {
+    const uint32_t c = big[j];
+    const uint32_t b = cstart[c], m = cstart[c + 1] - b;
+    uint32_t np2 = 1;
+    while (np2 < m) np2 <<= 1;
+    for (uint32_t i = threadIdx.x; i < np2; i += blockDim.x) v[i] = i < m ? sidx[b + i] : 0xffffffffu;
+    __syncthreads();
+    for (uint32_t k = 2; k <= np2; k <<= 1)
+      for (uint32_t h = k >> 1; h > 0; h >>= 1) {
+        for (uint32_t i = threadIdx.x; i < np2; i += blockDim.x) {
+          const uint32_t l = i ^ h;
+          if (l > i) {
+            const bool up = (i & k) == 0;
+            const uint32_t x = v[i], y = v[l];
+            if ((x > y) == up) {
+              v[i] = y;
+              v[l] = x;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) sidx[b + i] = v[i];
+    __syncthreads();
   }
 }
 
@@ -1094,15 +1185,56 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
                              cudaMemcpyHostToDevice, s));
   PYFOF_CUDA(cudaMemsetAsync(cstart, 0, sizeof(uint32_t) * (total_cells + 2), s));
   const uint32_t sentinel = (uint32_t)total_cells;
+  // slots within the cells go to va (radix scratch when the sort is needed)
   if (ntiles) {
-    fof_key_kernel<<<(unsigned)ntiles, BLK, 0, s>>>(xp, dR, dT, L, half, sentinel, keys, cstart);
+    fof_key_kernel<<<(unsigned)ntiles, BLK, 0, s>>>(xp, dR, dT, L, half, sentinel, keys, cstart, va);
     PYFOF_CHECK_LAUNCH();
   }
-  PYFOF_TRY(exclusive_scan_u32(cstart, cstart, (int64_t)total_cells + 1, nullptr, W, s));
-  uint32_t *skey, *sidx;
+  // Per-cell sorts pay off where the radix sort needs a fourth pass (keys of
+  // more than 24 bits) and every cell fits one block's sort; otherwise, and
+  // always with cell_order 2, a stable radix sort of all keys.
   const uint64_t max_key = (n_active < n) ? total_cells : (total_cells ? total_cells - 1 : 0);
-  PYFOF_TRY(radix_sort_pairs(keys, nullptr, n, bits_for(max_key), ka, va, kb, vb, &skey, &sidx,
-                             W, s));
+  const bool try_cells = a.cell_order == 1 || (a.cell_order == 0 && bits_for(max_key) > 24);
+  uint32_t *dmax = reinterpret_cast<uint32_t *>(ctx.d_flags + FLAG_COUNT_A);
+  PYFOF_CUDA(cudaMemsetAsync(dmax, 0, sizeof(uint32_t), s));
+  const unsigned cgrid0 = (unsigned)std::max<int64_t>(
+      1, std::min<int64_t>(ceil_div((int64_t)std::max<uint64_t>(total_cells, 1), (int64_t)BLK),
+                           (int64_t)kNumSMs * 16));
+  if (total_cells > 0) {
+    fof_max_count_kernel<<<cgrid0, BLK, 0, s>>>(cstart, (int64_t)total_cells, dmax);
+    PYFOF_CHECK_LAUNCH();
+  }
+  PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags + FLAG_COUNT_A, dmax, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  PYFOF_TRY(exclusive_scan_u32(cstart, cstart, (int64_t)total_cells + 1, nullptr, W, s));
+  PYFOF_CUDA(cudaStreamSynchronize(s));
+  const uint32_t max_occ = (uint32_t)ctx.h_flags[FLAG_COUNT_A];
+  ctx.last_max_cell = max_occ;
+  ctx.last_cell_sorts = 0;
+  uint32_t *skey, *sidx;
+  if (try_cells && max_occ <= (uint32_t)CELL_SORT_MAX) {
+    ctx.last_cell_sorts = 1;
+    // cells of more than CELL_SORT_SMALL particles: at most n / (CELL_SORT_SMALL + 1)
+    uint32_t *big = W.carve<uint32_t>(
+        (size_t)std::min<int64_t>(n_active / (CELL_SORT_SMALL + 1) + 1, (int64_t)total_cells + 1));
+    uint32_t *nbig = W.carve<uint32_t>(1);
+    if (!big || !nbig) { set_error("workspace exhausted (cell sort)"); return kAlloc; }
+    PYFOF_CUDA(cudaMemsetAsync(nbig, 0, sizeof(uint32_t), s));
+    const unsigned sgrid = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>(ceil_div(std::max<int64_t>(n, 1), (int64_t)BLK), (int64_t)kNumSMs * 16));
+    fof_cell_scatter_kernel<<<sgrid, BLK, 0, s>>>(keys, va, cstart, n, ka, vb);
+    PYFOF_CHECK_LAUNCH();
+    if (total_cells > 0) {
+      fof_cell_sort_small_kernel<<<cgrid0, BLK, 0, s>>>(cstart, (int64_t)total_cells, vb, big, nbig);
+      PYFOF_CHECK_LAUNCH();
+      fof_cell_sort_big_kernel<<<kNumSMs * 2, 1024, 0, s>>>(cstart, big, nbig, vb);
+      PYFOF_CHECK_LAUNCH();
+    }
+    skey = ka;
+    sidx = vb;
+  } else {
+    PYFOF_TRY(radix_sort_pairs(keys, nullptr, n, bits_for(max_key), ka, va, kb, vb, &skey, &sidx,
+                               W, s));
+  }
   // --- sorted FP32 coordinates, DSU
   float4 *pos = W.carve<float4>(std::max<int64_t>(n_active, 1));
   uint32_t *prid = W.carve<uint32_t>(std::max<int64_t>(n_active, 1));

@@ -24,6 +24,7 @@ struct FofArgs {
   int32_t bound_fp64 = 0;  // 1: plain FP64 unbinding path instead of the FP32 product path
   int32_t bound_per_halo = 0;  // 1: FP64, one halo per launch sequence (the plain baseline)
   int64_t big_np = 0;          // PM halos above this many members use the chunked removal loop (0: default)
+  int32_t cell_order = 0;      // 0: by key width, 1: per-cell sorts where cells allow, 2: radix sort
   // masses are divided by m_div right after their check (code units); only
   // with mp in the library's own scratch, which the check then rewrites
   double m_div = 1.0;

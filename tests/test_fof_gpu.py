@@ -108,6 +108,30 @@ def test_sparse_rows_with_dense_cells():
         _assert_same(g, o)
 
 
+@pytest.mark.parametrize("clump", [200, 3000, 12000])
+def test_cell_order_paths(clump):
+    """The stable cell order by per-cell sorts (cells up to 8192 particles,
+    small ones by insertion, larger ones by a block sort) and by the radix
+    sort (a fuller cell): the same partition and numbering as the oracle."""
+    rng = np.random.default_rng(clump)
+    back = rng.uniform(0, 40.0, (3, 60000))
+    cents = rng.uniform(0, 40.0, (3, 6))
+    clumps = [c[:, None] + rng.normal(0, 0.12, (3, clump)) for c in cents.T]
+    xp = np.mod(np.concatenate([back] + clumps, axis=1), 40.0)
+    o = oracle_core(xp, L_Box=40.0, linking_length=0.2, np_halo_min=10)
+    for mode in (1, 2, 0):
+        _native.set_option("cell_order", mode)
+        try:
+            g = P._fof_core(xp, L_Box=40.0, linking_length=0.2, np_halo_min=10)
+        finally:
+            _native.set_option("cell_order", 0)
+        m = _native.get_stat("max_cell")
+        assert (m > 8192) == (clump == 12000) and m > 32
+        # per-cell sorts only where asked for and every cell fits a block
+        assert _native.get_stat("cell_sorts") == (1 if (mode == 1 and m <= 8192) else 0)
+        _assert_same(g, o)
+
+
 def test_partially_periodic_filament():
     rng = np.random.default_rng(5)
     n = 6000
