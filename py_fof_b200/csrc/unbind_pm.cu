@@ -902,6 +902,27 @@ __device__ __forceinline__ int bsum_i(int v, int *red) {
   return t;
 }
 
+// Seven block sums at once: each value is reduced in the same order as by
+// bsum_d (warp butterfly, then the warp partials in warp order), so the
+// results are bit-identical, with 2 barriers instead of 21.
+__device__ __forceinline__ void bsum7_d(double *v, double *red) {
+  constexpr int NW = IBLK / 32;
+#pragma unroll
+  for (int j = 0; j < 7; ++j)
+    for (int o = 16; o > 0; o >>= 1) v[j] += __shfl_xor_sync(0xffffffffu, v[j], o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int j = 0; j < 7; ++j) red[j * NW + (threadIdx.x >> 5)] = v[j];
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < 7; ++j) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[j * NW + w];
+    v[j] = t;
+  }
+}
+
 // One block per pending halo: combine the potential, then the inner
 // removal loop of bound_check_grid (:2739-2855).  Leaves status -1 when the
 // potential must be refreshed (next pass).
@@ -919,7 +940,7 @@ __global__ void __launch_bounds__(IBLK) pm_inner_kernel(const Members m, PmHalo 
   const int h = list[blockIdx.x];
   PmHalo &p = H[h];
   if (!p.pending) return;
-  __shared__ double red_d[IBLK / 32];
+  __shared__ double red7[7 * (IBLK / 32)];
   __shared__ int red_i[IBLK / 32];
   __shared__ unsigned hist[256];
   __shared__ int s_err;
@@ -947,6 +968,8 @@ __global__ void __launch_bounds__(IBLK) pm_inner_kernel(const Members m, PmHalo 
   int deleted = 0, status = -1;
   for (;;) {
     double a7[7] = {0, 0, 0, 0, 0, 0, 0};
+    // top-digit histogram of the energies, filled by the energy sweep below
+    for (int t = threadIdx.x; t < 256; t += IBLK) hist[t] = 0;
     for (int64_t i = threadIdx.x; i < np; i += IBLK) {
       const int64_t k = b0 + i;
       if (!keep[k]) continue;
@@ -954,7 +977,7 @@ __global__ void __launch_bounds__(IBLK) pm_inner_kernel(const Members m, PmHalo 
       a7[0] += wi;
       for (int d = 0; d < 3; ++d) { a7[1 + d] += wi * (double)m.q[d][k]; a7[4 + d] += wi * (double)m.v[d][k]; }
     }
-    for (int j = 0; j < 7; ++j) a7[j] = bsum_d(a7[j], red_d);
+    bsum7_d(a7, red7);
     float qc[3], vc[3];
     for (int d = 0; d < 3; ++d) {
       qc[d] = __double2float_rn(a7[1 + d] / a7[0]);
@@ -973,6 +996,7 @@ __global__ void __launch_bounds__(IBLK) pm_inner_kernel(const Members m, PmHalo 
       if (!isfinite(e)) s_err = kInvalid;
       en[k] = e;
       nu += e >= 0.0f;
+      if (e >= 0.0f) atomicAdd(&hist[__float_as_uint(e + 0.0f) >> 24], 1u);
     }
     nu = bsum_i(nu, red_i);
     if (s_err) break;
@@ -985,25 +1009,30 @@ __global__ void __launch_bounds__(IBLK) pm_inner_kernel(const Members m, PmHalo 
     // radix select of the nb largest energies among the unbound members:
     // key = bits of (E + 0) (E >= 0, so the bits order like the values)
     unsigned prefix = 0, mask = 0;
-    int need = nb;
+    int need = nb, n_eq = 0;
     for (int shift = 24; shift >= 0; shift -= 8) {
-      for (int t = threadIdx.x; t < 256; t += IBLK) hist[t] = 0;
-      __syncthreads();
-      for (int64_t i = threadIdx.x; i < np; i += IBLK) {
-        const int64_t k = b0 + i;
-        if (!keep[k]) continue;
-        const float e = en[k];
-        if (!(e >= 0.0f)) continue;
-        const unsigned key = __float_as_uint(e + 0.0f);
-        if ((key & mask) != prefix) continue;
-        atomicAdd(&hist[(key >> shift) & 255u], 1u);
+      if (shift != 24) {  // the top digit's histogram came with the energies
+        for (int t = threadIdx.x; t < 256; t += IBLK) hist[t] = 0;
+        __syncthreads();
+        for (int64_t i = threadIdx.x; i < np; i += IBLK) {
+          const int64_t k = b0 + i;
+          if (!keep[k]) continue;
+          const float e = en[k];
+          if (!(e >= 0.0f)) continue;
+          const unsigned key = __float_as_uint(e + 0.0f);
+          if ((key & mask) != prefix) continue;
+          atomicAdd(&hist[(key >> shift) & 255u], 1u);
+        }
+        __syncthreads();
       }
-      __syncthreads();
       // digit holding the need-th largest key
       int digit = 255, above = 0;
       for (; digit >= 0; --digit) {
         const int c = (int)hist[digit];
-        if (above + c >= need) break;
+        if (above + c >= need) {
+          n_eq = c;  // at shift 0: the members whose key equals the threshold
+          break;
+        }
         above += c;
       }
       __syncthreads();
@@ -1014,8 +1043,21 @@ __global__ void __launch_bounds__(IBLK) pm_inner_kernel(const Members m, PmHalo 
     // delete every key > threshold and the `need` lowest indices among
     // key == threshold (equal energies: lower index first)
     const unsigned thr = prefix;
+    if (need == n_eq) {
+      // every member at the threshold goes: no index order needed
+      for (int64_t i = threadIdx.x; i < np; i += IBLK) {
+        const int64_t k = b0 + i;
+        if (!keep[k]) continue;
+        const float e = en[k];
+        if (e >= 0.0f && __float_as_uint(e + 0.0f) >= thr) {
+          keep[k] = 0;
+          jd[k] = 1;
+        }
+      }
+      __syncthreads();
+    }
     int taken_eq = 0;
-    for (int64_t base = 0; base < np; base += IBLK) {
+    for (int64_t base = 0; base < (need == n_eq ? 0 : np); base += IBLK) {
       const int64_t i = base + threadIdx.x;
       int64_t k = b0 + i;
       bool del_gt = false, is_eq = false;
