@@ -137,24 +137,60 @@ __global__ void ub_write_kernel(const uint32_t *__restrict__ mcand, const Member
   }
 }
 
+// Sums of K values over each run of equal keys among the lanes of a warp
+// (a segmented suffix scan over runs of consecutive lanes).  Returns true on
+// the first lane of a run, which then holds the run's sums.  All 32 lanes
+// must call it.
+template <int K>
+__device__ __forceinline__ bool warp_run_sums(uint32_t key, double (&v)[K]) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const uint32_t prev = __shfl_up_sync(FULL, key, 1);
+  const bool head = lane == 0 || prev != key;
+  const unsigned heads = __ballot_sync(FULL, head);
+  const int run = 31 - __clz(heads & (FULL >> (31 - lane)));  // the run's first lane
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int orun = __shfl_down_sync(FULL, run, o);
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      const double t = __shfl_down_sync(FULL, v[j], o);
+      if (lane + o < 32 && orun == run) v[j] += t;
+    }
+  }
+  return head;
+}
+
 // Angular momentum of the kept members of valid halos about their centre
-// (fof_fortran.f90:321-350), accumulated per candidate in two passes.
+// (fof_fortran.f90:321-350), accumulated per candidate in two passes.  A
+// candidate's members are consecutive, so each warp first sums its lanes per
+// candidate and adds those sums with one atomic per candidate and value
+// (summation order differs from the reference's serial loop; the tests
+// allow for that).
 __global__ void ub_com_kernel(Coords xp, Coords vp, const double *mp,
                               const uint32_t *__restrict__ mcand, const Members m,
                               const uint8_t *__restrict__ keep, const uint32_t *__restrict__ valid,
                               const int64_t *__restrict__ cand_anchor, int64_t M, double L,
                               double half, double *acc) {
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    const uint32_t c = mcand[k];
-    if (!valid[c] || !keep[k]) continue;
-    const int64_t i = m.pid[k], a = cand_anchor[c];
-    const double wi = mp ? mp[i] : 1.0;
-    atomicAdd(&acc[7 * (int64_t)c], wi);
-    for (int d = 0; d < 3; ++d) {
-      atomicAdd(&acc[7 * (int64_t)c + 1 + d], wi * unwrap(xp.get(i, d), xp.get(a, d), half, L));
-      atomicAdd(&acc[7 * (int64_t)c + 4 + d], wi * vp.get(i, d));
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < M; base += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = base + threadIdx.x;
+    uint32_t c = 0xffffffffu;
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // weight, 3 weighted positions, 3 weighted velocities, count
+    if (k < M) {
+      c = mcand[k];
+      if (valid[c] && keep[k]) {
+        const int64_t i = m.pid[k], a = cand_anchor[c];
+        const double wi = mp ? mp[i] : 1.0;
+        v[0] = wi;
+        for (int d = 0; d < 3; ++d) {
+          v[1 + d] = wi * unwrap(xp.get(i, d), xp.get(a, d), half, L);
+          v[4 + d] = wi * vp.get(i, d);
+        }
+        v[7] = 1.0;
+      }
     }
+    if (warp_run_sums<8>(c, v) && v[7] > 0.0)
+      for (int j = 0; j < 7; ++j) atomicAdd(&acc[7 * (int64_t)c + j], v[j]);
   }
 }
 
@@ -164,22 +200,29 @@ __global__ void ub_angmom_kernel(Coords xp, Coords vp, const double *mp,
                                  const uint32_t *__restrict__ valid,
                                  const int64_t *__restrict__ cand_anchor, const double *acc,
                                  int64_t M, double L, double half, double *am) {
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    const uint32_t c = mcand[k];
-    if (!valid[c] || !keep[k]) continue;
-    const double ws = acc[7 * (int64_t)c];
-    if (!(ws > 0.0)) continue;
-    const int64_t i = m.pid[k], a = cand_anchor[c];
-    const double wi = mp ? mp[i] : 1.0;
-    double dx[3], dv[3];
-    for (int d = 0; d < 3; ++d) {
-      dx[d] = unwrap(xp.get(i, d), xp.get(a, d), half, L) - acc[7 * (int64_t)c + 1 + d] / ws;
-      dv[d] = vp.get(i, d) - acc[7 * (int64_t)c + 4 + d] / ws;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < M; base += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = base + threadIdx.x;
+    uint32_t c = 0xffffffffu;
+    double v[4] = {0, 0, 0, 0};  // angular momentum, count
+    if (k < M) {
+      c = mcand[k];
+      const double ws = valid[c] && keep[k] ? acc[7 * (int64_t)c] : 0.0;
+      if (ws > 0.0) {
+        const int64_t i = m.pid[k], a = cand_anchor[c];
+        const double wi = mp ? mp[i] : 1.0;
+        double dx[3], dv[3];
+        for (int d = 0; d < 3; ++d) {
+          dx[d] = unwrap(xp.get(i, d), xp.get(a, d), half, L) - acc[7 * (int64_t)c + 1 + d] / ws;
+          dv[d] = vp.get(i, d) - acc[7 * (int64_t)c + 4 + d] / ws;
+        }
+        v[0] = wi * (dx[1] * dv[2] - dx[2] * dv[1]);
+        v[1] = wi * (dx[2] * dv[0] - dx[0] * dv[2]);
+        v[2] = wi * (dx[0] * dv[1] - dx[1] * dv[0]);
+        v[3] = 1.0;
+      }
     }
-    atomicAdd(&am[3 * (int64_t)c + 0], wi * (dx[1] * dv[2] - dx[2] * dv[1]));
-    atomicAdd(&am[3 * (int64_t)c + 1], wi * (dx[2] * dv[0] - dx[0] * dv[2]));
-    atomicAdd(&am[3 * (int64_t)c + 2], wi * (dx[0] * dv[1] - dx[1] * dv[0]));
+    if (warp_run_sums<4>(c, v) && v[3] > 0.0)
+      for (int j = 0; j < 3; ++j) atomicAdd(&am[3 * (int64_t)c + j], v[j]);
   }
 }
 
