@@ -526,62 +526,87 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) sr_gather_kernel(
     const bool tl = p.two_level != 0;
     const DepthConst k_eps = depth_const((float)eps), k_ai = depth_const((float)ai);
     R acc = 0, comp = 0;
-    for (int64_t z = cz - kk; z <= cz + kk; ++z) {
-      if (z < 0 || z >= n2) continue;
-      for (int64_t y = cy - kk; y <= cy + kk; ++y) {
-        if (y < 0 || y >= n1) continue;
-        for (int64_t x = cx - kk; x <= cx + kk; ++x) {
-          if (x < 0 || x >= n0) continue;
+    // The (2kk+1)^3 neighbour cells, 32 at a time: a lane loads one cell's
+    // source range, the ranges are concatenated by a warp prefix sum and
+    // streamed in batches of 32 (a lane finds its source's cell by a binary
+    // search over the prefix), so small cells share batches.
+    const int wd = 2 * kk + 1, ncell = wd * wd * wd;
+    for (int cb0 = 0; cb0 < ncell; cb0 += 32) {
+      const int j = cb0 + lane;
+      uint32_t s0 = 0, cnt = 0;
+      if (j < ncell) {
+        const int64_t x = cx + j % wd - kk, y = cy + (j / wd) % wd - kk, z = cz + j / (wd * wd) - kk;
+        if (x >= 0 && x < n0 && y >= 0 && y < n1 && z >= 0 && z < n2) {
           const int64_t c = p.cell_off + x + n0 * (y + n1 * z);
-          uint32_t s0 = cstart[c], s1 = cstart[c + 1];
+          uint32_t a = cstart[c], b = cstart[c + 1];
           if (UPDATE) {
-            s0 = rpos[s0];
-            s1 = rpos[s1];
+            a = rpos[a];
+            b = rpos[b];
           }
-          for (uint32_t base = s0; base < s1; base += 32) {
-            const uint32_t t = base + lane;
-            uint32_t se = 0;
-            float4 sv = make_float4(0.f, 0.f, 0.f, 0.f);
-            bool cand = false;
-            if (t < s1) {
-              se = UPDATE ? rsrc[t] : t;
-              sv = src4[se];
-              cand = UPDATE || keep[cmem[se]] != 0;
-              const float bx = fmaxf(fmaxf(lo[0] - sv.x, sv.x - hi[0]), 0.f);
-              const float by = fmaxf(fmaxf(lo[1] - sv.y, sv.y - hi[1]), 0.f);
-              const float bz = fmaxf(fmaxf(lo[2] - sv.z, sv.z - hi[2]), 0.f);
-              cand = cand && (bx * bx + by * by + bz * bz <= amax2);
+          s0 = a;
+          cnt = b - a;
+        }
+      }
+      uint32_t incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const uint32_t excl = incl - cnt;
+      const uint32_t T = __shfl_sync(FULL, incl, 31);
+      for (uint32_t g0 = 0; g0 < T; g0 += 32) {
+        const uint32_t g = g0 + (uint32_t)lane;
+        int owner = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const uint32_t v = __shfl_sync(FULL, incl, owner + step - 1);
+          if (v <= g) owner += step;
+        }
+        owner &= 31;
+        const uint32_t os0 = __shfl_sync(FULL, s0, owner);
+        const uint32_t oex = __shfl_sync(FULL, excl, owner);
+        uint32_t se = 0;
+        float4 sv = make_float4(0.f, 0.f, 0.f, 0.f);
+        bool cand = false;
+        if (g < T) {
+          const uint32_t t = os0 + (g - oex);
+          se = UPDATE ? rsrc[t] : t;
+          sv = src4[se];
+          cand = UPDATE || keep[cmem[se]] != 0;
+          const float bx = fmaxf(fmaxf(lo[0] - sv.x, sv.x - hi[0]), 0.f);
+          const float by = fmaxf(fmaxf(lo[1] - sv.y, sv.y - hi[1]), 0.f);
+          const float bz = fmaxf(fmaxf(lo[2] - sv.z, sv.z - hi[2]), 0.f);
+          cand = cand && (bx * bx + by * by + bz * bz <= amax2);
+        }
+        unsigned mask = __ballot_sync(FULL, cand);
+        while (mask) {
+          const int bl = __ffs(mask) - 1;
+          mask &= mask - 1;
+          const float jx = __shfl_sync(FULL, sv.x, bl), jy = __shfl_sync(FULL, sv.y, bl);
+          const float jz = __shfl_sync(FULL, sv.z, bl), jw = __shfl_sync(FULL, sv.w, bl);
+          const uint32_t je = __shfl_sync(FULL, se, bl);
+          if (active && je != e) {
+            R dx, dy, dz;
+            if (tl) {
+              dx = (R)jx - (R)me.x; dy = (R)jy - (R)me.y; dz = (R)jz - (R)me.z;
+            } else {
+              dx = (R)__fsub_rn(jx, me.x); dy = (R)__fsub_rn(jy, me.y); dz = (R)__fsub_rn(jz, me.z);
             }
-            unsigned mask = __ballot_sync(FULL, cand);
-            while (mask) {
-              const int bl = __ffs(mask) - 1;
-              mask &= mask - 1;
-              const float jx = __shfl_sync(FULL, sv.x, bl), jy = __shfl_sync(FULL, sv.y, bl);
-              const float jz = __shfl_sync(FULL, sv.z, bl), jw = __shfl_sync(FULL, sv.w, bl);
-              const uint32_t je = __shfl_sync(FULL, se, bl);
-              if (active && je != e) {
-                R dx, dy, dz;
-                if (tl) {
-                  dx = (R)jx - (R)me.x; dy = (R)jy - (R)me.y; dz = (R)jz - (R)me.z;
-                } else {
-                  dx = (R)__fsub_rn(jx, me.x); dy = (R)__fsub_rn(jy, me.y); dz = (R)__fsub_rn(jz, me.z);
-                }
-                const R r2 = dx * dx + dy * dy + dz * dz;
-                if (r2 < a2) {
-                  R dphi;
-                  if constexpr (sizeof(R) == 4) {
-                    const float rinv = rsqrtf(r2), d = r2 * rinv;
-                    dphi = -(fac * (depth_fast(d, rinv, k_eps) - depth_fast(d, rinv, k_ai)));
-                  } else {
-                    const R d = sqrt(r2);
-                    dphi = -(fac * (depth_c<R>(d, eps) - depth_c<R>(d, ai)));
-                  }
-                  const R yv = (R)jw * dphi - comp;
-                  const R tt = acc + yv;
-                  comp = (tt - acc) - yv;
-                  acc = tt;
-                }
+            const R r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 < a2) {
+              R dphi;
+              if constexpr (sizeof(R) == 4) {
+                const float rinv = rsqrtf(r2), d = r2 * rinv;
+                dphi = -(fac * (depth_fast(d, rinv, k_eps) - depth_fast(d, rinv, k_ai)));
+              } else {
+                const R d = sqrt(r2);
+                dphi = -(fac * (depth_c<R>(d, eps) - depth_c<R>(d, ai)));
               }
+              const R yv = (R)jw * dphi - comp;
+              const R tt = acc + yv;
+              comp = (tt - acc) - yv;
+              acc = tt;
             }
           }
         }
