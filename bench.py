@@ -461,10 +461,11 @@ def run_b200(args):
                                            "padded grid per transform, two transforms)",
                       "solves_per_call": counts["pm_solves"]}
     else:
-        kname = "fof_link_kernel"
+        kname = "fof_link"
         k_ms = mean(st, "link")
         k_bytes = LINK_BYTES_PER_PARTICLE * n + LINK_BYTES_PER_CELL * _native.get_stat("cells")
-        roof_extra = {"algorithmic_bytes": "20 B per particle + 4 B per cell"}
+        roof_extra = {"kernels": "fof_link_dense_kernel + fof_link_kernel (one link stage)",
+                      "algorithmic_bytes": "20 B per particle + 4 B per cell"}
     achieved = k_bytes / (k_ms * 1e-3) / 1e9 if k_ms > 0 else None
     ratio = _traffic(args.workload, kname)
     traffic = ratio * k_bytes if ratio is not None else None

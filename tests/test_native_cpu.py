@@ -101,6 +101,18 @@ def test_device_units_carry_the_host_conversion(mass, units):
     assert all(x.dtype == y.dtype and np.array_equal(x, y) for x, y in zip(dev.dense(), host.dense()))
 
 
+def test_options_validated():
+    """Options are plain settings of the library (no device work): accepted
+    values stick, others are refused with the library's message."""
+    from py_fof_b200 import _native
+    _native.set_option("cell_order", 1)
+    _native.set_option("cell_order", 0)
+    with pytest.raises(ValueError, match="cell_order"):
+        _native.set_option("cell_order", 3)
+    with pytest.raises(ValueError, match="unknown option"):
+        _native.set_option("no_such_option", 1)
+
+
 def test_catalogue_from_ids():
     hid = np.array([0, 2, 1, 2, 0, 1, 3], np.int32)
     res = P.catalogue_from_ids(hid > 0, hid)
