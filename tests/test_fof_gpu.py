@@ -267,3 +267,11 @@ def test_lognormal_field_partition(seed):
     assert o[1].max() > 20
     assert np.array_equal(g[0], o[0])
     assert np.array_equal(g[1], o[1])
+    # the cell order by per-cell sorts (the path of the largest boxes)
+    _native.set_option("cell_order", 1)
+    try:
+        g1 = P._fof_core(x, **kw)
+    finally:
+        _native.set_option("cell_order", 0)
+    assert _native.get_stat("cell_sorts") == 1
+    assert np.array_equal(g1[0], o[0]) and np.array_equal(g1[1], o[1])
