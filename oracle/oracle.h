@@ -28,6 +28,21 @@ int32_t oracle_fof_fortran(const double *xp, const double *vp, const double *mp,
                            int32_t n_threads, int64_t ng_val, double ng_global_val,
                            int32_t *in_halo, int32_t *halo_id, double *ang_mom);
 
+/* oracle_fof_fortran plus diagnostics of the unbinding (both may be NULL):
+ * energy[i] = the specific energy of candidate member i at its last
+ * evaluation in the removal loop (kept: the final one; removed: the one that
+ * removed it), phi_scale[i] = max |phi| of its candidate's first-pass
+ * potential; NaN for particles of no candidate.  The tests bound the
+ * energies of members the GPU classifies differently with them. */
+int32_t oracle_fof_fortran_diag(const double *xp, const double *vp, const double *mp,
+                                const int32_t *np_halo, int32_t nhalo, int64_t total_np,
+                                double L_Box, double link, int32_t np_halo_min,
+                                int32_t bound_check, int32_t verbose, double softening,
+                                double a_val, double b_val, double s15_val,
+                                int32_t n_threads, int64_t ng_val, double ng_global_val,
+                                int32_t *in_halo, int32_t *halo_id, double *ang_mom,
+                                float *energy, float *phi_scale);
+
 /* Thread count actually used by the last oracle_fof_fortran call. */
 int32_t oracle_last_threads(void);
 
@@ -48,6 +63,18 @@ int32_t oracle_bound_batch(const float *xv, const float *mp, const int64_t *pid,
                            int64_t ng_val, double ng_global_val,
                            int32_t *np_bound, int32_t *status, int32_t *final_members,
                            float *phi_out, int32_t *method_out);
+
+/* oracle_bound_batch plus diagnostics (both may be NULL): energy_tab[k] =
+ * the last specific energy of the member at table position k, phimax[h] =
+ * max |phi| of candidate h's first-pass potential. */
+int32_t oracle_bound_batch_diag(const float *xv, const float *mp, const int64_t *pid,
+                                const int32_t *cand_np, int32_t ncand,
+                                double softening, double a_val, double b_val, double s15,
+                                int32_t np_halo_min, int32_t verbose, int32_t n_threads,
+                                int64_t ng_val, double ng_global_val,
+                                int32_t *np_bound, int32_t *status, int32_t *final_members,
+                                float *phi_out, int32_t *method_out, float *energy_tab,
+                                float *phimax);
 
 /* First-pass potential of one candidate with the reference solver selected by
  * the reference rules (direct FP64 sum or PM+C2), members in pid order;

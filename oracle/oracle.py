@@ -46,6 +46,8 @@ def lib():
             ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
             ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
             ctypes.c_int32, ctypes.c_int64, ctypes.c_double, _i32p, _i32p, _dp]
+        L.oracle_fof_fortran_diag.restype = ctypes.c_int32
+        L.oracle_fof_fortran_diag.argtypes = L.oracle_fof_fortran.argtypes + [_fp, _fp]
         L.oracle_last_threads.restype = ctypes.c_int32
         L.oracle_bound_batch.restype = ctypes.c_int32
         L.oracle_bound_batch.argtypes = [
@@ -74,8 +76,14 @@ def _p(a, t):
 
 def fof_fortran(xp_halo, vp_halo, mp_halo, np_halo, nhalo, L_Box, linking_length,
                 np_halo_min, bound_check, verbose, softening, a_val, b_val, s_15_val,
-                n_threads, total_np, ng_val=256, ng_global_val=512.0):
-    """Oracle counterpart of the f2py entry ``fof_fortran.fof_fortran``."""
+                n_threads, total_np, ng_val=256, ng_global_val=512.0, diag=False):
+    """Oracle counterpart of the f2py entry ``fof_fortran.fof_fortran``.
+
+    With ``diag=True`` it also returns the unbinding diagnostics
+    ``energy`` (each candidate member's specific energy at its last
+    evaluation in the removal loop) and ``phi_scale`` (max |phi| of its
+    candidate's first-pass potential), float32 per particle, NaN outside
+    candidates."""
     xp = np.asfortranarray(xp_halo, dtype=np.float64)
     vp = np.asfortranarray(vp_halo, dtype=np.float64)
     mp = np.ascontiguousarray(mp_halo, dtype=np.float64)
@@ -84,13 +92,18 @@ def fof_fortran(xp_halo, vp_halo, mp_halo, np_halo, nhalo, L_Box, linking_length
     in_halo = np.zeros(n, dtype=np.int32)
     halo_id = np.zeros(n, dtype=np.int32)
     ang_mom = np.zeros((3, max(int(nhalo), 0)), dtype=np.float64, order="F")
-    ierr = lib().oracle_fof_fortran(
-        _p(xp, _dp), _p(vp, _dp), _p(mp, _dp), _p(nph, _i32p), int(nhalo), n,
-        float(L_Box), float(linking_length), int(np_halo_min), int(bound_check), int(verbose),
-        float(softening), float(a_val), float(b_val), float(s_15_val), int(n_threads),
-        int(ng_val), float(ng_global_val), _p(in_halo, _i32p), _p(halo_id, _i32p),
-        _p(ang_mom, _dp))
-    return in_halo, halo_id, ang_mom, int(ierr)
+    args = [_p(xp, _dp), _p(vp, _dp), _p(mp, _dp), _p(nph, _i32p), int(nhalo), n,
+            float(L_Box), float(linking_length), int(np_halo_min), int(bound_check), int(verbose),
+            float(softening), float(a_val), float(b_val), float(s_15_val), int(n_threads),
+            int(ng_val), float(ng_global_val), _p(in_halo, _i32p), _p(halo_id, _i32p),
+            _p(ang_mom, _dp)]
+    if not diag:
+        ierr = lib().oracle_fof_fortran(*args)
+        return in_halo, halo_id, ang_mom, int(ierr)
+    energy = np.zeros(n, np.float32)
+    phi_scale = np.zeros(n, np.float32)
+    ierr = lib().oracle_fof_fortran_diag(*args, _p(energy, _fp), _p(phi_scale, _fp))
+    return in_halo, halo_id, ang_mom, int(ierr), energy, phi_scale
 
 
 def last_threads() -> int:

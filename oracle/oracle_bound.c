@@ -1000,7 +1000,8 @@ static int cmp_energy(const void *a, const void *b, void *ctx)
  * candidate (table order); returns ierr, fills status/np_bound/keep/member. */
 static int check_grid(const bctx *c, const htask *tk, const float *xv, const float *mp,
                       const int64_t *pid, int32_t *member, int np, int *status_out,
-                      int *np_bound_out, char *keep, float *phi_out, int phi_only)
+                      int *np_bound_out, char *keep, float *phi_out, int phi_only,
+                      float *energy_tab, float *phimax_out)
 {
     const double a = c->a;
     const int nmin = c->np_min;
@@ -1152,6 +1153,11 @@ static int check_grid(const bctx *c, const htask *tk, const float *xv, const flo
             if (np_bound == 1 || n_source == 1) phi[i] = 0.0f;
             if (!isfinite(phi[i])) { ierr = 4; goto out; }
         }
+        if (pass == 1 && phimax_out) {
+            float m = 0.0f;
+            for (int i = 0; i < np; ++i) if (keep[i] && fabsf(phi[i]) > m) m = fabsf(phi[i]);
+            *phimax_out = m;
+        }
         if (phi_only) { *status_out = 0; goto done; }
         int deleted = 0;
         for (;;) {
@@ -1206,6 +1212,10 @@ done:
     *np_bound_out = np_bound;
     if (phi_out)
         for (int i = 0; i < np; ++i) phi_out[i] = phi[i];
+    /* diagnostics for the tests' energy band: each member's specific energy
+     * at its last evaluation (the final one if kept, at removal otherwise) */
+    if (energy_tab)
+        for (int i = 0; i < np; ++i) energy_tab[member[i]] = energy[i];
 out:
     free(q); free(w); free(phi); free(energy); free(phid); free(order); free(jdel);
     free(selfp); free(wt); free(first); free(phi_c1); free(phi_c2); free(phi_in);
@@ -1257,6 +1267,20 @@ int32_t oracle_bound_batch(const float *xv, const float *mp, const int64_t *pid,
                            double ng_global_val, int32_t *np_bound, int32_t *status,
                            int32_t *final_members, float *phi_out, int32_t *method_out)
 {
+    return oracle_bound_batch_diag(xv, mp, pid, cand_np, ncand, softening, a_val, b_val, s15,
+                                   np_halo_min, verbose, n_threads, ng_val, ng_global_val,
+                                   np_bound, status, final_members, phi_out, method_out, NULL,
+                                   NULL);
+}
+
+int32_t oracle_bound_batch_diag(const float *xv, const float *mp, const int64_t *pid,
+                                const int32_t *cand_np, int32_t ncand, double softening,
+                                double a_val, double b_val, double s15, int32_t np_halo_min,
+                                int32_t verbose, int32_t n_threads, int64_t ng_val,
+                                double ng_global_val, int32_t *np_bound, int32_t *status,
+                                int32_t *final_members, float *phi_out, int32_t *method_out,
+                                float *energy_tab, float *phimax)
+{
     bctx c;
     ctx_init(&c, softening, a_val, b_val, s15, np_halo_min, verbose, ng_val, ng_global_val);
     int64_t *off = (int64_t *)malloc(sizeof(int64_t) * ((size_t)ncand + 1));
@@ -1294,7 +1318,8 @@ int32_t oracle_bound_batch(const float *xv, const float *mp, const int64_t *pid,
             for (int i = 0; i < np; ++i) member[i] = (int32_t)(off[h] + i);
             int st = -1, nb = 0;
             e = check_grid(&c, &tasks[h], xv, mp, pid, member, np, &st, &nb, keep,
-                           phi_out ? phi_out + off[h] : NULL, 0);
+                           phi_out ? phi_out + off[h] : NULL, 0, energy_tab,
+                           phimax ? phimax + h : NULL);
             if (e) {
 #pragma omp critical(oracle_bound_err)
                 if (!ierr) ierr = e;
@@ -1329,7 +1354,7 @@ int32_t oracle_bound_first_potential(const float *xv, const float *mp, const int
     char *keep = (char *)malloc((size_t)np);
     for (int i = 0; i < np; ++i) member[i] = i;
     int st, nb;
-    e = check_grid(&c, &t, xv, mp, pid, member, np, &st, &nb, keep, phi, 1);
+    e = check_grid(&c, &t, xv, mp, pid, member, np, &st, &nb, keep, phi, 1, NULL, NULL);
     free(member); free(keep);
     return e ? -e : t.gid;
 }

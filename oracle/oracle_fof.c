@@ -420,6 +420,23 @@ int32_t oracle_fof_fortran(const double *xp, const double *vp, const double *mp,
                            int32_t n_threads, int64_t ng_val, double ng_global_val,
                            int32_t *in_halo, int32_t *halo_id, double *ang_mom)
 {
+    return oracle_fof_fortran_diag(xp, vp, mp, np_halo, nhalo, total_np, L_Box, link,
+                                   np_halo_min, bound_check, verbose, softening, a_val, b_val,
+                                   s15_val, n_threads, ng_val, ng_global_val, in_halo, halo_id,
+                                   ang_mom, NULL, NULL);
+}
+
+int32_t oracle_fof_fortran_diag(const double *xp, const double *vp, const double *mp,
+                                const int32_t *np_halo, int32_t nhalo, int64_t total_np,
+                                double L_Box, double link, int32_t np_halo_min,
+                                int32_t bound_check, int32_t verbose, double softening,
+                                double a_val, double b_val, double s15_val,
+                                int32_t n_threads, int64_t ng_val, double ng_global_val,
+                                int32_t *in_halo, int32_t *halo_id, double *ang_mom,
+                                float *energy, float *phi_scale)
+{
+    if (energy)
+        for (int64_t i = 0; i < total_np; ++i) { energy[i] = NAN; phi_scale[i] = NAN; }
     for (int64_t i = 0; i < total_np; ++i) { in_halo[i] = 0; halo_id[i] = 0; }
     for (int64_t i = 0; i < 3 * (int64_t)(nhalo > 0 ? nhalo : 0); ++i) ang_mom[i] = 0.0;
     if (n_threads > 256) return 10;
@@ -518,9 +535,23 @@ int32_t oracle_fof_fortran(const double *xp, const double *vp, const double *mp,
                     }
                     off += cnp[c];
                 }
-            ierr = oracle_bound_batch(xv, mpf, pid, cnp, (int32_t)ncand, softening, a_val, b_val,
-                                      s15_val, np_halo_min, verbose, T, ng_val, ng_global_val,
-                                      nb, st, fm, NULL, NULL);
+            float *etab = energy ? (float *)malloc(sizeof(float) * (size_t)ntot) : NULL;
+            float *pmax = energy ? (float *)calloc((size_t)ncand, sizeof(float)) : NULL;
+            ierr = oracle_bound_batch_diag(xv, mpf, pid, cnp, (int32_t)ncand, softening, a_val,
+                                           b_val, s15_val, np_halo_min, verbose, T, ng_val,
+                                           ng_global_val, nb, st, fm, NULL, NULL, etab, pmax);
+            if (ierr == 0 && etab && pmax) {
+                int64_t o2 = 0;
+                for (int64_t cc = 0; cc < ncand; ++cc) {
+                    for (int32_t k = 0; k < cnp[cc]; ++k) {
+                        energy[pid[o2 + k] - 1] = etab[o2 + k];
+                        phi_scale[pid[o2 + k] - 1] = pmax[cc];
+                    }
+                    o2 += cnp[cc];
+                }
+            }
+            free(etab);
+            free(pmax);
             if (ierr == 0) {
                 int32_t valid = 0;
                 off = 0;
