@@ -15,22 +15,28 @@ background sigma 1; link 0.2, np_halo_min 10, s_15 = 15 * 0.67 * 256 / 300.
 
 * value: particles per second (Mpart/s) of the whole call (binning, linking,
   labelling, candidate packing, unbinding of every candidate, outputs) with
-  the inputs resident in HBM, on the library's default FP32 unbinding path,
+  the inputs resident in HBM, on the library's default FP64 unbinding path
+  (the plain FP64 GPU path the FoF + unbinding configuration names),
   device-timed with CUDA events on the stream the library launches on.
   All ranks run their own replica (one periodic box is one region, which
   this path does not split): value = N * particles / max-over-ranks time.
 * unbind: candidates unbound per second of unbinding stage time for the
-  batched FP32 path, the batched FP64 path and the plain per-halo FP64 path
-  (one halo per launch sequence), each on the same input.
+  batched FP64 path (the value's), the batched FP32 product path and the
+  plain per-halo FP64 path (one halo per launch sequence), each on the same
+  input.
 * e2e: the same metric through the public API ``py_fof_b200.fof`` with
   pinned host inputs, host<->device copies inside the timed region.
 * roofline: the dominant kernel group.  With unbinding: the particle-mesh
-  convolutions (the FFT kernels), algorithmic bytes 16 (n+2) n^2 per solve
-  on an n^3 grid over their event-timed device time.  Plain FoF: the linking
-  kernel, 20 B per particle + 4 B per cell.
-* cpu_baseline: the CPU restatement of the reference (oracle/, OpenMP) on
-  this host, on a bounded sample of the workload (a sub-volume with the same
-  recipe and density).
+  convolutions (the FFT kernels), algorithmic bytes 4 s (n+2) n^2 per solve
+  on an n^3 grid of s-byte reals over their event-timed device time.  Plain
+  FoF: the linking kernels, 20 B per particle + 4 B per cell.
+  roofline_fof_link: the linking kernels on every workload.
+* cpu_baseline: the CPU restatement of the reference (oracle/, OpenMP, the
+  reference's thread policy) on this host: one full call of the workload
+  after one untimed call on a sub-volume (which builds the Green tables),
+  or, for workloads too large for one call in 30 s, a stated sample.
+* --impl reference: the same restatement on the same workload, every timed
+  step one full call; the untimed warm-up steps run on the sub-volume.
 Under torchrun (N > 1) rank 0 prints the single JSON line.
 """
 from __future__ import annotations
@@ -65,9 +71,11 @@ WORKLOADS = {
     "fof_lognormal_256": ("lognormal", 256, 128),
     "fof_lognormal_128": ("lognormal", 128, 64),
 }
-# CPU sample of each workload: a sub-volume with the same recipe and density,
-# or the first halos of the same list
-CPU_SAMPLE = {
+# Warm-up input of the CPU arms (a sub-volume with the same recipe and
+# density, or the first halos of the same list), and the CPU sample of the
+# workloads too large for full CPU calls within the bench's time (None: the
+# timed CPU calls run the workload itself)
+CPU_WARMUP = {
     "fof_unbind_256": "fof_unbind_128",
     "fof_unbind_128": "fof_unbind_128",
     "fof_256": "fof_64",
@@ -79,6 +87,11 @@ CPU_SAMPLE = {
     "fof_lognormal_512": "fof_lognormal_128",
     "fof_lognormal_256": "fof_lognormal_128",
     "fof_lognormal_128": "fof_lognormal_128",
+}
+CPU_SAMPLE = {
+    "unbind_nfw_20k": "unbind_nfw_20k:2000",
+    "fof_lognormal_1024": "fof_lognormal_512",
+    "fof_lognormal_512": "fof_lognormal_256",
 }
 LINK = 0.2
 NP_MIN = 10
@@ -199,6 +212,20 @@ def make_workload(name, seed=0, device=None):
                 on_device=False)
 
 
+def _config(workload, wl, n_job, world, scaling):
+    """The config dict both arms print for one workload (the reference arm
+    with world = 1)."""
+    n = wl["xp"].shape[1]
+    in_bytes = 24 * n + (24 * n if wl["vp"] is not None else 0) + (8 * n if wl["mp"] is not None else 0)
+    l2 = (f"inputs larger than L2 ({in_bytes / 1e6:.0f} MB of positions, velocities and masses "
+          "> 126 MB), no flush") if in_bytes > 126e6 else "inputs smaller than L2"
+    return {"workload": workload, "particles": n_job if scaling == "strong" else n,
+            "L_Box": wl["L"], "link": LINK, "np_halo_min": wl["np_min"], "bound_check": wl["bound"],
+            "softening": SOFTENING, "s_15": wl["s15"], "regions": len(wl["np_halo"]),
+            "unbinding": "fp64" if wl["bound"] else None, "l2": l2,
+            "parallelism": (f"regions sharded x{world}" if scaling == "strong" else f"replicas x{world}")}
+
+
 def cpu_port_run(wl, threads):
     """One call of the CPU restatement (oracle/) on the workload."""
     from oracle import oracle as O
@@ -217,44 +244,50 @@ def cpu_port_run(wl, threads):
 
 
 def _sample_kind(name, workload):
+    if name == workload:
+        return f"the {workload} workload itself"
     if ":" in name:
         return f"the first {name.partition(':')[2]} halos of the {workload} list"
     return f"a sub-volume of {workload} with the same recipe and density"
 
 
-def cpu_baseline(workload, seed, budget_s=15.0):
-    """The oracle on a bounded sample of `workload`, repeated for ~budget_s."""
-    name = CPU_SAMPLE[workload]
-    wl = make_workload(name, seed)
+def _cpu_input(workload, seed):
+    name = CPU_SAMPLE.get(workload, workload)
+    return name, make_workload(name, seed)
+
+
+def cpu_baseline(workload, seed):
+    """The oracle on the workload (or its stated sample): one untimed call
+    on the warm-up sub-volume (thread pool, Green tables), then one timed
+    call."""
     threads = os.cpu_count() or 1
-    cpu_port_run(wl, threads)  # first call builds the Green's function tables
-    dts = []
-    deadline = time.perf_counter() + budget_s
-    used = threads
-    while time.perf_counter() < deadline or not dts:
-        dt, _, used = cpu_port_run(wl, threads)
-        dts.append(dt)
+    cpu_port_run(make_workload(CPU_WARMUP[workload], seed), threads)
+    name, wl = _cpu_input(workload, seed)
+    dt, _, used = cpu_port_run(wl, threads)
     n = wl["xp"].shape[1]
-    return {"value": n / (sum(dts) / len(dts)) / 1e6, "unit": "Mpart/s", "cores": used,
-            "kind": "port",
-            "sample": f"{name}: {n} particles, {_sample_kind(name, workload)}, {len(dts)} calls "
-                      "after one untimed call, reference thread policy"}
+    return {"value": n / dt / 1e6, "unit": "Mpart/s", "cores": used, "kind": "port",
+            "sample": f"{name}: {n} particles, {_sample_kind(name, workload)}, one call after one "
+                      f"untimed call on {CPU_WARMUP[workload]}, reference thread policy "
+                      "(one region: 2 linking threads; unbinding one flat dynamic pool over "
+                      "candidates)"}
 
 
 def run_reference(args):
     """--impl reference: the reference's CPU algorithm (restated in oracle/,
-    the reference itself cannot be built here) on all host cores, each step a
-    bounded sample of the workload."""
+    the reference itself cannot be built here) with the reference's thread
+    policy on all host cores.  Warm-up steps run on the workload's
+    sub-volume; every timed step is one full call on the workload itself
+    (or its stated sample for the two largest workloads)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    name = CPU_SAMPLE[args.workload]
-    wl = make_workload(name, args.seed)
-    n = wl["xp"].shape[1]
-    L, bound = wl["L"], wl["bound"]
     threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        cpu_port_run(wl, threads)
+    warm = make_workload(CPU_WARMUP[args.workload], args.seed)
+    for _ in range(max(1, args.warmup)):
+        cpu_port_run(warm, threads)
+    del warm
+    name, wl = _cpu_input(args.workload, args.seed)
+    n = wl["xp"].shape[1]
     times, used = [], threads
     for _ in range(args.steps):
         dt, _, used = cpu_port_run(wl, threads)
@@ -266,11 +299,11 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "particles": n, "L_Box": L, "link": LINK,
-                   "np_halo_min": wl["np_min"], "bound_check": bound, "softening": SOFTENING},
+        "config": _config(args.workload, wl, n, 1, "weak"),
         "cpu_baseline": {"value": v, "unit": "Mpart/s", "cores": used, "kind": "port",
                          "sample": f"{name}: {n} particles per step, "
-                                   f"{_sample_kind(name, args.workload)}, reference thread policy"},
+                                   f"{_sample_kind(name, args.workload)}; warm-up steps on "
+                                   f"{CPU_WARMUP[args.workload]}; reference thread policy"},
         "e2e": {"value": v, "unit": "Mpart/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -328,7 +361,6 @@ def run_b200(args):
     hid = torch.zeros(n, dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(dev)
     _native.set_stream(stream.cuda_stream)
-    _native.set_option("timing", 1)
 
     def step():
         _, ierr = _native.run_device(
@@ -337,23 +369,33 @@ def run_b200(args):
             d["np_min"], int(bound), 0, SOFTENING, 1.0, 0.0, s15, 0, ih.data_ptr(), hid.data_ptr())
         if ierr:
             raise RuntimeError(f"ierr={ierr}: {_native.last_error()}")
-        return {k: _native.last_stage_ms(k) for k in ("link", "fof", "unbind", "call", "pm_fft")} | {
-            "pm_fft_bytes": _native.get_stat("pm_fft_bytes")}
 
     def timed(steps):
+        """Device time per call over `steps` back-to-back calls (no stage
+        timers, no host reads between calls)."""
         torch.cuda.synchronize(dev)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        st = [step() for _ in range(steps)]
+        for _ in range(steps):
+            step()
         e1.record(stream)
         torch.cuda.synchronize(dev)
-        return e0.elapsed_time(e1) / steps, st
+        return e0.elapsed_time(e1) / steps
 
-    def mean(st, k):
-        return sum(s[k] for s in st) / len(st)
+    def stages(k=2):
+        """Stage device times (library timers) averaged over k more calls,
+        outside any timed region."""
+        st = []
+        with _native.options(timing=1):
+            for _ in range(k):
+                step()
+                st.append({key: _native.last_stage_ms(key) for key in ("link", "fof", "unbind", "call",
+                                                                        "pm_fft")}
+                          | {"pm_fft_bytes": _native.get_stat("pm_fft_bytes")})
+        return {key: sum(x[key] for x in st) / len(st) for key in st[0]}
 
-    # the product path: batched FP32 unbinding (library default)
+    # the product path: the library default (FP64 unbinding)
     for _ in range(max(args.warmup, 0)):
         step()
     torch.cuda.synchronize(dev)
@@ -362,7 +404,7 @@ def run_b200(args):
         dist.barrier()
     sampler = ClockSampler(local)
     sampler.start()
-    ms, st = timed(args.steps)
+    ms = timed(args.steps)
     clocks = sampler.stop()
     launches = _native.get_stat("launches") - launches0
     if world > 1:
@@ -375,6 +417,8 @@ def run_b200(args):
     ngroups = int(hid.max().item())
     counts = {k: _native.get_stat(k) for k in ("candidates", "direct_halos", "pm_halos",
                                                "valid_halos", "pm_solves")}
+    ncells = _native.get_stat("cells")
+    st = stages()
 
     if args.profile_run:
         # only the warm-up and timed product steps (for a profiler's launch list)
@@ -382,34 +426,37 @@ def run_b200(args):
             dist.destroy_process_group()
         if rank == 0:
             print(json.dumps({"profile_run": args.workload, "ms_per_step": ms_max,
-                              "gpu_launches": launches, "pm_fft_bytes_per_call": mean(st, "pm_fft_bytes"),
-                              "pm_fft_ms_per_call": mean(st, "pm_fft"), "pm_solves": counts["pm_solves"],
-                              "link_ms": mean(st, "link"), "cells": _native.get_stat("cells")}),
+                              "gpu_launches": launches, "pm_fft_bytes_per_call": st["pm_fft_bytes"],
+                              "pm_fft_ms_per_call": st["pm_fft"], "pm_solves": counts["pm_solves"],
+                              "link_ms": st["link"], "cells": ncells}),
                   flush=True)
         return 0
 
     unbind = None
+    fp32_st = None
     if bound:
         ncand = counts["candidates"]
 
         def leg(ms_call, st_):
-            u = mean(st_, "unbind")
+            u = st_["unbind"]
             return {"halos_per_s": ncand / (u * 1e-3) if u > 0 else None, "unbind_ms": u,
                     "call_ms": ms_call}
 
-        legs = {"fp32_batched": leg(ms, st)}
-        _native.set_option("unbind_fp64", 1)
-        step()
-        legs["fp64_batched"] = leg(*timed(max(1, args.steps // 3)))
-        _native.set_option("unbind_per_halo", 1)
-        legs["fp64_per_halo"] = leg(*timed(1))
-        _native.set_option("unbind_per_halo", 0)
-        _native.set_option("unbind_fp64", 0)
+        legs = {"fp64_batched": leg(ms, st)}
+        with _native.options(unbind_fp64=0):
+            step()
+            ms32 = timed(max(1, args.steps // 3))
+            fp32_st = stages()
+            legs["fp32_batched"] = leg(ms32, fp32_st)
+        with _native.options(unbind_per_halo=1):
+            ms_ph = timed(1)
+            legs["fp64_per_halo"] = leg(ms_ph, stages(1))
         base = legs["fp64_per_halo"]["halos_per_s"]
         unbind = {"halos": ncand, "direct": counts["direct_halos"], "pm": counts["pm_halos"],
                   "valid": counts["valid_halos"], "pm_solves": counts["pm_solves"], **legs,
-                  "fp32_vs_fp64_per_halo": (legs["fp32_batched"]["halos_per_s"] / base)
-                  if base else None}
+                  "fp32_vs_fp64_per_halo": (legs["fp32_batched"]["halos_per_s"] / base) if base else None,
+                  "fp32_vs_fp64_batched": (legs["fp32_batched"]["halos_per_s"] /
+                                           legs["fp64_batched"]["halos_per_s"])}
 
     # end to end through the public API with pinned host buffers
     def pinned(a):
@@ -452,23 +499,28 @@ def run_b200(args):
         d2h = 4 * n + 24 * (len(d["regions"][0]) if d["regions"] is not None else 1)
 
     peak, peak_kind = _peaks()
+
+    def roof(kname, k_ms, k_bytes, extra):
+        achieved = k_bytes / (k_ms * 1e-3) / 1e9 if k_ms > 0 else None
+        ratio = _traffic(args.workload, kname)
+        return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": ratio * k_bytes if ratio is not None else None,
+                "kernel": kname, "peak_kind": peak_kind, "algorithmic_bytes_per_call": k_bytes,
+                "kernel_ms_per_call": k_ms, **extra}
+
+    link_bytes = LINK_BYTES_PER_PARTICLE * n + LINK_BYTES_PER_CELL * ncells
+    roof_link = roof("fof_link", st["link"], link_bytes,
+                     {"kernels": "fof_link_dense_kernel + fof_link_kernel (one link stage)",
+                      "algorithmic_bytes": "20 B per particle + 4 B per cell"})
     if bound:
-        kname = "pm_convolve"
-        k_ms = mean(st, "pm_fft")
-        k_bytes = mean(st, "pm_fft_bytes")
-        roof_extra = {"kernels": "k_fft_x_r2c, k_fft_yz (3 launches), k_fft_x_c2r per batch",
-                      "algorithmic_bytes": "16 (n+2) n^2 per solve (a read and a write of the "
-                                           "padded grid per transform, two transforms)",
-                      "solves_per_call": counts["pm_solves"]}
+        roof_main = roof("pm_convolve_fp64", st["pm_fft"], st["pm_fft_bytes"],
+                         {"kernels": "k_x_r2c, k_lines (3 launches), k_x_c2r per batch (FP64 grids)",
+                          "algorithmic_bytes": "32 (n+2) n^2 per solve on FP64 grids (a read and a "
+                                               "write of the padded grid per transform, two transforms)",
+                          "solves_per_call": counts["pm_solves"]})
     else:
-        kname = "fof_link"
-        k_ms = mean(st, "link")
-        k_bytes = LINK_BYTES_PER_PARTICLE * n + LINK_BYTES_PER_CELL * _native.get_stat("cells")
-        roof_extra = {"kernels": "fof_link_dense_kernel + fof_link_kernel (one link stage)",
-                      "algorithmic_bytes": "20 B per particle + 4 B per cell"}
-    achieved = k_bytes / (k_ms * 1e-3) / 1e9 if k_ms > 0 else None
-    ratio = _traffic(args.workload, kname)
-    traffic = ratio * k_bytes if ratio is not None else None
+        roof_main = roof_link
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -483,25 +535,17 @@ def run_b200(args):
         "metric": "fof_mpart_per_s", "value": value, "unit": "Mpart/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
         "higher_is_better": True, "scaling": scaling, "vs_baseline": None,
-        "dtype": "f64 linking; f32 unbinding" if bound else "f64",
+        "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": args.workload, "particles": n_job if scaling == "strong" else n, "L_Box": Lbox, "link": LINK,
-                   "np_halo_min": d["np_min"], "bound_check": bound, "softening": SOFTENING,
-                   "s_15": s15, "regions": len(nph), "groups": ngroups, "unbinding": "fp32 batched" if bound else None,
-                   "l2": "inputs larger than L2 (402 MB positions)" if n >= 2 ** 24 else
-                         "inputs smaller than L2",
-                   "parallelism": (f"regions sharded x{world}" if scaling == "strong"
-                                   else f"replicas x{world}")},
-        "stages_ms": {"fof": mean(st, "fof"), "link_kernel": mean(st, "link"),
-                      "unbind": mean(st, "unbind"), "pm_fft": mean(st, "pm_fft")},
+        "config": _config(args.workload, d, n_job, world, scaling),
+        "groups": ngroups,
+        "stages_ms": {"fof": st["fof"], "link_kernel": st["link"], "unbind": st["unbind"],
+                      "pm_fft": st["pm_fft"]},
         "unbind": unbind,
         "e2e": {"value": e2e_value, "unit": "Mpart/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, **({"note": e2e_note} if e2e_note else {})},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": kname, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_call": k_bytes, "kernel_ms_per_call": k_ms,
-                     **roof_extra},
+        "roofline": roof_main,
+        "roofline_fof_link": roof_link,
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,

@@ -50,8 +50,12 @@ int32_t pyfof_shutdown(void);
  * truncated to len) and returns its full length. */
 int32_t pyfof_last_error(char *buf, int64_t len);
 
-/* Library options: "unbind_fp64" (1 = FP64 unbinding, batched; 0 = FP32
- * product path), "unbind_per_halo" (1 = the plain FP64 baseline: one halo per
+/* Library options: "unbind_fp64" (1 = FP64 unbinding, batched, the
+ * default: the direct sums of candidates up to 1000 members reproduce the
+ * reference's FP64 arithmetic bit for bit; 0 = the FP32 product path, whose
+ * potentials differ by FP32 rounding, so particles with a specific energy
+ * within about 1e-5 of the halo's |phi| scale of zero may be classified
+ * differently), "unbind_per_halo" (1 = the plain FP64 baseline: one halo per
  * launch sequence), "timing" (1 = record stage times), "unbind_big_np"
  * (particle-mesh halos above this many members run their removal loop
  * spread over the whole GPU; 0 = the default of 32768), "cell_order" (how
@@ -60,6 +64,9 @@ int32_t pyfof_last_error(char *buf, int64_t len);
  * radix sort; 1 = per-cell sorts whenever no cell holds more than 8192; 2 =
  * always the radix sort; all give the same order). */
 int32_t pyfof_set_option(const char *key, int64_t value);
+
+/* Current value of a pyfof_set_option key.  No reference counterpart. */
+int32_t pyfof_get_option(const char *key, int64_t *value);
 
 /* Issue all later work of the selected device on `stream` (a cudaStream_t;
  * NULL restores the library's own stream).  Lets a caller order calls with
@@ -76,7 +83,8 @@ int32_t pyfof_set_stream(void *stream);
  * particle mesh), "valid_halos" (halos written to the output),
  * "refined_regions" (two-level inner regions), "pm_solves" (halo-grid
  * convolutions over all passes), "pm_fft_bytes" (their algorithmic bytes:
- * 16 (n+2) n^2 per solve on an n^3 grid). */
+ * 4 s (n+2) n^2 per solve on an n^3 grid of s-byte reals: a read and a
+ * write of the padded grid per transform, two transforms). */
 int32_t pyfof_get_stat(const char *key, int64_t *value);
 
 /* Device time of the linking kernel of the last call, when timing is on. */

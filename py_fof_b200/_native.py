@@ -44,7 +44,7 @@ def _units_ptr(units):
 
 # every symbol include/pyfof_b200.h declares
 EXPORTED = ("pyfof_version", "pyfof_init", "pyfof_shutdown", "pyfof_last_error",
-            "pyfof_set_option", "pyfof_set_stream", "pyfof_get_stat", "pyfof_last_link_ms", "pyfof_last_stage_ms",
+            "pyfof_set_option", "pyfof_get_option", "pyfof_set_stream", "pyfof_get_stat", "pyfof_last_link_ms", "pyfof_last_stage_ms",
             "pyfof_halo_potential", "pyfof_halo_potential_direct_static", "pyfof_run",
             "pyfof_run_device", "pyfof_slot_create", "pyfof_slot_destroy", "pyfof_slot_run",
             "pyfof_slot_stat", "pyfof_run_catalogue", "pyfof_run_units")
@@ -72,6 +72,8 @@ def load():
         L.pyfof_last_error.argtypes = [ctypes.c_char_p, ctypes.c_int64]
         L.pyfof_set_option.restype = ctypes.c_int32
         L.pyfof_set_option.argtypes = [ctypes.c_char_p, ctypes.c_int64]
+        L.pyfof_get_option.restype = ctypes.c_int32
+        L.pyfof_get_option.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
         L.pyfof_set_stream.restype = ctypes.c_int32
         L.pyfof_set_stream.argtypes = [ctypes.c_void_p]
         L.pyfof_get_stat.restype = ctypes.c_int32
@@ -124,6 +126,36 @@ def last_error() -> str:
 def set_option(key: str, value: int) -> None:
     if load().pyfof_set_option(key.encode(), int(value)) != 0:
         raise ValueError(last_error())
+
+
+def get_option(key: str) -> int:
+    v = ctypes.c_int64(0)
+    if load().pyfof_get_option(key.encode(), ctypes.byref(v)) != 0:
+        raise ValueError(last_error())
+    return int(v.value)
+
+
+class options:
+    """Context manager: set library options, restore their values after.
+
+        with _native.options(unbind_fp64=0):
+            ...
+    """
+
+    def __init__(self, **opts):
+        self.opts = opts
+        self.old = {}
+
+    def __enter__(self):
+        for k, v in self.opts.items():
+            self.old[k] = get_option(k)
+            set_option(k, v)
+        return self
+
+    def __exit__(self, *exc):
+        for k, v in self.old.items():
+            set_option(k, v)
+        return False
 
 
 def set_stream(stream_handle: int) -> None:

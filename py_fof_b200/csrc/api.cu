@@ -19,7 +19,7 @@ thread_local std::string g_last_error;
 std::mutex g_ctx_mu;
 Context *g_ctx[64] = {};
 int g_default_device = 0;
-int g_bound_fp64 = 0;
+int g_bound_fp64 = 1;  // FP64 unbinding by default: direct sums bit-exact with the reference
 int g_bound_per_halo = 0;
 int g_timing = 0;
 int64_t g_big_np = 0;
@@ -240,6 +240,17 @@ int32_t pyfof_set_option(const char *key, int64_t value) {
     g_cell_order = (int)value;
     return kOk;
   }
+  set_error("unknown option %s", key);
+  return kInvalid;
+}
+
+int32_t pyfof_get_option(const char *key, int64_t *value) {
+  if (!key || !value) return kInvalid;
+  if (!std::strcmp(key, "unbind_fp64")) { *value = g_bound_fp64; return kOk; }
+  if (!std::strcmp(key, "unbind_per_halo")) { *value = g_bound_per_halo; return kOk; }
+  if (!std::strcmp(key, "timing")) { *value = g_timing; return kOk; }
+  if (!std::strcmp(key, "unbind_big_np")) { *value = g_big_np; return kOk; }
+  if (!std::strcmp(key, "cell_order")) { *value = g_cell_order; return kOk; }
   set_error("unknown option %s", key);
   return kInvalid;
 }

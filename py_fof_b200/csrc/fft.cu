@@ -283,9 +283,13 @@ __device__ __forceinline__ void stage_b_smem(const cplx_t<R> *src, cplx_t<R> *ds
 // half spectra are separated with the Hermitian symmetry of real
 // transforms.  All loops have compile-time trip counts, so every thread
 // issues its loads before the first one returns.
-template <typename R, int N>
+// FIX: the input is the fixed-point deposit grid (64-bit integers, grid b
+// scaled by inv_scale[b]) instead of R values.
+template <typename R, int N, bool FIX>
 __global__ void __launch_bounds__(Cfg<R, N>::T) k_x_r2c(const R *__restrict__ rho, cplx_t<R> *__restrict__ spec,
-                                                        int nhp, int nlines) {
+                                                        int nhp, int nlines,
+                                                        const unsigned long long *__restrict__ acc,
+                                                        const double *__restrict__ inv_scale) {
   using C = cplx_t<R>;
   constexpr int T = Cfg<R, N>::T, W = kW<R>, WP = W + 1, NH = N / 2 + 1, SUP = N / 2 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -300,8 +304,16 @@ __global__ void __launch_bounds__(Cfg<R, N>::T) k_x_r2c(const R *__restrict__ rh
     const int idx = threadIdx.x + it * T;
     if (idx < W * SUP) {
       const int p = idx / SUP, x = idx - p * SUP;
-      const R va = 2 * p < nl ? src[(2 * p) * SUP + x] : (R)0;
-      const R vb = 2 * p + 1 < nl ? src[(2 * p + 1) * SUP + x] : (R)0;
+      R va, vb;
+      if constexpr (FIX) {
+        const int la = L0 + 2 * p;
+        va = 2 * p < nl ? (R)((double)acc[(int64_t)la * SUP + x] * inv_scale[la / (SUP * SUP)]) : (R)0;
+        vb = 2 * p + 1 < nl ? (R)((double)acc[(int64_t)(la + 1) * SUP + x] * inv_scale[(la + 1) / (SUP * SUP)])
+                            : (R)0;
+      } else {
+        va = 2 * p < nl ? src[(2 * p) * SUP + x] : (R)0;
+        vb = 2 * p + 1 < nl ? src[(2 * p + 1) * SUP + x] : (R)0;
+      }
       t0[p + WP * x] = mk<C>(va, vb);
     }
   }
@@ -569,7 +581,8 @@ int32_t prepare() {
   std::call_once(once, [] {
     const size_t sm = smem_bytes<R, N>();
     int32_t r = kOk;
-    if (r == kOk) r = allow_smem(k_x_r2c<R, N>, sm);
+    if (r == kOk) r = allow_smem(k_x_r2c<R, N, false>, sm);
+    if (r == kOk) r = allow_smem(k_x_r2c<R, N, true>, sm);
     if (r == kOk) r = allow_smem(k_x_c2r<R, N, N / 2 + 1>, sm);
     if (r == kOk) r = allow_smem(k_x_c2r<R, N, N>, sm);
     if (r == kOk) r = allow_smem(k_lines<R, N, -1, false>, sm);
@@ -581,7 +594,8 @@ int32_t prepare() {
 }
 
 template <typename R, int N>
-int32_t convolve_n(R *rho, cplx_t<R> *spec, const R *green, int sup, int batch, cudaStream_t s) {
+int32_t convolve_n(R *rho, cplx_t<R> *spec, const R *green, int sup, int batch, cudaStream_t s,
+                   const unsigned long long *acc, const double *inv_scale) {
   PYFOF_TRY((prepare<R, N>()));
   constexpr int W = kW<R>, T = Cfg<R, N>::T;
   const int nhp = (int)spec_row<R>(N);
@@ -589,7 +603,12 @@ int32_t convolve_n(R *rho, cplx_t<R> *spec, const R *green, int sup, int batch, 
   const size_t sm = smem_bytes<R, N>();
   const int64_t bstride = (int64_t)N * N * nhp;
   const int64_t nlines = (int64_t)batch * sup * sup;
-  k_x_r2c<R, N><<<(unsigned)ceil_div(nlines, 2 * W), T, sm, s>>>(rho, spec, nhp, (int)nlines);
+  if (acc)
+    k_x_r2c<R, N, true><<<(unsigned)ceil_div(nlines, 2 * W), T, sm, s>>>(rho, spec, nhp, (int)nlines, acc,
+                                                                         inv_scale);
+  else
+    k_x_r2c<R, N, false><<<(unsigned)ceil_div(nlines, 2 * W), T, sm, s>>>(rho, spec, nhp, (int)nlines, nullptr,
+                                                                          nullptr);
   PYFOF_CHECK_LAUNCH();
   // y forward: lines (kx, z < sup), input y < sup, output all y
   k_lines<R, N, -1, false><<<(unsigned)((int64_t)ntiles * sup * batch), T, sm, s>>>(
@@ -651,17 +670,17 @@ int32_t c2r_full_n(const R *green, cplx_t<R> *spec, R *out, cudaStream_t s) {
 
 template <typename R>
 int32_t pm_convolve_batch(R *rho, cplx_t<R> *spec, const R *green, int n, int sup, int batch,
-                          cudaStream_t s) {
+                          cudaStream_t s, const unsigned long long *acc, const double *inv_scale) {
   if (sup != n / 2 + 1 || batch < 1 || (int64_t)batch * sup * sup >= (int64_t)1 << 30) {
     set_error("invalid convolution batch (n %d, support %d, batch %d)", n, sup, batch);
     return kInvalid;
   }
   switch (n) {
-    case 48: return convolve_n<R, 48>(rho, spec, green, sup, batch, s);
-    case 64: return convolve_n<R, 64>(rho, spec, green, sup, batch, s);
-    case 128: return convolve_n<R, 128>(rho, spec, green, sup, batch, s);
-    case 216: return convolve_n<R, 216>(rho, spec, green, sup, batch, s);
-    case 256: return convolve_n<R, 256>(rho, spec, green, sup, batch, s);
+    case 48: return convolve_n<R, 48>(rho, spec, green, sup, batch, s, acc, inv_scale);
+    case 64: return convolve_n<R, 64>(rho, spec, green, sup, batch, s, acc, inv_scale);
+    case 128: return convolve_n<R, 128>(rho, spec, green, sup, batch, s, acc, inv_scale);
+    case 216: return convolve_n<R, 216>(rho, spec, green, sup, batch, s, acc, inv_scale);
+    case 256: return convolve_n<R, 256>(rho, spec, green, sup, batch, s, acc, inv_scale);
     default: set_error("unsupported FFT size %d", n); return kInvalid;
   }
 }
@@ -678,8 +697,10 @@ int32_t c2r_full(const R *green, cplx_t<R> *spec, R *out, int n, cudaStream_t s)
   }
 }
 
-template int32_t pm_convolve_batch<float>(float *, float2 *, const float *, int, int, int, cudaStream_t);
-template int32_t pm_convolve_batch<double>(double *, double2 *, const double *, int, int, int, cudaStream_t);
+template int32_t pm_convolve_batch<float>(float *, float2 *, const float *, int, int, int, cudaStream_t,
+                                          const unsigned long long *, const double *);
+template int32_t pm_convolve_batch<double>(double *, double2 *, const double *, int, int, int, cudaStream_t,
+                                           const unsigned long long *, const double *);
 template int32_t c2r_full<float>(const float *, float2 *, float *, int, cudaStream_t);
 template int32_t c2r_full<double>(const double *, double2 *, double *, int, cudaStream_t);
 

@@ -43,9 +43,13 @@ constexpr int64_t spec_elems(int n) {
 //   spec  batch of half spectra (scratch)
 //   green half-spectrum table of real values, unpadded rows:
 //         green[((kz*n + ky)*(n/2+1) + kx]
+//   acc, inv_scale (optional): the density as 64-bit fixed-point cubes
+//         (value of grid b = acc * inv_scale[b]) read in place of rho; the
+//         output still goes to rho, which may alias acc
 template <typename R>
 int32_t pm_convolve_batch(R *rho, cplx_t<R> *spec, const R *green, int n, int sup, int batch,
-                          cudaStream_t s);
+                          cudaStream_t s, const unsigned long long *acc = nullptr,
+                          const double *inv_scale = nullptr);
 
 // FFTW-style c2r of a real half-spectrum table (the Green's function) into a
 // full n^3 real grid (unnormalised); used once per table to extract the

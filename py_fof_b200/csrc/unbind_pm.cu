@@ -200,6 +200,14 @@ struct PmHalo {      // device copy of one PM halo's parameters
   int32_t pad;
 };
 
+// One refined region of a two-level halo (bound_fortran.f90:614-823)
+struct TlRegion {
+  int32_t h, b, r, n_in;
+  float lo[3], hi[3];  // region bounds (grid units)
+  float bo;            // source margin 3.5 + 3/r
+  float u0[3];         // inner grid origin
+};
+
 // TSC weights and self potential (bound_fortran.f90:2562-2602).  FP32
 // weights as in the reference; the self term accumulates in FP64.
 template <typename R>
@@ -338,53 +346,112 @@ __global__ void pm_cellcount_kernel(const uint32_t *__restrict__ key, int64_t M,
 
 // ---------------------------------------------------------------- passes
 
-template <typename R>
-__global__ void pm_deposit_kernel(const Members m, const PmHalo *__restrict__ H,
-                                  const int32_t *__restrict__ mhalo, const uint8_t *__restrict__ keep,
-                                  const int3 *__restrict__ first, const float *__restrict__ wt,
-                                  const int32_t *__restrict__ slot, int64_t M, R *__restrict__ rho) {
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    const int h = mhalo[k];
-    if (h < 0 || !keep[k]) continue;
-    const PmHalo &p = H[h];
-    const int sl = slot[h];
-    if (sl < 0 || !p.pending) continue;
-    const int sup = p.sup;
-    R *g = rho + (int64_t)sl * sup * sup * sup;
-    const int3 f = first[k];
-    const float *w9 = wt + 9 * k;
-    const float wk = m.w[k];
-    for (int sz = 0; sz < 3; ++sz) {
-      const int z = f.z + sz - 1;
-      for (int sy = 0; sy < 3; ++sy) {
-        const int y = f.y + sy - 1;
-        for (int sx = 0; sx < 3; ++sx) {
-          const int x = f.x + sx - 1;
-          const R v = (R)__fmul_rn(__fmul_rn(__fmul_rn(wk, w9[sx]), w9[3 + sy]), w9[6 + sz]);
-          atomicAdd(&g[((int64_t)z * sup + y) * sup + x], v);
-        }
-      }
-    }
+// Deterministic deposit.  The TSC contributions (the reference's FP32
+// products w*wx*wy*wz, bound_fortran.f90:2657-2672) are added as 64-bit
+// fixed-point integers: integer addition is associative, so the deposited
+// grid does not depend on the order in which threads add, and every run
+// gives the same bits.  The scale 2^(61 - e), e = ilogb(kept mass), keeps
+// the sum of a halo's contributions below 2^62 (TSC weights sum to one per
+// member); one unit is 2^-61 of the kept mass, far below FP32 rounding.
+__device__ __forceinline__ int fx_exp(double mass) {
+  return (mass > 0.0 && isfinite(mass)) ? ilogb(mass) : 0;
+}
+
+__device__ __forceinline__ unsigned long long fx_quantum(float v, double scale) {
+  return __double2ull_rn((double)v * scale);
+}
+
+// Inverse scale of every grid of a batch: inv[j] = 2^(e - 61) of the halo
+// that owns grid j (its region's halo for refined regions, A != nullptr).
+__global__ void pm_batch_scale_kernel(const PmHalo *__restrict__ H, const int32_t *__restrict__ batch, int nb,
+                                      const TlRegion *__restrict__ A, double *__restrict__ inv) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nb; j += gridDim.x * blockDim.x) {
+    const int h = A ? A[batch[j]].h : batch[j];
+    inv[j] = scalbn(1.0, fx_exp(H[h].mkeep) - 61);
   }
 }
 
-// TSC gather and the C1 potential (bound_fortran.f90:2681-2703)
+// Last entry e0 of the ascending array off[0..n] with off[e0] <= idx.
+__device__ __forceinline__ int seg_of(const uint32_t *__restrict__ off, int n, uint32_t idx) {
+  int lo = 0, hi = n;  // off[lo] <= idx < off[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= idx) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Deposit of the kept members of a batch of halos (batch[j] = halo of
+// grid j, bpre = prefix of their member counts, bsrc[j] = first position of
+// halo j in cmem, the members sorted by short-range cell and a Morton
+// sub-key).  A warp takes 32 consecutive members of that spatial order;
+// lanes whose TSC stencils start at the same node add their contributions
+// with warp reductions first (exact integer sums), and one lane per stencil
+// node issues the atomic.
+__global__ void __launch_bounds__(BLK) pm_deposit_kernel(const Members m, const PmHalo *__restrict__ H,
+                                                         const int32_t *__restrict__ batch,
+                                                         const uint32_t *__restrict__ bpre,
+                                                         const uint32_t *__restrict__ bsrc, int nb,
+                                                         const uint32_t *__restrict__ cmem,
+                                                         const uint8_t *__restrict__ keep,
+                                                         const int3 *__restrict__ first,
+                                                         const float *__restrict__ wt, int sup,
+                                                         unsigned long long *__restrict__ acc) {
+  const uint32_t total = bpre[nb];
+  const int lane = threadIdx.x & 31;
+  const uint32_t stride = ((gridDim.x * blockDim.x) >> 5) << 5;
+  const int64_t sup3 = (int64_t)sup * sup * sup;
+  for (uint32_t i0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) << 5; i0 < total; i0 += stride) {
+    const uint32_t idx = i0 + lane;
+    bool ok = idx < total;
+    int j = 0;
+    int64_t k = 0;
+    if (ok) {
+      j = seg_of(bpre, nb, idx);
+      k = cmem[bsrc[j] + (idx - bpre[j])];
+      ok = keep[k] != 0;
+    }
+    const unsigned act = __ballot_sync(0xffffffffu, ok);
+    if (!ok) continue;
+    const double sc = scalbn(1.0, 61 - fx_exp(H[batch[j]].mkeep));
+    const int3 f = first[k];
+    const float *w9 = wt + 9 * k;
+    const float wk = m.w[k];
+    const uint64_t base = (uint64_t)j * sup3 + ((uint64_t)(f.z - 1) * sup + (f.y - 1)) * sup + (f.x - 1);
+    const unsigned grp = __match_any_sync(act, base);
+    const bool leader = (__ffs(grp) - 1) == lane;
+    for (int sz = 0; sz < 3; ++sz)
+      for (int sy = 0; sy < 3; ++sy)
+        for (int sx = 0; sx < 3; ++sx) {
+          const float v = __fmul_rn(__fmul_rn(__fmul_rn(wk, w9[sx]), w9[3 + sy]), w9[6 + sz]);
+          const unsigned long long q = fx_quantum(v, sc);
+          // q < 2^62: three 21-bit pieces, each group sum below 2^26
+          const unsigned s0 = __reduce_add_sync(grp, (unsigned)(q & 0x1FFFFFull));
+          const unsigned s1 = __reduce_add_sync(grp, (unsigned)((q >> 21) & 0x1FFFFFull));
+          const unsigned s2 = __reduce_add_sync(grp, (unsigned)(q >> 42));
+          if (leader)
+            atomicAdd(&acc[base + ((uint64_t)sz * sup + sy) * sup + sx],
+                      (unsigned long long)s0 + ((unsigned long long)s1 << 21) + ((unsigned long long)s2 << 42));
+        }
+  }
+}
+
+// TSC gather and the C1 potential (bound_fortran.f90:2681-2703) at the kept
+// members of a batch; grid j holds the potential of halo batch[j].
 template <typename R>
 __global__ void pm_gather_kernel(const Members m, const PmHalo *__restrict__ H,
-                                 const int32_t *__restrict__ mhalo, const uint8_t *__restrict__ keep,
-                                 const int3 *__restrict__ first, const float *__restrict__ wt,
-                                 const R *__restrict__ selfv, const int32_t *__restrict__ slot, int64_t M,
+                                 const int32_t *__restrict__ batch, const uint32_t *__restrict__ bpre, int nb,
+                                 const uint8_t *__restrict__ keep, const int3 *__restrict__ first,
+                                 const float *__restrict__ wt, const R *__restrict__ selfv, int sup,
                                  const R *__restrict__ rho, double a_val, R *__restrict__ phi_c1) {
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    const int h = mhalo[k];
-    if (h < 0 || !keep[k]) continue;
-    const PmHalo &p = H[h];
-    const int sl = slot[h];
-    if (sl < 0 || !p.pending) continue;
-    const int sup = p.sup;
-    const R *g = rho + (int64_t)sl * sup * sup * sup;
+  const uint32_t total = bpre[nb];
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    const int j = seg_of(bpre, nb, idx);
+    const PmHalo &p = H[batch[j]];
+    const int64_t k = p.off + (idx - bpre[j]);
+    if (!keep[k]) continue;
+    const R *g = rho + (int64_t)j * sup * sup * sup;
     const int3 f = first[k];
     const float *w9 = wt + 9 * k;
     R raw = 0;
@@ -669,13 +736,6 @@ __global__ void sr_removed_fill_kernel(const uint32_t *__restrict__ flag, const 
 
 // One refined region: halo h, region b (8x8x8 regions of 16 grid cells),
 // ratio r, inner grid n_in (bound_two_level_build_halo, :614-823).
-struct TlRegion {
-  int32_t h, b, r, n_in;
-  float lo[3], hi[3];  // region bounds (grid units)
-  float bo;            // source margin 3.5 + 3/r
-  float u0[3];         // inner grid origin
-};
-
 __device__ __forceinline__ void tl_t(const Members &m, const PmHalo &p, int64_t k, float *t) {
 #pragma unroll
   for (int d = 0; d < 3; ++d)
@@ -777,17 +837,6 @@ __global__ void tl_target_kernel(const int32_t *__restrict__ preg, int64_t M,
 
 // Node range checks of sources and targets, and the inner self term of
 // every target (:729-800).
-// Last entry e0 of the ascending array off[0..n] with off[e0] <= idx.
-__device__ __forceinline__ int seg_of(const uint32_t *__restrict__ off, int n, uint32_t idx) {
-  int lo = 0, hi = n;  // off[lo] <= idx < off[hi]
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (off[mid] <= idx) lo = mid;
-    else hi = mid;
-  }
-  return lo;
-}
-
 // Set-up of the refined regions, flat over all their sources and targets:
 // every source must fall inside its region's inner grid, and every target
 // gets its inner self term.
@@ -841,13 +890,14 @@ __global__ void tl_self_kernel(const Members m, const PmHalo *__restrict__ H,
 
 // Inner PM of a batch of refined regions of one inner grid size
 // (bound_two_level_run_pm, :825-942): deposit of the kept sources ...
-template <typename R>
 __global__ void tl_deposit_kernel(const Members m, const PmHalo *__restrict__ H,
                                   const TlRegion *__restrict__ A, const int32_t *__restrict__ batch,
                                   const uint32_t *__restrict__ bpre, int nb,
                                   const uint32_t *__restrict__ src_start, const uint32_t *__restrict__ src,
-                                  const uint8_t *__restrict__ keep, int sup, R *__restrict__ rho) {
-  // flat over the sources of the batch: bpre[j] = first index of region j
+                                  const uint8_t *__restrict__ keep, int sup,
+                                  unsigned long long *__restrict__ acc) {
+  // flat over the sources of the batch: bpre[j] = first index of region j;
+  // fixed-point integer adds as pm_deposit_kernel (order-independent)
   const uint32_t total = bpre[nb];
   for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
     const int j = seg_of(bpre, nb, idx);
@@ -856,7 +906,8 @@ __global__ void tl_deposit_kernel(const Members m, const PmHalo *__restrict__ H,
     const PmHalo &p = H[Rg.h];
     const int64_t k = src[src_start[a] + (idx - bpre[j])];
     if (!keep[k]) continue;
-    R *g = rho + (int64_t)j * sup * sup * sup;
+    unsigned long long *g = acc + (int64_t)j * sup * sup * sup;
+    const double sc = scalbn(1.0, 61 - fx_exp(p.mkeep));
     float t[3], w9[9];
     int f[3];
     tl_t(m, p, k, t);
@@ -865,8 +916,9 @@ __global__ void tl_deposit_kernel(const Members m, const PmHalo *__restrict__ H,
     for (int sz = 0; sz < 3; ++sz)
       for (int sy = 0; sy < 3; ++sy)
         for (int sx = 0; sx < 3; ++sx) {
-          const R v = (R)__fmul_rn(__fmul_rn(__fmul_rn(wk, w9[sx]), w9[3 + sy]), w9[6 + sz]);
-          atomicAdd(&g[((int64_t)(f[2] + sz - 1) * sup + (f[1] + sy - 1)) * sup + (f[0] + sx - 1)], v);
+          const float v = __fmul_rn(__fmul_rn(__fmul_rn(wk, w9[sx]), w9[3 + sy]), w9[6 + sz]);
+          atomicAdd(&g[((int64_t)(f[2] + sz - 1) * sup + (f[1] + sy - 1)) * sup + (f[0] + sx - 1)],
+                    fx_quantum(v, sc));
         }
   }
 }
@@ -1449,13 +1501,6 @@ __global__ void pm_fill_u8(uint8_t *a, int64_t n, uint8_t v) {
     a[i] = v;
 }
 
-template <typename R>
-__global__ void pm_zero_kernel(R *a, int64_t n) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    a[i] = (R)0;
-}
-
 // Members per 16-cell region of every 256-grid halo
 // (bound_two_level_setup_ratios, bound_fortran.f90:551-568).
 __global__ void pm_region_count_kernel(const Members m, const PmHalo *__restrict__ H,
@@ -1787,9 +1832,12 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
   // sized for the largest batch, serves every batch of every pass
   const size_t budget = ctx.pm_budget;
   auto round256 = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  // per grid: the fixed-point deposit grid (8 B a node; the convolved
+  // potential, R, is written back over it) and the half spectrum
   auto batch_bytes = [&](int n, int nb) {
     const size_t sup = n / 2 + 1;
-    return round256(sizeof(R) * nb * sup * sup * sup) + sizeof(cplx_t<R>) * (size_t)nb * spec_elems<R>(n);
+    return round256(sizeof(unsigned long long) * nb * sup * sup * sup) +
+           sizeof(cplx_t<R>) * (size_t)nb * spec_elems<R>(n);
   };
   auto max_batch = [&](int n) { return (int)std::max<size_t>(1, budget / batch_bytes(n, 1)); };
   size_t scratch_bytes = 256;
@@ -1805,10 +1853,20 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
     if (cnt) scratch_bytes = std::max(scratch_bytes, batch_bytes(nin, std::min(cnt, max_batch(nin))));
   }
   unsigned char *scratch = W.carve<unsigned char>(scratch_bytes);
-  int32_t *dpend = W.carve<int32_t>(nh), *dslot = W.carve<int32_t>(nh);
-  int32_t *dbatch = W.carve<int32_t>(std::max(na, 1));
-  uint32_t *dbpre = W.carve<uint32_t>(2 * (size_t)(std::max(na, 1) + 1));
-  if (!scratch || !dpend || !dslot || !dbatch || !dbpre) { set_error("workspace exhausted (PM grids)"); return kAlloc; }
+  int32_t *dpend = W.carve<int32_t>(nh);
+  const int nbat = std::max(std::max(na, nh), 1);
+  int32_t *dbatch = W.carve<int32_t>(nbat);
+  uint32_t *dbpre = W.carve<uint32_t>(2 * (size_t)(nbat + 1));
+  uint32_t *dbsrc = W.carve<uint32_t>(nbat);
+  double *dinv = W.carve<double>(nbat);
+  if (!scratch || !dpend || !dbatch || !dbpre || !dbsrc || !dinv) {
+    set_error("workspace exhausted (PM grids)");
+    return kAlloc;
+  }
+  // first position of every halo's members in cmem (PM members sort by
+  // cell, and the cells of halo h follow those of halo h-1)
+  std::vector<uint32_t> cm_off(nh + 1, 0);
+  for (int h = 0; h < nh; ++h) cm_off[h + 1] = cm_off[h] + (uint32_t)H[h].np;
   // halos above kBigNp members: chunked removal loop
   std::vector<BigHalo> hbig;
   std::vector<BigChunk> hch;
@@ -1876,23 +1934,34 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
       const int maxb = max_batch(n);
       for (size_t g0 = 0; g0 < grp.size(); g0 += maxb) {
         const int nb = (int)std::min<size_t>(maxb, grp.size() - g0);
-        std::vector<int32_t> hslot(nh, -1);
-        for (int j = 0; j < nb; ++j) hslot[grp[g0 + j]] = j;
-        PYFOF_CUDA(cudaMemcpyAsync(dslot, hslot.data(), sizeof(int32_t) * nh, cudaMemcpyHostToDevice, s));
-        R *rho = reinterpret_cast<R *>(scratch);
-        cplx_t<R> *spec = reinterpret_cast<cplx_t<R> *>(scratch + round256(sizeof(R) * (size_t)nb * sup * sup * sup));
+        // the batch's halos, their member prefix and their first cmem position
+        std::vector<uint32_t> bp(2 * (size_t)nb + 1, 0);
+        for (int j = 0; j < nb; ++j) {
+          const int h = grp[g0 + j];
+          bp[j + 1] = bp[j] + (uint32_t)H[h].np;
+          bp[nb + 1 + j] = cm_off[h];
+        }
+        PYFOF_CUDA(cudaMemcpyAsync(dbatch, grp.data() + g0, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s));
+        PYFOF_CUDA(cudaMemcpyAsync(dbpre, bp.data(), sizeof(uint32_t) * (nb + 1), cudaMemcpyHostToDevice, s));
+        PYFOF_CUDA(cudaMemcpyAsync(dbsrc, bp.data() + nb + 1, sizeof(uint32_t) * nb, cudaMemcpyHostToDevice, s));
+        unsigned long long *acc = reinterpret_cast<unsigned long long *>(scratch);
+        R *rho = reinterpret_cast<R *>(scratch);  // the convolved grids overwrite acc
+        cplx_t<R> *spec = reinterpret_cast<cplx_t<R> *>(
+            scratch + round256(sizeof(unsigned long long) * (size_t)nb * sup * sup * sup));
         const int64_t ng = (int64_t)nb * sup * sup * sup;
-        pm_zero_kernel<R><<<(unsigned)std::min<int64_t>(ceil_div(ng, BLK), 148 * 16), BLK, 0, s>>>(rho, ng);
+        PYFOF_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * ng, s));
+        pm_batch_scale_kernel<<<(unsigned)ceil_div(nb, 128), 128, 0, s>>>(dH, dbatch, nb, nullptr, dinv);
         PYFOF_CHECK_LAUNCH();
-        pm_deposit_kernel<R><<<gM, BLK, 0, s>>>(m, dH, mhalo, keep, first, wt, dslot, M, rho);
+        const unsigned gb = (unsigned)std::min<int64_t>(ceil_div(std::max<uint32_t>(bp[nb], 1), BLK), 148 * 16);
+        pm_deposit_kernel<<<gb, BLK, 0, s>>>(m, dH, dbatch, dbpre, dbsrc, nb, cmem, keep, first, wt, sup, acc);
         PYFOF_CHECK_LAUNCH();
         if (ctx.timing) ctx.conv_timer.begin(s);
-        PYFOF_TRY(pm_convolve_batch<R>(rho, spec, (const R *)green_of[n]->g, n, sup, nb, s));
+        PYFOF_TRY(pm_convolve_batch<R>(rho, spec, (const R *)green_of[n]->g, n, sup, nb, s, acc, dinv));
         if (ctx.timing) ctx.conv_timer.end(s);
         ctx.last_pm_solves += nb;
-        ctx.last_pm_fft_bytes += 16.0 * nb * (n + 2.0) * n * n;
-        pm_gather_kernel<R><<<gM, BLK, 0, s>>>(m, dH, mhalo, keep, first, wt, selfv, dslot, M, rho, a.a_val,
-                                               c1);
+        ctx.last_pm_fft_bytes += 4.0 * sizeof(R) * nb * (n + 2.0) * n * n;
+        pm_gather_kernel<R><<<gb, BLK, 0, s>>>(m, dH, dbatch, dbpre, nb, keep, first, wt, selfv, sup, rho,
+                                               a.a_val, c1);
         PYFOF_CHECK_LAUNCH();
       }
     }
@@ -1908,8 +1977,10 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
       const R *gin = (const R *)(r == 2 ? g_r2 : g_r4)->g;
       for (size_t g0 = 0; g0 < regs.size(); g0 += maxb) {
         const int nb = (int)std::min<size_t>(maxb, regs.size() - g0);
-        R *rho = reinterpret_cast<R *>(scratch);
-        cplx_t<R> *spec = reinterpret_cast<cplx_t<R> *>(scratch + round256(sizeof(R) * (size_t)nb * sup * sup * sup));
+        unsigned long long *acc = reinterpret_cast<unsigned long long *>(scratch);
+        R *rho = reinterpret_cast<R *>(scratch);  // the convolved grids overwrite acc
+        cplx_t<R> *spec = reinterpret_cast<cplx_t<R> *>(
+            scratch + round256(sizeof(unsigned long long) * (size_t)nb * sup * sup * sup));
         // prefix counts of the batch's sources and targets (flat launches)
         std::vector<uint32_t> bp(2 * (size_t)(nb + 1), 0);
         for (int j = 0; j < nb; ++j) {
@@ -1920,16 +1991,17 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
         PYFOF_CUDA(cudaMemcpyAsync(dbatch, regs.data() + g0, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s));
         PYFOF_CUDA(cudaMemcpyAsync(dbpre, bp.data(), sizeof(uint32_t) * bp.size(), cudaMemcpyHostToDevice, s));
         const int64_t ng = (int64_t)nb * sup * sup * sup;
-        pm_zero_kernel<R><<<(unsigned)std::min<int64_t>(ceil_div(ng, BLK), 148 * 16), BLK, 0, s>>>(rho, ng);
+        PYFOF_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * ng, s));
+        pm_batch_scale_kernel<<<(unsigned)ceil_div(nb, 128), 128, 0, s>>>(dH, dbatch, nb, dA, dinv);
         PYFOF_CHECK_LAUNCH();
         const unsigned gd = (unsigned)std::min<int64_t>(ceil_div(std::max<uint32_t>(bp[nb], 1), BLK), 148 * 16);
-        tl_deposit_kernel<R><<<gd, BLK, 0, s>>>(m, dH, dA, dbatch, dbpre, nb, src_start, src, keep, sup, rho);
+        tl_deposit_kernel<<<gd, BLK, 0, s>>>(m, dH, dA, dbatch, dbpre, nb, src_start, src, keep, sup, acc);
         PYFOF_CHECK_LAUNCH();
         if (ctx.timing) ctx.conv_timer.begin(s);
-        PYFOF_TRY(pm_convolve_batch<R>(rho, spec, gin, nin, sup, nb, s));
+        PYFOF_TRY(pm_convolve_batch<R>(rho, spec, gin, nin, sup, nb, s, acc, dinv));
         if (ctx.timing) ctx.conv_timer.end(s);
         ctx.last_pm_solves += nb;
-        ctx.last_pm_fft_bytes += 16.0 * nb * (nin + 2.0) * nin * nin;
+        ctx.last_pm_fft_bytes += 4.0 * sizeof(R) * nb * (nin + 2.0) * nin * nin;
         const unsigned gg = (unsigned)std::min<int64_t>(
             ceil_div(std::max<uint32_t>(bp[2 * nb + 1], 1), BLK), 148 * 16);
         tl_gather_kernel<R><<<gg, BLK, 0, s>>>(m, dH, dA, dbatch, dbpre + nb + 1, nb, tgt_start, tgt, keep,

@@ -6,8 +6,11 @@ place of FFTW3f, so PM parity is a tolerance, not bit equality:
   * first-pass potentials (C1 + C2): FP64 device path within 1e-5 of the
     oracle, FP32 product path within 1e-5 of the FP64 device path
     (relative to the halo's largest |phi|);
-  * end-to-end membership: only particles whose specific energy is within
-    a small relative band around zero may be classified differently.
+  * end-to-end membership: only particles whose oracle specific energy is
+    within the energy band around zero (tests/helpers.py ENERGY_BAND times
+    the halo's max |phi|) may be classified differently; halo counts and the
+    ids of particles both keep are equal; each result's angular momentum
+    matches its own members.
 """
 import numpy as np
 import pytest
@@ -15,7 +18,7 @@ import pytest
 import py_fof_b200 as P
 from oracle import oracle as O
 from py_fof_b200 import _native
-from tests.helpers import oracle_core
+from tests.helpers import check_ang_mom_consistent, check_unbinding_band, oracle_core_diag
 
 pytestmark = pytest.mark.gpu
 
@@ -96,19 +99,15 @@ def _pm_halos(seed, sizes):
 def test_pm_unbinding_end_to_end(fp64):
     xs, vs, ms = _pm_halos(7, [1200, 2500, 4000, 9000, 1100, 600, 300])
     kw = dict(vp_list=vs, mp_list=ms, L_Box=512.0, linking_length=0.3, np_halo_min=10,
-              bound_check=True)
-    _native.set_option("unbind_fp64", int(fp64))
-    try:
+              bound_check=True, return_ang_mom=True)
+    with _native.options(unbind_fp64=int(fp64)):
         g = P._fof_core(xs, **kw)
-    finally:
-        _native.set_option("unbind_fp64", 0)
-    o = oracle_core(xs, **kw)
     assert _native.get_stat("pm_halos") >= 3
-    n_in = int(o[0].sum())
-    mism = int((g[0] != o[0]).sum())
-    assert n_in > 1000
-    assert mism <= max(3, n_in // 1000), (mism, n_in)
-    assert int(g[1].max()) == int(o[1].max())
+    o, energy, scale = oracle_core_diag(xs, **kw)
+    assert int(o[0].sum()) > 1000
+    flips, worst = check_unbinding_band(g, o, energy, scale)
+    print(f"pm fp64={fp64}: {flips} flips, worst |E|/max|phi| = {worst:.2e}")
+    check_ang_mom_consistent(g, xs, vs, ms, 512.0)
 
 
 @pytest.mark.parametrize("fp64", [True, False])
@@ -117,35 +116,26 @@ def test_large_halo_removal_loop(fp64):
     loop spread over the GPU against the oracle."""
     xs, vs, ms = _pm_halos(21, [40000, 3000, 1500])
     kw = dict(vp_list=vs, mp_list=ms, L_Box=512.0, linking_length=0.3, np_halo_min=10,
-              bound_check=True)
-    _native.set_option("unbind_fp64", int(fp64))
-    try:
+              bound_check=True, return_ang_mom=True)
+    with _native.options(unbind_fp64=int(fp64)):
         g = P._fof_core(xs, **kw)
-    finally:
-        _native.set_option("unbind_fp64", 0)
-    o = oracle_core(xs, **kw)
-    n_in = int(o[0].sum())
-    assert n_in > 30000
-    mism = int((g[0] != o[0]).sum())
-    assert mism <= max(3, n_in // 1000), (mism, n_in)
-    assert int(g[1].max()) == int(o[1].max())
+    o, energy, scale = oracle_core_diag(xs, **kw)
+    assert int(o[0].sum()) > 30000
+    flips, worst = check_unbinding_band(g, o, energy, scale)
+    print(f"large halo fp64={fp64}: {flips} flips, worst |E|/max|phi| = {worst:.2e}")
+    check_ang_mom_consistent(g, xs, vs, ms, 512.0)
 
 
 def test_chunked_loop_equals_block_loop():
     """Every PM halo through the chunked removal loop (threshold lowered)
     against the one-block loop: the same algorithm, centre sums in another
-    order, so only marginally bound members may differ."""
+    order, so only particles inside the energy band may differ."""
     xs, vs, ms = _pm_halos(7, [1200, 2500, 4000, 9000, 1100, 600, 300])
     kw = dict(vp_list=vs, mp_list=ms, L_Box=512.0, linking_length=0.3, np_halo_min=10,
               bound_check=True, return_ang_mom=True)
-    _native.set_option("unbind_fp64", 1)
-    try:
+    with _native.options(unbind_fp64=1):
         a = P._fof_core(xs, **kw)
-        _native.set_option("unbind_big_np", 1000)
-        b = P._fof_core(xs, **kw)
-    finally:
-        _native.set_option("unbind_big_np", 0)
-        _native.set_option("unbind_fp64", 0)
-    n_in = int(a[0].sum())
-    assert int((a[0] != b[0]).sum()) <= max(2, n_in // 2000)
-    assert int(a[1].max()) == int(b[1].max())
+        with _native.options(unbind_big_np=1000):
+            b = P._fof_core(xs, **kw)
+    _, energy, scale = oracle_core_diag(xs, **kw)
+    check_unbinding_band(a, b, energy, scale)

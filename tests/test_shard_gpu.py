@@ -1,8 +1,9 @@
 """List input split across two ranks that both run the native library on
 the one GPU of the test box (gloo for the output exchange; the ranks'
-kernels never wait on each other): the result equals the single call, up to
-the particle-mesh deposit's atomic summation order (different halos share a
-batch in the two runs), which may flip a marginally bound member."""
+kernels never wait on each other): the result equals the single call bit
+for bit in membership and halo ids (each halo's unbinding does not depend on
+which halos share its batch: the particle-mesh deposit adds fixed-point
+integers)."""
 import os
 import socket
 
@@ -50,6 +51,6 @@ def test_sharded_native_equals_single_call(tmp_path):
     assert hid.max() > 5
     for r in range(2):
         z = np.load(f"{out}_{r}.npz")
-        assert int((z["ih"] != ih).sum()) <= max(2, int(ih.sum()) // 1000)
-        assert int(z["hid"].max()) == int(hid.max())
-        assert np.allclose(z["am"], am, rtol=1e-4, atol=1e-4 * np.abs(am).max())
+        assert np.array_equal(z["ih"], ih)
+        assert np.array_equal(z["hid"], hid)
+        assert np.allclose(z["am"], am, rtol=1e-9, atol=1e-9 * np.abs(am).max())

@@ -9,7 +9,7 @@ import pytest
 
 import py_fof_b200 as P
 from py_fof_b200 import _native, workloads as W
-from tests.helpers import angmom_close, oracle_core
+from tests.helpers import check_unbinding_band, oracle_core_diag, angmom_close, oracle_core
 
 pytestmark = pytest.mark.gpu
 
@@ -62,10 +62,9 @@ def test_physical_unbinding_within_tolerance():
               units="physical", softening=0.1 * dx, n_sim=512 ** 3, ng_global=512.0)
     assert P._prepare(xs_phys, device_units=True, **kw).units[0] == dx
     g = P._fof_core(xs_phys, **kw)
-    o = oracle_core(xs_phys, **kw)
-    n_in = int(o[0].sum())
-    assert n_in > 1000
-    assert int((g[0] != o[0]).sum()) <= max(3, n_in // 1000)
+    o, energy, scale = oracle_core_diag(xs_phys, **kw)
+    assert int(o[0].sum()) > 1000
+    check_unbinding_band(g, o, energy, scale)
 
 
 def test_invalid_raw_mass_rejected_before_conversion():
