@@ -1260,6 +1260,143 @@ static int classify(const bctx *c, const float *xv, const int32_t *cand_np, cons
     return 0;
 }
 
+/* ------------------------------------------------ the reference's schedule
+ *
+ * bound_classify's groups and queues (bound_fortran.f90:2986-3067) and
+ * compute_bound_parallel_config / the phase build of bound_check_batch
+ * (:332-401, :1627-1665): group g = grid class (direct-summation halos join
+ * group 1); cost = n(n-1)/2 for direct halos, 6 V log2 V + 12 V + 64 n +
+ * 9 n log2 max(2,n) with V = bn(g)^3 for PM halos; each group's queue in
+ * descending cost (ties: ascending candidate index); phase 1 runs group 4
+ * with g4_team workers, phase 2 groups 1-3 with a greedy split of the
+ * remaining threads (or one phase per group, 3 down to 1, when there are
+ * fewer threads than groups); a worker takes halos only from its own
+ * group's queue.  The reference's group-4 workers each own g4_nest threads
+ * for their short-range sums (a nested team whose per-thread partial sums
+ * make results thread-count dependent); here every halo's sums run on its
+ * worker's thread alone, so results do not depend on the thread count. */
+typedef struct {
+    int nphases;
+    int workers[5][4];
+    int next[4], last[4];
+    int32_t *queue;
+} sched_t;
+
+static void bound_parallel_config(int T, const int M[4], const double W[4], const double L[4],
+                                  int nmax4, int *g4_team, int *g4_nest, int gteam[3])
+{
+    if (M[3] == 0) { *g4_team = 0; *g4_nest = 1; }
+    else {
+        *g4_nest = (T >= 2 && M[3] <= 10 * T && nmax4 > 10000) ? 2 : 1;
+        int t = T / *g4_nest;
+        if (t < 1) t = 1;
+        *g4_team = M[3] < t ? M[3] : t;
+    }
+    int B = M[0] + M[1] + M[2];
+    if (B > T) B = T;
+    int K = (M[0] > 0) + (M[1] > 0) + (M[2] > 0);
+    gteam[0] = gteam[1] = gteam[2] = 0;
+    if (B >= K && K > 0) {
+        for (int g = 0; g < 3; ++g) if (M[g] > 0) gteam[g] = 1;
+        int used = gteam[0] + gteam[1] + gteam[2];
+        while (used < B) {
+            int best = -1;
+            double best_gain = -1.0;
+            for (int g = 0; g < 3; ++g)
+                if (gteam[g] >= 1 && gteam[g] < M[g]) {
+                    double before = fmax(L[g], W[g] / (double)gteam[g]);
+                    double after = fmax(L[g], W[g] / (double)(gteam[g] + 1));
+                    if (before - after > best_gain) { best_gain = before - after; best = g; }
+                }
+            if (best_gain <= 0.0) {
+                double best_load = -1.0;
+                for (int g = 0; g < 3; ++g)
+                    if (gteam[g] >= 1 && gteam[g] < M[g] && W[g] / (double)gteam[g] > best_load) {
+                        best_load = W[g] / (double)gteam[g];
+                        best = g;
+                    }
+            }
+            if (best < 0) break;
+            ++gteam[best];
+            ++used;
+        }
+    }
+}
+
+static const double *g_cost_sort;
+static int cmp_cost_desc(const void *a, const void *b)
+{
+    int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
+    if (g_cost_sort[x] > g_cost_sort[y]) return -1;
+    if (g_cost_sort[x] < g_cost_sort[y]) return 1;
+    return (x > y) - (x < y);
+}
+
+static int schedule(const bctx *c, const htask *tasks, const int32_t *cand_np, int32_t ncand, int T,
+                    sched_t *sc)
+{
+    static pthread_mutex_t mu = PTHREAD_MUTEX_INITIALIZER;
+    memset(sc, 0, sizeof(*sc));
+    int M[4] = {0, 0, 0, 0}, nmax4 = 0;
+    double W[4] = {0, 0, 0, 0}, L[4] = {0, 0, 0, 0};
+    double *cost = (double *)malloc(sizeof(double) * (size_t)(ncand > 0 ? ncand : 1));
+    int *grp = (int *)malloc(sizeof(int) * (size_t)(ncand > 0 ? ncand : 1));
+    sc->queue = (int32_t *)malloc(sizeof(int32_t) * (size_t)(ncand > 0 ? ncand : 1));
+    if (!cost || !grp || !sc->queue) { free(cost); free(grp); free(sc->queue); sc->queue = NULL; return 1; }
+    for (int32_t h = 0; h < ncand; ++h) {
+        const double nn = (double)cand_np[h];
+        int g;
+        if (tasks[h].gid == 0) {
+            g = 0;
+            cost[h] = nn * (nn - 1.0) / 2.0;
+        } else {
+            g = tasks[h].gid - 1;
+            const double vol = (double)c->bn[g] * (double)c->bn[g] * (double)c->bn[g];
+            cost[h] = 6.0 * vol * log(vol) / log(2.0) + 12.0 * vol + 64.0 * nn +
+                      9.0 * nn * log(fmax(2.0, nn)) / log(2.0);
+        }
+        grp[h] = g;
+        ++M[g];
+        W[g] += cost[h];
+        if (cost[h] > L[g]) L[g] = cost[h];
+        if (g == 3 && cand_np[h] > nmax4) nmax4 = cand_np[h];
+    }
+    int cur[4];
+    cur[0] = 0;
+    for (int g = 1; g < 4; ++g) cur[g] = cur[g - 1] + M[g - 1];
+    for (int g = 0; g < 4; ++g) { sc->next[g] = cur[g]; sc->last[g] = cur[g] + M[g] - 1; }
+    for (int32_t h = 0; h < ncand; ++h) sc->queue[cur[grp[h]]++] = h;
+    pthread_mutex_lock(&mu);
+    g_cost_sort = cost;
+    for (int g = 0; g < 4; ++g)
+        if (M[g] > 1) qsort(sc->queue + sc->next[g], (size_t)M[g], sizeof(int32_t), cmp_cost_desc);
+    pthread_mutex_unlock(&mu);
+    int g4_team, g4_nest, gt[3];
+    bound_parallel_config(T, M, W, L, nmax4, &g4_team, &g4_nest, gt);
+    if (g4_team > 0) {
+        sc->workers[sc->nphases][3] = g4_team;
+        ++sc->nphases;
+    }
+    if (M[0] + M[1] + M[2] > 0) {
+        int B = M[0] + M[1] + M[2];
+        if (B > T) B = T;
+        int K = (M[0] > 0) + (M[1] > 0) + (M[2] > 0);
+        if (B >= K) {
+            for (int g = 0; g < 3; ++g) sc->workers[sc->nphases][g] = gt[g];
+            ++sc->nphases;
+        } else {
+            for (int g = 2; g >= 0; --g)
+                if (M[g] > 0) {
+                    sc->workers[sc->nphases][g] = M[g] < B ? M[g] : B;
+                    ++sc->nphases;
+                }
+        }
+    }
+    free(cost);
+    free(grp);
+    return 0;
+}
+
 int32_t oracle_bound_batch(const float *xv, const float *mp, const int64_t *pid,
                            const int32_t *cand_np, int32_t ncand, double softening,
                            double a_val, double b_val, double s15, int32_t np_halo_min,
@@ -1306,33 +1443,54 @@ int32_t oracle_bound_batch_diag(const float *xv, const float *mp, const int64_t 
                 !get_green(TL_NR4, H_SPLIT, 14.0, 0)) ierr = 1;
         }
         int T = n_threads > 0 ? n_threads : omp_get_max_threads();
-#pragma omp parallel for schedule(dynamic, 1) num_threads(T)
-        for (int32_t h = 0; h < ncand; ++h) {
-            int e;
+        sched_t sc;
+        if (schedule(&c, tasks, cand_np, ncand, T, &sc)) {
+            ierr = 3;
+        } else {
+            omp_set_max_active_levels(2);
+            for (int ph = 0; ph < sc.nphases && !ierr; ++ph) {
+                int wg[1024], nslots = 0;
+                for (int g = 3; g >= 0; --g)
+                    for (int l = 0; l < sc.workers[ph][g] && nslots < 1024; ++l) wg[nslots++] = g;
+                if (nslots <= 0) continue;
+#pragma omp parallel num_threads(nslots)
+                {
+                    const int g = wg[omp_get_thread_num()];
+                    for (;;) {
+                        int e, pos;
 #pragma omp atomic read
-            e = ierr;
-            if (e) continue;
-            int np = cand_np[h];
-            int32_t *member = (int32_t *)malloc(sizeof(int32_t) * (size_t)np);
-            char *keep = (char *)malloc((size_t)np);
-            for (int i = 0; i < np; ++i) member[i] = (int32_t)(off[h] + i);
-            int st = -1, nb = 0;
-            e = check_grid(&c, &tasks[h], xv, mp, pid, member, np, &st, &nb, keep,
-                           phi_out ? phi_out + off[h] : NULL, 0, energy_tab,
-                           phimax ? phimax + h : NULL);
-            if (e) {
+                        e = ierr;
+                        if (e) break;
+#pragma omp atomic capture
+                        pos = sc.next[g]++;
+                        if (pos > sc.last[g]) break;
+                        const int32_t h = sc.queue[pos];
+                        int np = cand_np[h];
+                        int32_t *member = (int32_t *)malloc(sizeof(int32_t) * (size_t)np);
+                        char *keep = (char *)malloc((size_t)np);
+                        for (int i = 0; i < np; ++i) member[i] = (int32_t)(off[h] + i);
+                        int st = -1, nb = 0;
+                        e = check_grid(&c, &tasks[h], xv, mp, pid, member, np, &st, &nb, keep,
+                                       phi_out ? phi_out + off[h] : NULL, 0, energy_tab,
+                                       phimax ? phimax + h : NULL);
+                        if (e) {
 #pragma omp critical(oracle_bound_err)
-                if (!ierr) ierr = e;
-            } else {
-                status[h] = st;
-                np_bound[h] = nb;
-                if (st == 0) {
-                    int cnt = 0;
-                    for (int i = 0; i < np; ++i) if (keep[i]) final_members[off[h] + cnt++] = member[i];
+                            if (!ierr) ierr = e;
+                        } else {
+                            status[h] = st;
+                            np_bound[h] = nb;
+                            if (st == 0) {
+                                int cnt = 0;
+                                for (int i = 0; i < np; ++i)
+                                    if (keep[i]) final_members[off[h] + cnt++] = member[i];
+                            }
+                        }
+                        free(member);
+                        free(keep);
+                    }
                 }
             }
-            free(member);
-            free(keep);
+            free(sc.queue);
         }
     }
     free(off);

@@ -10,7 +10,7 @@ stores inputs plus the test's expected answers as ``.npz`` fixtures in this
 directory.
 
 Usage (needs the reference checkout, read-only):
-    python tests/golden/make_golden.py [path/to/reference]
+    python tests/golden/make_golden.py path/to/reference   (or PYFOF_REFERENCE=...)
 The fixtures are committed; tests never read the reference tree.
 """
 from __future__ import annotations
@@ -113,4 +113,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PYFOF_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py <reference checkout> (or set PYFOF_REFERENCE)")
+    main(ref)
