@@ -311,6 +311,104 @@ def run_reference(args):
     return 0
 
 
+def _exact_potential(q, w, targets, softening, a_val=1.0):
+    """Exact softened direct-sum potential in FP64 (torch on the device, a
+    plain library reference): phi_t = -a/(6 pi) sum_{j != t} w_j D(|q_j - q_t|)
+    with D the spline-softened 1/r of the reference's direct path
+    (bound_fortran.f90:3080-3102)."""
+    import torch
+    dev = torch.device("cuda")
+    qd = torch.from_numpy(np.ascontiguousarray(q, dtype=np.float64)).to(dev)
+    wd = torch.from_numpy(np.ascontiguousarray(w, dtype=np.float64)).to(dev)
+    tg = torch.from_numpy(np.ascontiguousarray(targets, dtype=np.int64)).to(dev)
+    h = float(softening)
+    out = torch.empty(len(targets), dtype=torch.float64, device=dev)
+    n = q.shape[1]
+    step = max(1, (1 << 26) // max(n, 1))
+    for s0 in range(0, len(targets), step):
+        t = tg[s0:s0 + step]
+        d = qd[:, None, :] - qd[:, t, None]
+        r = torch.sqrt((d * d).sum(0))
+        e = 2.0 * r / h
+        inner = (208.0 - e * e * (112.0 + e * e * (-56.0 + e * (14.0 + e * (8.0 - 3.0 * e))))) / (70.0 * h)
+        es = torch.clamp(e, min=1e-300)
+        outer = (128.0 - (e * e * (448.0 + e * (-280.0 + e * (56.0 + e * (14.0 + e * (-8.0 + e)))))
+                          - 224.0 * e - 12.0 / es)) / (70.0 * h)
+        D = torch.where(r >= h, 1.0 / torch.clamp(r, min=1e-300), torch.where(e <= 1.0, inner, outer))
+        D[torch.arange(len(t), device=dev), t] = 0.0  # no self term
+        out[s0:s0 + len(t)] = -(a_val / (6.0 * np.pi)) * (D * wd[None, :]).sum(1)
+    return out.cpu().numpy()
+
+
+def potential_error_report(d, seed=0, per_stratum=6):
+    """Per-halo first-pass potential errors of the FP32 product path against
+    the FP64 device path and both against the exact FP64 direct sum, and the
+    energy error of each halo's final kept set (FP32 path), for a sample of
+    the list's halos stratified by size.  Errors are max |phi - phi_ref| over
+    the compared members divided by max |phi_ref| of the halo; energies are
+    specific energies 1/2 |v - v_c|^2 + phi of the kept members (v_c their
+    mean velocity) with the FP32 path's and the exact potential of the kept
+    set, divided by max |E|.  Halos above 20,000 members are compared at
+    4096 sampled members."""
+    import py_fof_b200 as P
+    from py_fof_b200 import _native
+    xs, vs = d["regions"]
+    sizes = np.array([x.shape[1] for x in xs])
+    strata = [("direct", 0, 1000), ("pm_1k_5k", 1000, 5000), ("pm_5k_20k", 5000, 20000),
+              ("pm_20k_200k", 20000, 200000), ("pm_200k_up", 200000, 1 << 40)]
+    rng = np.random.default_rng(seed + 77)
+    kw = dict(vp_list=vs, L_Box=d["L"], linking_length=LINK, np_halo_min=d["np_min"], bound_check=True,
+              softening=SOFTENING, ng_global=d["ng_global"])
+    with _native.options(unbind_fp64=0):
+        ih32 = P.fof(xs, **kw)
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    out = {}
+    for name, lo, hi in strata:
+        idx = np.nonzero((sizes > lo) & (sizes <= hi))[0]
+        if idx.size == 0:
+            continue
+        pick = rng.choice(idx, size=min(per_stratum, idx.size), replace=False)
+        rows = []
+        for r in pick:
+            x, v = xs[r], vs[r]
+            n = x.shape[1]
+            q = (x - x[:, :1]).astype(np.float32)
+            w = np.ones(n, np.float32)
+            p32, g = _native.halo_potential(q, w, softening=SOFTENING, s15=d["s15"], fp64=False)
+            p64, _ = _native.halo_potential(q, w, softening=SOFTENING, s15=d["s15"], fp64=True)
+            tg = np.arange(n) if n <= 20000 else np.sort(rng.choice(n, 4096, replace=False))
+            ex = _exact_potential(q, w, tg, SOFTENING)
+            sc = np.abs(ex).max()
+            row = {"np": int(n), "method": int(g),
+                   "fp32_vs_fp64": float(np.abs(p32 - p64).max() / np.abs(p64).max()),
+                   "fp32_vs_exact": float(np.abs(p32[tg] - ex).max() / sc),
+                   "fp64_vs_exact": float(np.abs(p64[tg] - ex).max() / sc)}
+            keep = np.nonzero(ih32[off[r]:off[r] + n])[0]
+            if keep.size >= 2:
+                qk = (x[:, keep] - x[:, keep[:1]]).astype(np.float32)
+                wk = np.ones(keep.size, np.float32)
+                pk32, _ = _native.halo_potential(qk, wk, softening=SOFTENING, s15=d["s15"], fp64=False)
+                tk = np.arange(keep.size) if keep.size <= 20000 else \
+                    np.sort(rng.choice(keep.size, 4096, replace=False))
+                exk = _exact_potential(qk, wk, tk, SOFTENING)
+                vk = v[:, keep] - v[:, keep].mean(axis=1, keepdims=True)
+                kin = 0.5 * (vk[:, tk] ** 2).sum(0)
+                e_ex = kin + exk
+                row["kept"] = int(keep.size)
+                row["energy_fp32_vs_exact"] = float(np.abs((kin + pk32[tk]) - e_ex).max() /
+                                                    np.abs(e_ex).max())
+            rows.append(row)
+        summ = {"halos": len(rows), "np_range": [int(min(r["np"] for r in rows)),
+                                                 int(max(r["np"] for r in rows))]}
+        for key in ("fp32_vs_fp64", "fp32_vs_exact", "fp64_vs_exact", "energy_fp32_vs_exact"):
+            vals = np.array([r[key] for r in rows if key in r])
+            if vals.size:
+                summ[key] = {"p50": float(np.percentile(vals, 50)), "p99": float(np.percentile(vals, 99)),
+                             "max": float(vals.max())}
+        out[name] = summ
+    return out
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -457,6 +555,8 @@ def run_b200(args):
                   "fp32_vs_fp64_per_halo": (legs["fp32_batched"]["halos_per_s"] / base) if base else None,
                   "fp32_vs_fp64_batched": (legs["fp32_batched"]["halos_per_s"] /
                                            legs["fp64_batched"]["halos_per_s"])}
+        if d["regions"] is not None and rank == 0 and not args.no_errors:
+            unbind["errors"] = potential_error_report(d, args.seed)
 
     # end to end through the public API with pinned host buffers
     def pinned(a):
@@ -660,6 +760,8 @@ def main():
     ap.add_argument("--workload", default="fof_unbind_256", choices=sorted(WORKLOADS) + ["serve"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-errors", action="store_true",
+                    help="skip the per-halo potential error report of list workloads")
     ap.add_argument("--profile-run", action="store_true",
                     help="run only the warm-up and timed steps of the default path")
     args = ap.parse_args()
