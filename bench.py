@@ -110,6 +110,18 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def _tile_table_note():
+    """The tile table the library loaded (path relative to the repository and
+    a hash of its contents), or the built-in defaults."""
+    import hashlib
+    from py_fof_b200 import _native
+    p = _native.tile_table_used()
+    if not p:
+        return {"table": "built-in defaults"}
+    return {"table": os.path.relpath(p, ROOT),
+            "sha256_16": hashlib.sha256(open(p, "rb").read()).hexdigest()[:16]}
+
+
 def _traffic(workload, kernel):
     """DRAM bytes per algorithmic byte of `kernel`, from a committed ncu
     summary (profiles/roofline_traffic.json), or None."""
@@ -268,8 +280,8 @@ def cpu_baseline(workload, seed):
     return {"value": n / dt / 1e6, "unit": "Mpart/s", "cores": used, "kind": "port",
             "sample": f"{name}: {n} particles, {_sample_kind(name, workload)}, one call after one "
                       f"untimed call on {CPU_WARMUP[workload]}, reference thread policy "
-                      "(one region: 2 linking threads; unbinding one flat dynamic pool over "
-                      "candidates)"}
+                      "(one region: 2 linking threads; unbinding in the reference's grid-class "
+                      "groups, cost-ordered queues and phase/team split)"}
 
 
 def run_reference(args):
@@ -493,7 +505,10 @@ def run_b200(args):
                           | {"pm_fft_bytes": _native.get_stat("pm_fft_bytes")})
         return {key: sum(x[key] for x in st) / len(st) for key in st[0]}
 
-    # the product path: the library default (FP64 unbinding)
+    # the product path: the library default (FP64 unbinding); --fp32 selects
+    # the FP32 path for profiler runs
+    if args.profile_run and args.fp32:
+        _native.set_option("unbind_fp64", 0)
     for _ in range(max(args.warmup, 0)):
         step()
     torch.cuda.synchronize(dev)
@@ -649,6 +664,7 @@ def run_b200(args):
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,
+        "tile_table": _tile_table_note(),
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -762,6 +778,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-errors", action="store_true",
                     help="skip the per-halo potential error report of list workloads")
+    ap.add_argument("--fp32", action="store_true",
+                    help="with --profile-run: the FP32 unbinding path")
     ap.add_argument("--profile-run", action="store_true",
                     help="run only the warm-up and timed steps of the default path")
     args = ap.parse_args()

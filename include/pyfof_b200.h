@@ -68,6 +68,19 @@ int32_t pyfof_set_option(const char *key, int64_t value);
 /* Current value of a pyfof_set_option key.  No reference counterpart. */
 int32_t pyfof_get_option(const char *key, int64_t *value);
 
+/* Tile table: launch shapes that never change a result, tuned per device
+ * by py_fof_b200.autotune (the reference's counterpart is its per-group
+ * thread split, bound_fortran.f90:332-401).  Keys: "direct_threads" (index
+ * = halo-size bucket 0..5 for halos of at most 32, 64, 128, 256, 512, 1000
+ * members; value 32, 64, 128 or 256 threads per block of the
+ * direct-summation removal loop), "pm_batch" (index = PM grid size 48, 64,
+ * 128, 216 or 256; value = halos per convolution batch, 0 = as many as the
+ * batch memory budget allows), "conv_waves" (index = grid size; value 1..64
+ * = full GPU waves the fused z pass of a convolution is split into at
+ * least).  Invalid keys or values give ierr 1 with a message. */
+int32_t pyfof_set_tile(const char *key, int64_t index, int64_t value);
+int32_t pyfof_get_tile(const char *key, int64_t index, int64_t *value);
+
 /* Issue all later work of the selected device on `stream` (a cudaStream_t;
  * NULL restores the library's own stream).  Lets a caller order calls with
  * its own work and time them with events on that stream. */

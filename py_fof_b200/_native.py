@@ -44,7 +44,7 @@ def _units_ptr(units):
 
 # every symbol include/pyfof_b200.h declares
 EXPORTED = ("pyfof_version", "pyfof_init", "pyfof_shutdown", "pyfof_last_error",
-            "pyfof_set_option", "pyfof_get_option", "pyfof_set_stream", "pyfof_get_stat", "pyfof_last_link_ms", "pyfof_last_stage_ms",
+            "pyfof_set_option", "pyfof_get_option", "pyfof_set_tile", "pyfof_get_tile", "pyfof_set_stream", "pyfof_get_stat", "pyfof_last_link_ms", "pyfof_last_stage_ms",
             "pyfof_halo_potential", "pyfof_halo_potential_direct_static", "pyfof_run",
             "pyfof_run_device", "pyfof_slot_create", "pyfof_slot_destroy", "pyfof_slot_run",
             "pyfof_slot_stat", "pyfof_run_catalogue", "pyfof_run_units")
@@ -74,6 +74,10 @@ def load():
         L.pyfof_set_option.argtypes = [ctypes.c_char_p, ctypes.c_int64]
         L.pyfof_get_option.restype = ctypes.c_int32
         L.pyfof_get_option.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
+        L.pyfof_set_tile.restype = ctypes.c_int32
+        L.pyfof_set_tile.argtypes = [ctypes.c_char_p, ctypes.c_int64, ctypes.c_int64]
+        L.pyfof_get_tile.restype = ctypes.c_int32
+        L.pyfof_get_tile.argtypes = [ctypes.c_char_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
         L.pyfof_set_stream.restype = ctypes.c_int32
         L.pyfof_set_stream.argtypes = [ctypes.c_void_p]
         L.pyfof_get_stat.restype = ctypes.c_int32
@@ -113,7 +117,8 @@ def load():
         if v != ABI_VERSION:
             raise NativeLibraryError(f"ABI version mismatch: library {v}, binding {ABI_VERSION}")
         _lib = L
-        return L
+    apply_tile_table()
+    return L
 
 
 def last_error() -> str:
@@ -133,6 +138,87 @@ def get_option(key: str) -> int:
     if load().pyfof_get_option(key.encode(), ctypes.byref(v)) != 0:
         raise ValueError(last_error())
     return int(v.value)
+
+
+# the tile table the autotuner writes (py_fof_b200.autotune); the
+# environment variable PYFOF_TILE_TABLE names another file ("" = none)
+TILE_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tiles.json")
+TILE_KEYS = ("direct_threads", "pm_batch", "conv_waves")
+_tile_table_used = None
+
+
+def set_tile(key: str, index: int, value: int) -> None:
+    if load().pyfof_set_tile(key.encode(), int(index), int(value)) != 0:
+        raise ValueError(last_error())
+
+
+def get_tile(key: str, index: int) -> int:
+    v = ctypes.c_int64(0)
+    if load().pyfof_get_tile(key.encode(), int(index), ctypes.byref(v)) != 0:
+        raise ValueError(last_error())
+    return int(v.value)
+
+
+def read_tile_table(path):
+    """Entries [(key, index, value)] of a tile table file (JSON: {key:
+    {index: value}} for the keys of TILE_KEYS; other top-level keys are
+    notes).  Raises ValueError on a malformed table."""
+    import json
+    with open(path) as f:
+        d = json.load(f)
+    if not isinstance(d, dict):
+        raise ValueError(f"{path}: not a JSON object")
+    out = []
+    for key in TILE_KEYS:
+        ent = d.get(key, {})
+        if not isinstance(ent, dict):
+            raise ValueError(f"{path}: {key} must map indices to values")
+        for idx, val in ent.items():
+            out.append((key, int(idx), int(val)))
+    return out
+
+
+def apply_tile_table(path=None):
+    """Set the library's tile table from `path` (default: PYFOF_TILE_TABLE or
+    the package's tiles.json when present).  Returns the path used or None."""
+    global _tile_table_used
+    if path is None:
+        path = os.environ.get("PYFOF_TILE_TABLE", TILE_TABLE)
+    if not path or not os.path.exists(path):
+        return None
+    for key, idx, val in read_tile_table(path):
+        if _lib.pyfof_set_tile(key.encode(), idx, val) != 0:
+            raise ValueError(f"{path}: {last_error()}")
+    _tile_table_used = path
+    return path
+
+
+def tile_table_used():
+    load()
+    return _tile_table_used
+
+
+class tiles:
+    """Context manager: set tile-table entries, restore them after.
+
+        with _native.tiles(("direct_threads", 0, 32)):
+            ...
+    """
+
+    def __init__(self, *entries):
+        self.entries = entries
+        self.old = []
+
+    def __enter__(self):
+        for key, idx, val in self.entries:
+            self.old.append((key, idx, get_tile(key, idx)))
+            set_tile(key, idx, val)
+        return self
+
+    def __exit__(self, *exc):
+        for key, idx, val in reversed(self.old):
+            set_tile(key, idx, val)
+        return False
 
 
 class options:

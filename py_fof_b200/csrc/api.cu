@@ -23,6 +23,7 @@ int g_bound_fp64 = 1;  // FP64 unbinding by default: direct sums bit-exact with 
 int g_bound_per_halo = 0;
 int g_timing = 0;
 int64_t g_big_np = 0;
+TileTable g_tiles;
 int g_cell_order = 0;
 }  // namespace
 
@@ -185,6 +186,7 @@ static int32_t run_common(Context &ctx, FofArgs &a) {
   a.bound_fp64 = g_bound_fp64;
   a.bound_per_halo = g_bound_per_halo;
   a.big_np = g_big_np;
+  a.tiles = g_tiles;
   a.cell_order = g_cell_order;
   int32_t r = fof_run(ctx, a);
   note_alloc_failure(ctx, r);
@@ -253,6 +255,48 @@ int32_t pyfof_get_option(const char *key, int64_t *value) {
   if (!std::strcmp(key, "cell_order")) { *value = g_cell_order; return kOk; }
   set_error("unknown option %s", key);
   return kInvalid;
+}
+
+// Tile table entries: "direct_threads" (index = size bucket 0..5, value 32,
+// 64, 128 or 256), "pm_batch" (index = grid size n, value >= 0),
+// "conv_waves" (index = grid size n, value 1..64).
+static int *tile_slot(const char *key, int64_t index) {
+  if (!key) return nullptr;
+  if (!std::strcmp(key, "direct_threads"))
+    return (index >= 0 && index < 6) ? &g_tiles.direct_threads[index] : nullptr;
+  const int gi = kGridIndex((int)index);
+  if (gi < 0 || index > 256) return nullptr;
+  if (!std::strcmp(key, "pm_batch")) return &g_tiles.pm_batch[gi];
+  if (!std::strcmp(key, "conv_waves")) return &g_tiles.conv_waves[gi];
+  return nullptr;
+}
+
+int32_t pyfof_set_tile(const char *key, int64_t index, int64_t value) {
+  int *slot = tile_slot(key, index);
+  if (!slot) {
+    set_error("unknown tile entry %s[%lld]", key ? key : "(null)", (long long)index);
+    return kInvalid;
+  }
+  bool ok;
+  if (!std::strcmp(key, "direct_threads")) ok = value == 32 || value == 64 || value == 128 || value == 256;
+  else if (!std::strcmp(key, "pm_batch")) ok = value >= 0 && value <= (1 << 20);
+  else ok = value >= 1 && value <= 64;
+  if (!ok) {
+    set_error("tile entry %s[%lld] out of range: %lld", key, (long long)index, (long long)value);
+    return kInvalid;
+  }
+  *slot = (int)value;
+  return kOk;
+}
+
+int32_t pyfof_get_tile(const char *key, int64_t index, int64_t *value) {
+  int *slot = tile_slot(key, index);
+  if (!slot || !value) {
+    set_error("unknown tile entry %s[%lld]", key ? key : "(null)", (long long)index);
+    return kInvalid;
+  }
+  *value = *slot;
+  return kOk;
 }
 
 int32_t pyfof_set_stream(void *stream) {
@@ -417,6 +461,7 @@ static int32_t run_host(Context &ctx, const double *xp, const double *vp, const 
   a.bound_fp64 = g_bound_fp64;
   a.bound_per_halo = g_bound_per_halo;
   a.big_np = g_big_np;
+  a.tiles = g_tiles;
   a.cell_order = g_cell_order;
   int32_t r = fof_run(ctx, a);
   if (r == kOk && cat) r = build_catalogue(ctx, a.halo_id, (int64_t)n, cat->members, cat->offsets, cat->cap,

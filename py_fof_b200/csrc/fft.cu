@@ -595,7 +595,7 @@ int32_t prepare() {
 
 template <typename R, int N>
 int32_t convolve_n(R *rho, cplx_t<R> *spec, const R *green, int sup, int batch, cudaStream_t s,
-                   const unsigned long long *acc, const double *inv_scale) {
+                   const unsigned long long *acc, const double *inv_scale, int waves) {
   PYFOF_TRY((prepare<R, N>()));
   constexpr int W = kW<R>, T = Cfg<R, N>::T;
   const int nhp = (int)spec_row<R>(N);
@@ -615,7 +615,7 @@ int32_t convolve_n(R *rho, cplx_t<R> *spec, const R *green, int sup, int batch, 
       spec, nullptr, bstride, (int64_t)N * nhp, nhp, sup, ntiles, 1, batch, sup, N);
   PYFOF_CHECK_LAUNCH();
   // z: forward, Green, inverse; lines (kx, ky), input and output z < sup;
-  // halos split into chunks so that the grid is at least four full waves
+  // halos split into chunks so that the grid is at least `waves` full waves
   const int64_t per = (int64_t)ntiles * N;
   static int conv_blocks_per_sm = 0;
   if (!conv_blocks_per_sm) {
@@ -626,7 +626,7 @@ int32_t convolve_n(R *rho, cplx_t<R> *spec, const R *green, int sup, int batch, 
     conv_blocks_per_sm = b;
   }
   const int64_t slots = (int64_t)conv_blocks_per_sm * kNumSMs;
-  const int nchunk = (int)std::max<int64_t>(1, std::min<int64_t>(batch, ceil_div(4 * slots, per)));
+  const int nchunk = (int)std::max<int64_t>(1, std::min<int64_t>(batch, ceil_div((int64_t)waves * slots, per)));
   const int nbb = (int)ceil_div(batch, nchunk);
   const int nchunk_used = (int)ceil_div(batch, nbb);
   k_lines<R, N, -1, true><<<(unsigned)(per * nchunk_used), T, smem_conv_bytes<R, N>(), s>>>(
@@ -670,17 +670,17 @@ int32_t c2r_full_n(const R *green, cplx_t<R> *spec, R *out, cudaStream_t s) {
 
 template <typename R>
 int32_t pm_convolve_batch(R *rho, cplx_t<R> *spec, const R *green, int n, int sup, int batch,
-                          cudaStream_t s, const unsigned long long *acc, const double *inv_scale) {
+                          cudaStream_t s, const unsigned long long *acc, const double *inv_scale, int waves) {
   if (sup != n / 2 + 1 || batch < 1 || (int64_t)batch * sup * sup >= (int64_t)1 << 30) {
     set_error("invalid convolution batch (n %d, support %d, batch %d)", n, sup, batch);
     return kInvalid;
   }
   switch (n) {
-    case 48: return convolve_n<R, 48>(rho, spec, green, sup, batch, s, acc, inv_scale);
-    case 64: return convolve_n<R, 64>(rho, spec, green, sup, batch, s, acc, inv_scale);
-    case 128: return convolve_n<R, 128>(rho, spec, green, sup, batch, s, acc, inv_scale);
-    case 216: return convolve_n<R, 216>(rho, spec, green, sup, batch, s, acc, inv_scale);
-    case 256: return convolve_n<R, 256>(rho, spec, green, sup, batch, s, acc, inv_scale);
+    case 48: return convolve_n<R, 48>(rho, spec, green, sup, batch, s, acc, inv_scale, waves);
+    case 64: return convolve_n<R, 64>(rho, spec, green, sup, batch, s, acc, inv_scale, waves);
+    case 128: return convolve_n<R, 128>(rho, spec, green, sup, batch, s, acc, inv_scale, waves);
+    case 216: return convolve_n<R, 216>(rho, spec, green, sup, batch, s, acc, inv_scale, waves);
+    case 256: return convolve_n<R, 256>(rho, spec, green, sup, batch, s, acc, inv_scale, waves);
     default: set_error("unsupported FFT size %d", n); return kInvalid;
   }
 }
@@ -698,9 +698,9 @@ int32_t c2r_full(const R *green, cplx_t<R> *spec, R *out, int n, cudaStream_t s)
 }
 
 template int32_t pm_convolve_batch<float>(float *, float2 *, const float *, int, int, int, cudaStream_t,
-                                          const unsigned long long *, const double *);
+                                          const unsigned long long *, const double *, int);
 template int32_t pm_convolve_batch<double>(double *, double2 *, const double *, int, int, int, cudaStream_t,
-                                           const unsigned long long *, const double *);
+                                           const unsigned long long *, const double *, int);
 template int32_t c2r_full<float>(const float *, float2 *, float *, int, cudaStream_t);
 template int32_t c2r_full<double>(const double *, double2 *, double *, int, cudaStream_t);
 

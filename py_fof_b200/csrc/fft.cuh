@@ -46,10 +46,12 @@ constexpr int64_t spec_elems(int n) {
 //   acc, inv_scale (optional): the density as 64-bit fixed-point cubes
 //         (value of grid b = acc * inv_scale[b]) read in place of rho; the
 //         output still goes to rho, which may alias acc
+//   waves the fused z pass splits the batch so that its grid covers at
+//         least this many full waves of the GPU (a launch shape only)
 template <typename R>
 int32_t pm_convolve_batch(R *rho, cplx_t<R> *spec, const R *green, int n, int sup, int batch,
                           cudaStream_t s, const unsigned long long *acc = nullptr,
-                          const double *inv_scale = nullptr);
+                          const double *inv_scale = nullptr, int waves = 4);
 
 // FFTW-style c2r of a real half-spectrum table (the Green's function) into a
 // full n^3 real grid (unnormalised); used once per table to extract the

@@ -35,7 +35,7 @@ namespace pyfof {
 
 namespace {
 
-constexpr int TILE = 8192;
+constexpr int TILE = 4096;  // particles per block of the bbox and key kernels (16 per thread)
 constexpr int BLK = 256;
 
 __device__ __forceinline__ int region_of_key(const uint64_t *cell_off, int nreg, uint64_t key) {

@@ -5,6 +5,23 @@
 
 namespace pyfof {
 
+// Launch shapes that never change a result (set from the tile table the
+// autotuner writes; pyfof_set_tile).  Index of a grid size n in the
+// per-grid arrays: kGridIndex(n).
+struct TileTable {
+  // threads per block of the direct-summation removal loop for halos of at
+  // most 32, 64, 128, 256, 512, 1000 members
+  int direct_threads[6] = {64, 64, 128, 128, 256, 256};
+  // halos per particle-mesh convolution batch for n = 48, 64, 128, 216,
+  // 256 (0: as many as the batch memory budget allows)
+  int pm_batch[5] = {0, 0, 0, 0, 0};
+  // the fused z pass of the convolution splits a batch so that its grid
+  // covers at least this many full waves of the GPU
+  int conv_waves[5] = {4, 4, 4, 4, 4};
+};
+inline int kGridIndex(int n) { return n == 48 ? 0 : n == 64 ? 1 : n == 128 ? 2 : n == 216 ? 3 : n == 256 ? 4 : -1; }
+constexpr int kDirectBucketEdge[6] = {32, 64, 128, 256, 512, 1000};
+
 // Arguments of one fof_fortran-equivalent call (fof_fortran.f90:10-58).
 // All particle arrays are device pointers.
 struct FofArgs {
@@ -25,6 +42,7 @@ struct FofArgs {
   int32_t bound_per_halo = 0;  // 1: FP64, one halo per launch sequence (the plain baseline)
   int64_t big_np = 0;          // PM halos above this many members use the chunked removal loop (0: default)
   int32_t cell_order = 0;      // 0: by key width, 1: per-cell sorts where cells allow, 2: radix sort
+  TileTable tiles;
   // masses are divided by m_div right after their check (code units); only
   // with mp in the library's own scratch, which the check then rewrites
   double m_div = 1.0;

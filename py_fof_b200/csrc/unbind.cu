@@ -320,6 +320,36 @@ bool GridRules::select(int64_t np, double span, int &gid, int &lev, double &sp) 
 
 // ------------------------------------------------------------ stage
 
+// The direct-summation removal loop over `nb` halos of at most `cap`
+// members, with `threads` threads per block.
+template <bool FP64, int NT>
+static int32_t launch_direct_nt(unsigned nb, int cap, const Members &m, const int64_t *off, const int32_t *list,
+                                const direct::DirectParams &P, HaloResult *res, uint8_t *keep, float *phi_out,
+                                int32_t *flags, const double *phi1, cudaStream_t s) {
+  const size_t smem = direct::direct_smem(cap);
+  PYFOF_CUDA(cudaFuncSetAttribute(direct::ub_direct_kernel<FP64, NT>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  direct::ub_direct_kernel<FP64, NT><<<nb, NT, smem, s>>>(m, off, list, P, res, keep, phi_out, flags, phi1, cap);
+  PYFOF_CHECK_LAUNCH();
+  return kOk;
+}
+
+static int32_t launch_direct_loop(bool fp64, int threads, unsigned nb, int cap, const Members &m,
+                                  const int64_t *off, const int32_t *list, const direct::DirectParams &P,
+                                  HaloResult *res, uint8_t *keep, float *phi_out, int32_t *flags,
+                                  const double *phi1, cudaStream_t s) {
+#define PYFOF_DIRECT_NT(NT)                                                                           \
+  return fp64 ? launch_direct_nt<true, NT>(nb, cap, m, off, list, P, res, keep, phi_out, flags, phi1, s) \
+              : launch_direct_nt<false, NT>(nb, cap, m, off, list, P, res, keep, phi_out, flags, phi1, s)
+  switch (threads) {
+    case 32: PYFOF_DIRECT_NT(32);
+    case 64: PYFOF_DIRECT_NT(64);
+    case 128: PYFOF_DIRECT_NT(128);
+    default: PYFOF_DIRECT_NT(256);
+  }
+#undef PYFOF_DIRECT_NT
+}
+
 int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
   cudaStream_t s = ctx.stream;
   Arena &W = ctx.work;
@@ -448,16 +478,41 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
         PYFOF_CHECK_LAUNCH();
         PYFOF_CUDA(cudaStreamSynchronize(s));
       }
-    } else if (a.bound_fp64) {
-      PYFOF_CUDA(cudaFuncSetAttribute(direct::ub_direct_kernel<true>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      direct::ub_direct_kernel<true><<<(unsigned)direct.size(), BLK, smem, s>>>(m, off, dl, P, res, keep,
-                                                                         st.phi_out, ctx.d_flags);
     } else {
-      PYFOF_CUDA(cudaFuncSetAttribute(direct::ub_direct_kernel<false>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      direct::ub_direct_kernel<false><<<(unsigned)direct.size(), BLK, smem, s>>>(m, off, dl, P, res, keep,
-                                                                          st.phi_out, ctx.d_flags);
+      // first-pass potentials flat over (halo, 64-target tile), then the
+      // removal loops, one block per halo, launched per halo-size bucket
+      // with the tile table's block size and shared memory for the bucket's
+      // largest halo
+      std::vector<int2> tl;
+      for (size_t e = 0; e < direct.size(); ++e)
+        for (int t0 = 0; t0 < tasks[direct[e]].np; t0 += direct::PT) tl.push_back(make_int2((int)e, t0));
+      int2 *dtl = W.carve<int2>(tl.size());
+      double *phi1 = W.carve<double>((size_t)std::max<int64_t>(M, 1));
+      int32_t *dbl = W.carve<int32_t>(direct.size());
+      if (!dtl || !phi1 || !dbl) { set_error("workspace exhausted (direct potentials)"); return kAlloc; }
+      PYFOF_CUDA(cudaMemcpyAsync(dtl, tl.data(), sizeof(int2) * tl.size(), cudaMemcpyHostToDevice, s));
+      if (a.bound_fp64)
+        direct::ub_direct_phi1_kernel<true><<<(unsigned)tl.size(), direct::PT, 0, s>>>(m, off, dl, dtl, P, phi1);
+      else
+        direct::ub_direct_phi1_kernel<false><<<(unsigned)tl.size(), direct::PT, 0, s>>>(m, off, dl, dtl, P, phi1);
+      PYFOF_CHECK_LAUNCH();
+      std::vector<int32_t> bl;
+      std::vector<size_t> bstart(7, 0);
+      for (int b = 0; b < 6; ++b) {
+        for (int32_t c : direct) {
+          const int np = tasks[c].np;
+          if (np <= kDirectBucketEdge[b] && (b == 0 || np > kDirectBucketEdge[b - 1])) bl.push_back(c);
+        }
+        bstart[b + 1] = bl.size();
+      }
+      PYFOF_CUDA(cudaMemcpyAsync(dbl, bl.data(), sizeof(int32_t) * bl.size(), cudaMemcpyHostToDevice, s));
+      for (int b = 0; b < 6; ++b) {
+        const unsigned nb = (unsigned)(bstart[b + 1] - bstart[b]);
+        if (!nb) continue;
+        const int cap = (kDirectBucketEdge[b] + 31) / 32 * 32;
+        PYFOF_TRY(launch_direct_loop(a.bound_fp64 != 0, a.tiles.direct_threads[b], nb, cap, m, off,
+                                     dbl + bstart[b], P, res, keep, st.phi_out, ctx.d_flags, phi1, s));
+      }
     }
     PYFOF_CHECK_LAUNCH();
   }

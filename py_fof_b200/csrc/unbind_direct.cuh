@@ -65,17 +65,6 @@ struct Kahan {
   }
 };
 
-__device__ __forceinline__ double block_sum_d(double v, double *red) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  __syncthreads();
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  double t = 0.0;
-  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-  return t;
-}
-
 __device__ __forceinline__ int block_sum_i(int v, int *red) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -95,34 +84,115 @@ struct DirectParams {
   int phi_only;   // stop after the first potential
 };
 
-// One block per halo: bound_check_grid for gid 0 (:2611-2864).  FP64=true
-// is the plain FP64 path, bit-exact with the reference arithmetic; FP64=false
-// the FP32 product path with compensated sums.
+// Sources j0 .. j0+cnt-1 (staged at sx[0..cnt)) of a target's first-pass
+// potential, in ascending index, skipping the target itself: the
+// reference's accumulation order (bound_fortran.f90:2619-2640; its i<j loop
+// adds each pair term to both ends, so every target sums its sources in
+// ascending order) and the same operations as the in-kernel first pass of
+// ub_direct_kernel.
 template <bool FP64>
-__global__ void __launch_bounds__(BLK) ub_direct_kernel(Members m, const int64_t *__restrict__ off,
-                                                        const int32_t *__restrict__ list,
-                                                        DirectParams P, HaloResult *__restrict__ res,
-                                                        uint8_t *__restrict__ keep_out,
-                                                        float *__restrict__ phi_out,
-                                                        int32_t *flags) {
+__device__ __forceinline__ void phi1_sources(const float *sx, const float *sy, const float *sz,
+                                             const float *sw, int j0, int cnt, int i, float xi, float yi,
+                                             float zi, const DirectParams &P, double &acc64, Kahan &acc32,
+                                             float h32, float inv_h, float inv70h) {
+  for (int k = 0; k < cnt; ++k) {
+    if (j0 + k == i) continue;
+    if (FP64) {
+      const double dx = (double)__fsub_rn(sx[k], xi);
+      const double dy = (double)__fsub_rn(sy[k], yi);
+      const double dz = (double)__fsub_rn(sz[k], zi);
+      const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
+                                            __dmul_rn(dz, dz)));
+      const double dd = __dmul_rn(P.fac, depth_continuous<double>(r, P.app));
+      acc64 = __dadd_rn(acc64, -__dmul_rn((double)sw[k], dd));
+    } else {
+      const float dx = sx[k] - xi, dy = sy[k] - yi, dz = sz[k] - zi;
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      acc32.add(-sw[k] * depth_f32(r2, h32, inv_h, inv70h));
+    }
+  }
+}
+
+// The first-pass potentials of many direct-summation halos, spread over
+// the whole GPU: block b takes the PT targets tiles[b] = (entry of list,
+// first target) of one halo and streams the halo's members through shared
+// memory in ascending order.  Each target's sum has exactly the order and
+// operations of the in-kernel first pass of ub_direct_kernel, so the
+// results are the same bits; the removal loop then starts from phi1.
+constexpr int PT = 64;
+template <bool FP64>
+__global__ void __launch_bounds__(PT) ub_direct_phi1_kernel(Members m, const int64_t *__restrict__ off,
+                                                            const int32_t *__restrict__ list,
+                                                            const int2 *__restrict__ tiles, DirectParams P,
+                                                            double *__restrict__ phi1) {
+  __shared__ float sx[PT], sy[PT], sz[PT], sw[PT];
+  const int2 t = tiles[blockIdx.x];
+  const int c = list[t.x];
+  const int64_t b0 = off[c];
+  const int np = (int)(off[c + 1] - b0);
+  const int i = t.y + threadIdx.x;
+  const bool act = i < np;
+  const float xi = act ? m.q[0][b0 + i] : 0.f, yi = act ? m.q[1][b0 + i] : 0.f,
+              zi = act ? m.q[2][b0 + i] : 0.f;
+  const float h32 = (float)P.app, inv_h = (float)(1.0 / P.app), inv70h = (float)(1.0 / (70.0 * P.app));
+  double acc64 = 0.0;
+  Kahan acc32;
+  for (int j0 = 0; j0 < np; j0 += PT) {
+    const int j = j0 + threadIdx.x;
+    if (j < np) {
+      sx[threadIdx.x] = m.q[0][b0 + j];
+      sy[threadIdx.x] = m.q[1][b0 + j];
+      sz[threadIdx.x] = m.q[2][b0 + j];
+      sw[threadIdx.x] = m.w[b0 + j];
+    }
+    __syncthreads();
+    if (act)
+      phi1_sources<FP64>(sx, sy, sz, sw, j0, min(PT, np - j0), i, xi, yi, zi, P, acc64, acc32, h32, inv_h,
+                         inv70h);
+    __syncthreads();
+  }
+  if (act) phi1[b0 + i] = FP64 ? acc64 : (double)((float)P.fac * acc32.s);
+}
+
+// Dynamic shared memory of ub_direct_kernel for halos of up to cap members
+// (cap a multiple of 32): nine float and two int arrays, one double array
+// and the keep flags.
+__host__ __device__ constexpr size_t direct_smem(int cap) { return (size_t)cap * (11 * 4 + 8 + 1); }
+
+// One block of NT threads per halo: bound_check_grid for gid 0
+// (:2611-2864).  FP64=true is the plain FP64 path, bit-exact with the
+// reference arithmetic; FP64=false the FP32 product path with compensated
+// sums.  phi1 (optional): the first-pass potentials from
+// ub_direct_phi1_kernel; null computes them here.  Every halo of the launch
+// has at most cap members.  No result depends on NT: every sum runs in an
+// order fixed by the member indices alone (per-target serial sums, the
+// FP64 centre sums in thread 0, the FP32 ones in warp 0 by index mod 32).
+template <bool FP64, int NT = BLK>
+__global__ void __launch_bounds__(NT) ub_direct_kernel(Members m, const int64_t *__restrict__ off,
+                                                       const int32_t *__restrict__ list,
+                                                       DirectParams P, HaloResult *__restrict__ res,
+                                                       uint8_t *__restrict__ keep_out,
+                                                       float *__restrict__ phi_out,
+                                                       int32_t *flags,
+                                                       const double *__restrict__ phi1 = nullptr,
+                                                       int cap = kDirectMax) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int c = list[blockIdx.x];
   const int64_t b0 = off[c];
   const int np = (int)(off[c + 1] - b0);
   float *qx = reinterpret_cast<float *>(smem);
-  float *qy = qx + kDirectMax, *qz = qy + kDirectMax;
-  float *vx = qz + kDirectMax, *vy = vx + kDirectMax, *vz = vy + kDirectMax;
-  float *w = vz + kDirectMax, *phi = w + kDirectMax, *en = phi + kDirectMax;
-  int *jdel = reinterpret_cast<int *>(en + kDirectMax);
-  int *unb = jdel + kDirectMax;
-  double *phid = reinterpret_cast<double *>(unb + kDirectMax);
-  unsigned char *keep = reinterpret_cast<unsigned char *>(phid + kDirectMax);
-  __shared__ double red_d[BLK / 32];
-  __shared__ int red_i[BLK / 32];
+  float *qy = qx + cap, *qz = qy + cap;
+  float *vx = qz + cap, *vy = vx + cap, *vz = vy + cap;
+  float *w = vz + cap, *phi = w + cap, *en = phi + cap;
+  int *jdel = reinterpret_cast<int *>(en + cap);
+  int *unb = jdel + cap;
+  double *phid = reinterpret_cast<double *>(unb + cap);
+  unsigned char *keep = reinterpret_cast<unsigned char *>(phid + cap);
+  __shared__ int red_i[NT / 32];
   __shared__ double s_qc[3], s_vc[3];
   __shared__ int s_nu, s_err;
 
-  for (int i = threadIdx.x; i < np; i += BLK) {
+  for (int i = threadIdx.x; i < np; i += NT) {
     const int64_t k = b0 + i;
     qx[i] = m.q[0][k]; qy[i] = m.q[1][k]; qz[i] = m.q[2][k];
     vx[i] = m.v[0][k]; vy[i] = m.v[1][k]; vz[i] = m.v[2][k];
@@ -138,12 +208,14 @@ __global__ void __launch_bounds__(BLK) ub_direct_kernel(Members m, const int64_t
 
   for (int pass = 1; pass <= kMaxPasses; ++pass) {
     int ks = 0;
-    for (int i = threadIdx.x; i < np; i += BLK) ks += keep[i];
+    for (int i = threadIdx.x; i < np; i += NT) ks += keep[i];
     const int n_source = block_sum_i(ks, red_i);
     // potential: full sum on the first pass, later passes add back the
     // sources removed since the previous refresh
-    for (int i = threadIdx.x; i < np; i += BLK) {
-      if (pass == 1) {
+    for (int i = threadIdx.x; i < np; i += NT) {
+      if (pass == 1 && phi1) {
+        phid[i] = phi1[b0 + i];
+      } else if (pass == 1) {
         if (FP64) {
           double acc = 0.0;
           for (int j = 0; j < np; ++j) {
@@ -196,7 +268,7 @@ __global__ void __launch_bounds__(BLK) ub_direct_kernel(Members m, const int64_t
     }
     njd = 0;
     __syncthreads();
-    for (int i = threadIdx.x; i < np; i += BLK) {
+    for (int i = threadIdx.x; i < np; i += NT) {
       if (!keep[i]) continue;
       float v = FP64 ? __double2float_rn(phid[i]) : (float)phid[i];
       if (np_bound == 1 || n_source == 1) v = 0.0f;
@@ -226,16 +298,18 @@ __global__ void __launch_bounds__(BLK) ub_direct_kernel(Members m, const int64_t
           s_qc[0] = __ddiv_rn(q0, ws); s_qc[1] = __ddiv_rn(q1, ws); s_qc[2] = __ddiv_rn(q2, ws);
           s_vc[0] = __ddiv_rn(v0, ws); s_vc[1] = __ddiv_rn(v1, ws); s_vc[2] = __ddiv_rn(v2, ws);
         }
-      } else {
+      } else if (threadIdx.x < 32) {
+        // warp 0: lane l sums the members l, l+32, ...; then a butterfly
         double a[7] = {0, 0, 0, 0, 0, 0, 0};
-        for (int i = threadIdx.x; i < np; i += BLK) {
+        for (int i = threadIdx.x; i < np; i += 32) {
           if (!keep[i]) continue;
           const double wi = (double)w[i];
           a[0] += wi;
           a[1] += wi * qx[i]; a[2] += wi * qy[i]; a[3] += wi * qz[i];
           a[4] += wi * vx[i]; a[5] += wi * vy[i]; a[6] += wi * vz[i];
         }
-        for (int k = 0; k < 7; ++k) a[k] = block_sum_d(a[k], red_d);
+        for (int k = 0; k < 7; ++k)
+          for (int o = 16; o > 0; o >>= 1) a[k] += __shfl_xor_sync(0xffffffffu, a[k], o);
         if (threadIdx.x == 0) {
           for (int d = 0; d < 3; ++d) { s_qc[d] = a[1 + d] / a[0]; s_vc[d] = a[4 + d] / a[0]; }
         }
@@ -247,7 +321,7 @@ __global__ void __launch_bounds__(BLK) ub_direct_kernel(Members m, const int64_t
       const float vc0 = __double2float_rn(s_vc[0]), vc1 = __double2float_rn(s_vc[1]),
                   vc2 = __double2float_rn(s_vc[2]);
       // specific energies (bound_fortran.f90:2773-2786), FP32
-      for (int i = threadIdx.x; i < np; i += BLK) {
+      for (int i = threadIdx.x; i < np; i += NT) {
         if (!keep[i]) continue;
         const float d0 = __fadd_rn(__fsub_rn(vx[i], vc0), __fmul_rn(P.b, __fsub_rn(qx[i], qc0)));
         const float d1 = __fadd_rn(__fsub_rn(vy[i], vc1), __fmul_rn(P.b, __fsub_rn(qy[i], qc1)));
@@ -272,7 +346,7 @@ __global__ void __launch_bounds__(BLK) ub_direct_kernel(Members m, const int64_t
       int nb = (int)ceil(0.02 * (double)np_bound);
       nb = max(1, nb);
       nb = min(nu, nb);
-      for (int t = threadIdx.x; t < nu; t += BLK) {
+      for (int t = threadIdx.x; t < nu; t += NT) {
         const int i = unb[t];
         const float ei = en[i];
         int rank = 0;
@@ -301,7 +375,7 @@ __global__ void __launch_bounds__(BLK) ub_direct_kernel(Members m, const int64_t
     if (threadIdx.x == 0) atomicCAS(&flags[FLAG_ERR], 0, s_err);
     return;
   }
-  for (int i = threadIdx.x; i < np; i += BLK) {
+  for (int i = threadIdx.x; i < np; i += NT) {
     keep_out[b0 + i] = keep[i];
     if (phi_out) phi_out[b0 + i] = phi[i];
   }

@@ -383,56 +383,34 @@ __device__ __forceinline__ int seg_of(const uint32_t *__restrict__ off, int n, u
 }
 
 // Deposit of the kept members of a batch of halos (batch[j] = halo of
-// grid j, bpre = prefix of their member counts, bsrc[j] = first position of
-// halo j in cmem, the members sorted by short-range cell and a Morton
-// sub-key).  A warp takes 32 consecutive members of that spatial order;
-// lanes whose TSC stencils start at the same node add their contributions
-// with warp reductions first (exact integer sums), and one lane per stencil
-// node issues the atomic.
+// grid j, bpre = prefix of their member counts), flat over the batch's
+// members in their stored order (coalesced member reads).  Each of a
+// member's 27 contributions is one 64-bit integer atomic add.
 __global__ void __launch_bounds__(BLK) pm_deposit_kernel(const Members m, const PmHalo *__restrict__ H,
                                                          const int32_t *__restrict__ batch,
-                                                         const uint32_t *__restrict__ bpre,
-                                                         const uint32_t *__restrict__ bsrc, int nb,
-                                                         const uint32_t *__restrict__ cmem,
+                                                         const uint32_t *__restrict__ bpre, int nb,
                                                          const uint8_t *__restrict__ keep,
                                                          const int3 *__restrict__ first,
                                                          const float *__restrict__ wt, int sup,
                                                          unsigned long long *__restrict__ acc) {
   const uint32_t total = bpre[nb];
-  const int lane = threadIdx.x & 31;
-  const uint32_t stride = ((gridDim.x * blockDim.x) >> 5) << 5;
   const int64_t sup3 = (int64_t)sup * sup * sup;
-  for (uint32_t i0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) << 5; i0 < total; i0 += stride) {
-    const uint32_t idx = i0 + lane;
-    bool ok = idx < total;
-    int j = 0;
-    int64_t k = 0;
-    if (ok) {
-      j = seg_of(bpre, nb, idx);
-      k = cmem[bsrc[j] + (idx - bpre[j])];
-      ok = keep[k] != 0;
-    }
-    const unsigned act = __ballot_sync(0xffffffffu, ok);
-    if (!ok) continue;
-    const double sc = scalbn(1.0, 61 - fx_exp(H[batch[j]].mkeep));
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    const int j = seg_of(bpre, nb, idx);
+    const PmHalo &p = H[batch[j]];
+    const int64_t k = p.off + (idx - bpre[j]);
+    if (!keep[k]) continue;
+    const double sc = scalbn(1.0, 61 - fx_exp(p.mkeep));
     const int3 f = first[k];
     const float *w9 = wt + 9 * k;
     const float wk = m.w[k];
-    const uint64_t base = (uint64_t)j * sup3 + ((uint64_t)(f.z - 1) * sup + (f.y - 1)) * sup + (f.x - 1);
-    const unsigned grp = __match_any_sync(act, base);
-    const bool leader = (__ffs(grp) - 1) == lane;
+    unsigned long long *g = acc + (int64_t)j * sup3;
     for (int sz = 0; sz < 3; ++sz)
       for (int sy = 0; sy < 3; ++sy)
         for (int sx = 0; sx < 3; ++sx) {
           const float v = __fmul_rn(__fmul_rn(__fmul_rn(wk, w9[sx]), w9[3 + sy]), w9[6 + sz]);
-          const unsigned long long q = fx_quantum(v, sc);
-          // q < 2^62: three 21-bit pieces, each group sum below 2^26
-          const unsigned s0 = __reduce_add_sync(grp, (unsigned)(q & 0x1FFFFFull));
-          const unsigned s1 = __reduce_add_sync(grp, (unsigned)((q >> 21) & 0x1FFFFFull));
-          const unsigned s2 = __reduce_add_sync(grp, (unsigned)(q >> 42));
-          if (leader)
-            atomicAdd(&acc[base + ((uint64_t)sz * sup + sy) * sup + sx],
-                      (unsigned long long)s0 + ((unsigned long long)s1 << 21) + ((unsigned long long)s2 << 42));
+          atomicAdd(&g[((int64_t)(f.z + sz - 1) * sup + (f.y + sy - 1)) * sup + (f.x + sx - 1)],
+                    fx_quantum(v, sc));
         }
   }
 }
@@ -536,6 +514,37 @@ __device__ __forceinline__ float depth_fast(float r, float rinv, const DepthCons
   return (128.0f - prim) * c.inv70h;
 }
 
+// FP64 path of the same kernel without divisions: 1/r from an FP32
+// reciprocal square root seed refined by two Newton-Raphson steps in FP64,
+// y <- y (3/2 - r2 y^2 / 2), which square the relative error each time
+// (2^-22 -> ~1e-13 -> a few FP64 ulps); the per-h constants are FP64
+// reciprocals.  For r2 outside the FP32 normal range the caller keeps the
+// plain sqrt/division form.
+struct DepthConst64 {
+  double h, two_over_h, inv70h, six_h;
+};
+__device__ __forceinline__ DepthConst64 depth_const64(double h) {
+  return DepthConst64{h, 2.0 / h, 1.0 / (70.0 * h), 6.0 * h};
+}
+__device__ __forceinline__ double rsqrt_nr64(double r2) {
+  double y = (double)rsqrtf((float)r2);
+  const double hr2 = 0.5 * r2;
+  y = y * (1.5 - hr2 * y * y);
+  y = y * (1.5 - hr2 * y * y);
+  return y;
+}
+__device__ __forceinline__ double depth_fast64(double r, double rinv, const DepthConst64 &c) {
+  if (r >= c.h) return rinv;
+  const double e = r * c.two_over_h;
+  if (e <= 1.0) {
+    const double prim = e * e * (112.0 + e * e * (-56.0 + e * (14.0 + e * (8.0 - 3.0 * e))));
+    return (208.0 - prim) * c.inv70h;
+  }
+  const double prim = e * e * (448.0 + e * (-280.0 + e * (56.0 + e * (14.0 + e * (-8.0 + e))))) -
+                      224.0 * e - c.six_h * rinv;
+  return (128.0 - prim) * c.inv70h;
+}
+
 struct SrChunk {
   uint32_t cell, e0;
 };
@@ -592,6 +601,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) sr_gather_kernel(
     const R fac = (R)(a_val / (6.0 * kPi));
     const bool tl = p.two_level != 0;
     const DepthConst k_eps = depth_const((float)eps), k_ai = depth_const((float)ai);
+    const DepthConst64 k64_eps = depth_const64((double)eps), k64_ai = depth_const64((double)ai);
     R acc = 0, comp = 0;
     // The (2kk+1)^3 neighbour cells, 32 at a time: a lane loads one cell's
     // source range, the ranges are concatenated by a warp prefix sum and
@@ -666,6 +676,9 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) sr_gather_kernel(
               if constexpr (sizeof(R) == 4) {
                 const float rinv = rsqrtf(r2), d = r2 * rinv;
                 dphi = -(fac * (depth_fast(d, rinv, k_eps) - depth_fast(d, rinv, k_ai)));
+              } else if (r2 > 1e-30 && r2 < 1e30) {
+                const double rinv = rsqrt_nr64(r2), d = r2 * rinv;
+                dphi = -(fac * (depth_fast64(d, rinv, k64_eps) - depth_fast64(d, rinv, k64_ai)));
               } else {
                 const R d = sqrt(r2);
                 dphi = -(fac * (depth_c<R>(d, eps) - depth_c<R>(d, ai)));
@@ -1839,7 +1852,12 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
     return round256(sizeof(unsigned long long) * nb * sup * sup * sup) +
            sizeof(cplx_t<R>) * (size_t)nb * spec_elems<R>(n);
   };
-  auto max_batch = [&](int n) { return (int)std::max<size_t>(1, budget / batch_bytes(n, 1)); };
+  auto max_batch = [&](int n) {
+    const int by_budget = (int)std::max<size_t>(1, budget / batch_bytes(n, 1));
+    const int cap = a.tiles.pm_batch[kGridIndex(n)];
+    return cap > 0 ? std::min(cap, by_budget) : by_budget;
+  };
+  auto waves = [&](int n) { return a.tiles.conv_waves[kGridIndex(n)]; };
   size_t scratch_bytes = 256;
   for (int n : {48, 64, 128, 256}) {
     int cnt = 0;
@@ -1857,16 +1875,11 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
   const int nbat = std::max(std::max(na, nh), 1);
   int32_t *dbatch = W.carve<int32_t>(nbat);
   uint32_t *dbpre = W.carve<uint32_t>(2 * (size_t)(nbat + 1));
-  uint32_t *dbsrc = W.carve<uint32_t>(nbat);
   double *dinv = W.carve<double>(nbat);
-  if (!scratch || !dpend || !dbatch || !dbpre || !dbsrc || !dinv) {
+  if (!scratch || !dpend || !dbatch || !dbpre || !dinv) {
     set_error("workspace exhausted (PM grids)");
     return kAlloc;
   }
-  // first position of every halo's members in cmem (PM members sort by
-  // cell, and the cells of halo h follow those of halo h-1)
-  std::vector<uint32_t> cm_off(nh + 1, 0);
-  for (int h = 0; h < nh; ++h) cm_off[h + 1] = cm_off[h] + (uint32_t)H[h].np;
   // halos above kBigNp members: chunked removal loop
   std::vector<BigHalo> hbig;
   std::vector<BigChunk> hch;
@@ -1935,15 +1948,10 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
       for (size_t g0 = 0; g0 < grp.size(); g0 += maxb) {
         const int nb = (int)std::min<size_t>(maxb, grp.size() - g0);
         // the batch's halos, their member prefix and their first cmem position
-        std::vector<uint32_t> bp(2 * (size_t)nb + 1, 0);
-        for (int j = 0; j < nb; ++j) {
-          const int h = grp[g0 + j];
-          bp[j + 1] = bp[j] + (uint32_t)H[h].np;
-          bp[nb + 1 + j] = cm_off[h];
-        }
+        std::vector<uint32_t> bp((size_t)nb + 1, 0);
+        for (int j = 0; j < nb; ++j) bp[j + 1] = bp[j] + (uint32_t)H[grp[g0 + j]].np;
         PYFOF_CUDA(cudaMemcpyAsync(dbatch, grp.data() + g0, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s));
         PYFOF_CUDA(cudaMemcpyAsync(dbpre, bp.data(), sizeof(uint32_t) * (nb + 1), cudaMemcpyHostToDevice, s));
-        PYFOF_CUDA(cudaMemcpyAsync(dbsrc, bp.data() + nb + 1, sizeof(uint32_t) * nb, cudaMemcpyHostToDevice, s));
         unsigned long long *acc = reinterpret_cast<unsigned long long *>(scratch);
         R *rho = reinterpret_cast<R *>(scratch);  // the convolved grids overwrite acc
         cplx_t<R> *spec = reinterpret_cast<cplx_t<R> *>(
@@ -1953,10 +1961,10 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
         pm_batch_scale_kernel<<<(unsigned)ceil_div(nb, 128), 128, 0, s>>>(dH, dbatch, nb, nullptr, dinv);
         PYFOF_CHECK_LAUNCH();
         const unsigned gb = (unsigned)std::min<int64_t>(ceil_div(std::max<uint32_t>(bp[nb], 1), BLK), 148 * 16);
-        pm_deposit_kernel<<<gb, BLK, 0, s>>>(m, dH, dbatch, dbpre, dbsrc, nb, cmem, keep, first, wt, sup, acc);
+        pm_deposit_kernel<<<gb, BLK, 0, s>>>(m, dH, dbatch, dbpre, nb, keep, first, wt, sup, acc);
         PYFOF_CHECK_LAUNCH();
         if (ctx.timing) ctx.conv_timer.begin(s);
-        PYFOF_TRY(pm_convolve_batch<R>(rho, spec, (const R *)green_of[n]->g, n, sup, nb, s, acc, dinv));
+        PYFOF_TRY(pm_convolve_batch<R>(rho, spec, (const R *)green_of[n]->g, n, sup, nb, s, acc, dinv, waves(n)));
         if (ctx.timing) ctx.conv_timer.end(s);
         ctx.last_pm_solves += nb;
         ctx.last_pm_fft_bytes += 4.0 * sizeof(R) * nb * (n + 2.0) * n * n;
@@ -1998,7 +2006,7 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
         tl_deposit_kernel<<<gd, BLK, 0, s>>>(m, dH, dA, dbatch, dbpre, nb, src_start, src, keep, sup, acc);
         PYFOF_CHECK_LAUNCH();
         if (ctx.timing) ctx.conv_timer.begin(s);
-        PYFOF_TRY(pm_convolve_batch<R>(rho, spec, gin, nin, sup, nb, s, acc, dinv));
+        PYFOF_TRY(pm_convolve_batch<R>(rho, spec, gin, nin, sup, nb, s, acc, dinv, waves(nin)));
         if (ctx.timing) ctx.conv_timer.end(s);
         ctx.last_pm_solves += nb;
         ctx.last_pm_fft_bytes += 4.0 * sizeof(R) * nb * (nin + 2.0) * nin * nin;
