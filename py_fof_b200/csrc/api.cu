@@ -46,6 +46,12 @@ Context::~Context() {
   }
   if (own_stream) cudaStreamDestroy(own_stream);
   if (aux_stream) cudaStreamDestroy(aux_stream);
+  if (side_stream) {
+    cudaStreamSynchronize(side_stream);
+    cudaStreamDestroy(side_stream);
+  }
+  if (ev_fork) cudaEventDestroy(ev_fork);
+  if (ev_join) cudaEventDestroy(ev_join);
   if (ev_alloc) cudaEventDestroy(ev_alloc);
   if (ev_inputs) cudaEventDestroy(ev_inputs);
   for (auto &e : ev) if (e) cudaEventDestroy(e);

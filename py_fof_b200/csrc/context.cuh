@@ -56,6 +56,10 @@ struct Context {
   cudaStream_t stream = nullptr;      // stream all work is issued on
   cudaStream_t own_stream = nullptr;  // the context's own stream (default)
   cudaStream_t aux_stream = nullptr;  // host-to-device copies of vp and mp
+  // direct-summation unbinding, overlapping the particle-mesh halos (created
+  // on first use); ev_fork/ev_join order it after and before `stream`
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev_alloc = nullptr, ev_inputs = nullptr;
   Arena work;    // per-call device memory, released at the end of every call
   int32_t *d_flags = nullptr;  // device status words (error codes, counters)

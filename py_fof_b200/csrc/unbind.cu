@@ -320,6 +320,19 @@ bool GridRules::select(int64_t np, double span, int &gid, int &lev, double &sp) 
 
 // ------------------------------------------------------------ stage
 
+// Orders the context's side stream after the work issued so far on `s`
+// (creating the stream and its events on first use).
+static int32_t fork_side(Context &ctx, cudaStream_t s) {
+  if (!ctx.side_stream) {
+    PYFOF_CUDA(cudaStreamCreateWithFlags(&ctx.side_stream, cudaStreamNonBlocking));
+    PYFOF_CUDA(cudaEventCreateWithFlags(&ctx.ev_fork, cudaEventDisableTiming));
+    PYFOF_CUDA(cudaEventCreateWithFlags(&ctx.ev_join, cudaEventDisableTiming));
+  }
+  PYFOF_CUDA(cudaEventRecord(ctx.ev_fork, s));
+  PYFOF_CUDA(cudaStreamWaitEvent(ctx.side_stream, ctx.ev_fork, 0));
+  return kOk;
+}
+
 // The direct-summation removal loop over `nb` halos of at most `cap`
 // members, with `threads` threads per block.
 template <bool FP64, int NT>
@@ -456,6 +469,17 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
 
   // 3. solvers
   PYFOF_CUDA(cudaMemsetAsync(ctx.d_flags, 0, sizeof(int32_t), s));
+  // Once the direct path is forked onto the side stream, every return
+  // orders `s` after it (the caller frees this call's memory on `s`).
+  bool side_forked = false;
+  struct SideJoin {
+    Context &c;
+    cudaStream_t s;
+    bool &on;
+    ~SideJoin() {
+      if (on) cudaStreamWaitEvent(s, c.ev_join, 0);
+    }
+  } side_join{ctx, s, side_forked};
   if (!direct.empty()) {
     int32_t *dl = W.carve<int32_t>(direct.size());
     if (!dl) { set_error("workspace exhausted (direct list)"); return kAlloc; }
@@ -496,23 +520,33 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
       else
         direct::ub_direct_phi1_kernel<false><<<(unsigned)tl.size(), direct::PT, 0, s>>>(m, off, dl, dtl, P, phi1);
       PYFOF_CHECK_LAUNCH();
+      // per bucket, largest halos first (they run longest)
       std::vector<int32_t> bl;
       std::vector<size_t> bstart(7, 0);
       for (int b = 0; b < 6; ++b) {
+        const size_t b0 = bl.size();
         for (int32_t c : direct) {
           const int np = tasks[c].np;
           if (np <= kDirectBucketEdge[b] && (b == 0 || np > kDirectBucketEdge[b - 1])) bl.push_back(c);
         }
+        std::stable_sort(bl.begin() + b0, bl.end(),
+                         [&](int32_t x, int32_t y) { return tasks[x].np > tasks[y].np; });
         bstart[b + 1] = bl.size();
       }
       PYFOF_CUDA(cudaMemcpyAsync(dbl, bl.data(), sizeof(int32_t) * bl.size(), cudaMemcpyHostToDevice, s));
-      for (int b = 0; b < 6; ++b) {
+      // the removal loops run on the side stream, overlapping the
+      // particle-mesh halos on `s` (disjoint halos, disjoint outputs)
+      PYFOF_TRY(fork_side(ctx, s));
+      side_forked = true;
+      for (int b = 5; b >= 0; --b) {
         const unsigned nb = (unsigned)(bstart[b + 1] - bstart[b]);
         if (!nb) continue;
         const int cap = (kDirectBucketEdge[b] + 31) / 32 * 32;
         PYFOF_TRY(launch_direct_loop(a.bound_fp64 != 0, a.tiles.direct_threads[b], nb, cap, m, off,
-                                     dbl + bstart[b], P, res, keep, st.phi_out, ctx.d_flags, phi1, s));
+                                     dbl + bstart[b], P, res, keep, st.phi_out, ctx.d_flags, phi1,
+                                     ctx.side_stream));
       }
+      PYFOF_CUDA(cudaEventRecord(ctx.ev_join, ctx.side_stream));
     }
     PYFOF_CHECK_LAUNCH();
   }
@@ -540,6 +574,10 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
     } else {
       PYFOF_TRY(unbind_pm(ctx, a, rules, m, tasks, pm, res, keep, st.phi_out, 0));
     }
+  }
+  if (side_forked) {
+    PYFOF_CUDA(cudaStreamWaitEvent(s, ctx.ev_join, 0));
+    side_forked = false;
   }
   PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   PYFOF_CUDA(cudaStreamSynchronize(s));

@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(NT) ub_direct_kernel(Members m, const int64_t 
   double *phid = reinterpret_cast<double *>(unb + cap);
   unsigned char *keep = reinterpret_cast<unsigned char *>(phid + cap);
   __shared__ int red_i[NT / 32];
-  __shared__ double s_qc[3], s_vc[3];
+  __shared__ double s_qc[3], s_vc[3], s_sum[7];
   __shared__ int s_nu, s_err;
 
   for (int i = threadIdx.x; i < np; i += NT) {
@@ -282,21 +282,28 @@ __global__ void __launch_bounds__(NT) ub_direct_kernel(Members m, const int64_t 
     for (;;) {
       // centre of mass and mean velocity of the kept set, FP64
       if (FP64) {
-        if (threadIdx.x == 0) {
-          double ws = 0, q0 = 0, q1 = 0, q2 = 0, v0 = 0, v1 = 0, v2 = 0;
+        // seven sequential sums in ascending index (the reference's order),
+        // one per lane of warp 0: the kept mass and the mass-weighted
+        // positions and velocities
+        if (threadIdx.x < 7) {
+          const int qi = threadIdx.x;
+          const float *src = qi == 1 ? qx : qi == 2 ? qy : qi == 3 ? qz : qi == 4 ? vx : qi == 5 ? vy : vz;
+          double acc = 0.0;
+#pragma unroll 4
           for (int i = 0; i < np; ++i) {
             if (!keep[i]) continue;
             const double wi = (double)w[i];
-            ws = __dadd_rn(ws, wi);
-            q0 = __dadd_rn(q0, __dmul_rn(wi, (double)qx[i]));
-            q1 = __dadd_rn(q1, __dmul_rn(wi, (double)qy[i]));
-            q2 = __dadd_rn(q2, __dmul_rn(wi, (double)qz[i]));
-            v0 = __dadd_rn(v0, __dmul_rn(wi, (double)vx[i]));
-            v1 = __dadd_rn(v1, __dmul_rn(wi, (double)vy[i]));
-            v2 = __dadd_rn(v2, __dmul_rn(wi, (double)vz[i]));
+            acc = __dadd_rn(acc, qi == 0 ? wi : __dmul_rn(wi, (double)src[i]));
           }
-          s_qc[0] = __ddiv_rn(q0, ws); s_qc[1] = __ddiv_rn(q1, ws); s_qc[2] = __ddiv_rn(q2, ws);
-          s_vc[0] = __ddiv_rn(v0, ws); s_vc[1] = __ddiv_rn(v1, ws); s_vc[2] = __ddiv_rn(v2, ws);
+          s_sum[qi] = acc;
+        }
+        __syncwarp();
+        if (threadIdx.x == 0) {
+          const double ws = s_sum[0];
+          for (int d = 0; d < 3; ++d) {
+            s_qc[d] = __ddiv_rn(s_sum[1 + d], ws);
+            s_vc[d] = __ddiv_rn(s_sum[4 + d], ws);
+          }
         }
       } else if (threadIdx.x < 32) {
         // warp 0: lane l sums the members l, l+32, ...; then a butterfly
