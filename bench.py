@@ -90,7 +90,7 @@ CPU_WARMUP = {
 }
 CPU_SAMPLE = {
     "unbind_nfw_20k": "unbind_nfw_20k:2000",
-    "fof_lognormal_1024": "fof_lognormal_512",
+    "fof_lognormal_1024": "fof_lognormal_256",
     "fof_lognormal_512": "fof_lognormal_256",
 }
 LINK = 0.2
@@ -670,17 +670,22 @@ def run_b200(args):
     return 0
 
 
-def serve_pool(seed=0, count=24):
-    """Distinct requests of the serving configuration, reduced: sizes
-    log-uniform on [1e4, 1e6] particles (the configuration goes to 1e8), the
-    64^3 recipe scaled to L_Box = N^(1/3) (64 halos per 262,144 particles);
-    every second request with unbinding (lognormal masses), half of those in
-    physical units; ng_global = 512 keeps s_15 above the candidate spans."""
+SERVE_REQUESTS = 2000
+SERVE_LOG_RANGE = (4.0, 8.0)
+
+
+def serve_pool(seed=0, count=24, log_range=SERVE_LOG_RANGE):
+    """Distinct requests of the serving configuration: sizes log-uniform on
+    [1e4, 1e8] particles, the 64^3 recipe scaled to L_Box = N^(1/3) (64
+    halos per 262,144 particles); every second request with unbinding
+    (lognormal masses), half of those in physical units; ng_global = 512
+    keeps s_15 above the candidate spans.  The stream draws its requests
+    from this pool."""
     from py_fof_b200 import workloads as W
     rng = np.random.default_rng(seed)
     pool = []
     for k in range(count):
-        n = int(10 ** rng.uniform(4.0, 6.0))
+        n = int(10 ** rng.uniform(*log_range))
         L = float(n ** (1.0 / 3.0))
         bound = k % 2 == 1
         d = W.plummer_box(n, L, max(1, round(64 * n / 262144)), seed=seed * 1000 + k,
@@ -735,7 +740,7 @@ def run_serve(args):
         P.fof_with_info(x, **kw)
         svc.append(time.perf_counter() - t)
     rate = 1.25 / float(np.mean(svc))  # offered load: 1.25x one-at-a-time capacity
-    nreq = 30 * max(1, args.steps)
+    nreq = SERVE_REQUESTS
     rng = np.random.default_rng(args.seed + 1)
     order = rng.integers(0, len(pool), nreq)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
@@ -756,7 +761,7 @@ def run_serve(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 linking; f32 unbinding", "data": "synthetic",
         "config": {"workload": "serve", "requests": nreq, "distinct_inputs": len(pool),
-                   "sizes": "log-uniform 1e4..1e6", "offered_req_per_s": rate,
+                   "sizes": "log-uniform 1e4..1e8", "offered_req_per_s": rate,
                    "arrivals": "Poisson", "unbinding_share": 0.5},
         "serve": res,
         "e2e": {"value": s["mpart_per_s"], "unit": "Mpart/s", "h2d_bytes_per_step": h2d,

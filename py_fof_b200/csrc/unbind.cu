@@ -14,6 +14,7 @@
 //      renumbered in candidate order, and angular momentum per input region
 //      (fof_fortran.f90:313-355)
 #include <algorithm>
+#include <mutex>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -339,9 +340,17 @@ template <bool FP64, int NT>
 static int32_t launch_direct_nt(unsigned nb, int cap, const Members &m, const int64_t *off, const int32_t *list,
                                 const direct::DirectParams &P, HaloResult *res, uint8_t *keep, float *phi_out,
                                 int32_t *flags, const double *phi1, cudaStream_t s) {
+  // the shared-memory limit is a property of the kernel, shared by every
+  // thread that launches it: set it once, to the largest size any launch
+  // asks for, so concurrent calls (serving slots) never lower it
+  static std::once_flag once;
+  static cudaError_t attr = cudaSuccess;
+  std::call_once(once, [] {
+    attr = cudaFuncSetAttribute(direct::ub_direct_kernel<FP64, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)direct::direct_smem(kDirectMax));
+  });
+  PYFOF_CUDA(attr);
   const size_t smem = direct::direct_smem(cap);
-  PYFOF_CUDA(cudaFuncSetAttribute(direct::ub_direct_kernel<FP64, NT>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   direct::ub_direct_kernel<FP64, NT><<<nb, NT, smem, s>>>(m, off, list, P, res, keep, phi_out, flags, phi1, cap);
   PYFOF_CHECK_LAUNCH();
   return kOk;
