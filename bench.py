@@ -759,7 +759,7 @@ def run_serve(args):
         "metric": "serve_mpart_per_s", "value": s["mpart_per_s"], "unit": "Mpart/s",
         "n_gpus": 1, "steps": args.steps, "warmup": 1, "ms_per_step": 1e3 / s["req_per_s"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64 linking; f32 unbinding", "data": "synthetic",
+        "dtype": "f64", "data": "synthetic",
         "config": {"workload": "serve", "requests": nreq, "distinct_inputs": len(pool),
                    "sizes": "log-uniform 1e4..1e8", "offered_req_per_s": rate,
                    "arrivals": "Poisson", "unbinding_share": 0.5},
