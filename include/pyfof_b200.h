@@ -90,7 +90,8 @@ int32_t pyfof_set_stream(void *stream);
  * the last call on the selected device "cells" (reference cell grid size),
  * "active" (particles in linked regions), "candidates" (FoF groups with at
  * least np_halo_min members), "dense_cells" (cells given a sub-cell index),
- * "max_cell" (particles in the fullest cell), "cell_sorts" (1 when the
+ * "max_cell" (particles in the fullest cell), "vd_cells" (very dense cells,
+ * linked by merge sub-cells narrower than link/sqrt(3)), "cell_sorts" (1 when the
  * cell order came from per-cell sorts, 0 from the radix sort),
  * "direct_halos" / "pm_halos" (candidates unbound by direct summation / the
  * particle mesh), "valid_halos" (halos written to the output),

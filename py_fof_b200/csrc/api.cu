@@ -321,6 +321,7 @@ static int32_t context_stat(const Context *c, const char *key, int64_t *value) {
   if (!std::strcmp(key, "active")) { *value = c->last_active; return kOk; }
   if (!std::strcmp(key, "candidates")) { *value = c->last_candidates; return kOk; }
   if (!std::strcmp(key, "dense_cells")) { *value = c->last_dense; return kOk; }
+  if (!std::strcmp(key, "vd_cells")) { *value = c->h_flags ? c->h_flags[FLAG_VD] : 0; return kOk; }
   if (!std::strcmp(key, "max_cell")) { *value = c->last_max_cell; return kOk; }
   if (!std::strcmp(key, "cell_sorts")) { *value = c->last_cell_sorts; return kOk; }
   if (!std::strcmp(key, "direct_halos")) { *value = c->last_direct; return kOk; }

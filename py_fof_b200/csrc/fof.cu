@@ -348,8 +348,25 @@ struct SubGrid {
   float inv[3];  // sub-cells per unit length
 };
 
+// Very dense cell: a dense cell whose merge sub-cells hold VD_OCC particles
+// or more on average.  All pairs inside one merge sub-cell are linked, so
+// such cells are linked sub-cell by sub-cell (fof_vd_intra_kernel,
+// fof_vd_inter_kernel) instead of pair by pair.
+constexpr int VD_OCC = 4;
+__device__ __forceinline__ bool is_vd(const RegionDev &r, int64_t n) {
+  return r.vd_k[0] > 0 && n > DENSE_T && n >= (int64_t)VD_OCC * r.vd_k[0] * r.vd_k[1] * r.vd_k[2];
+}
+
 __device__ __forceinline__ SubGrid dense_sub(const RegionDev &r, int64_t n) {
   SubGrid g;
+  if (is_vd(r, n)) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      g.s[d] = r.vd_k[d];
+      g.inv[d] = r.vd_inv[d];
+    }
+    return g;
+  }
   const int k = max(1, (int)cbrtf(__fdiv_rn((float)n, SUB_OCC)));
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -566,6 +583,7 @@ __global__ void __launch_bounds__(BLK, 3) fof_link_dense_kernel(
     if (valid) me = D.dpos[cb + k];
     const int ip = valid ? __float_as_int(me.w) : -1;
     const RegionDev &r = R[prid[cb]];
+    const bool my_vd = is_vd(r, cn);
     const int64_t local = (int64_t)C.cell - (int64_t)r.cell_off;
     const int64_t N0 = r.N[0], N1 = r.N[1], N2 = r.N[2];
     const int64_t ixyz[3] = {local % N0, (local / N0) % N1, local / (N0 * N1)};
@@ -619,8 +637,10 @@ __global__ void __launch_bounds__(BLK, 3) fof_link_dense_kernel(
         nb_e = cell_start[jc + 1];
         dense = nb_e - nb_b > DENSE_T;
         // pairs with a lower dense cell are that cell's; pairs with sparse
-        // cells are all tested here
+        // cells are all tested here; pairs of two very dense cells are the
+        // merge kernels'
         if ((dense && jl < local) || nb_e == nb_b) use = false;
+        if (use && dense && my_vd && is_vd(r, nb_e - nb_b)) use = false;
         own = jl == local;
         if (use) {
           const SubGrid g = dense ? dense_sub(r, nb_e - nb_b) : SubGrid{{1, 1, 1}, {0.f, 0.f, 0.f}};
@@ -879,6 +899,145 @@ __global__ void __launch_bounds__(BLK) fof_dense_build_kernel(
   }
 }
 
+// Very dense cells, step 1: every particle of a merge sub-cell joins the
+// sub-cell's first particle (every pair inside one passes the exact test,
+// see region_geometry).  One block per dense cell; the others return.
+__global__ void __launch_bounds__(BLK) fof_vd_intra_kernel(
+    const uint32_t *__restrict__ list, const uint32_t *__restrict__ cs, const RegionDev *__restrict__ R,
+    const uint64_t *__restrict__ cell_off, int nreg, int stride, const uint32_t *__restrict__ tab,
+    const float4 *__restrict__ dpos, int *parent, int32_t *flags) {
+  const uint32_t c = list[blockIdx.x];
+  const int64_t base = cs[c];
+  const int64_t n = (int64_t)cs[c + 1] - base;
+  const RegionDev &r = R[nreg == 1 ? 0 : region_of_key(cell_off, nreg, (uint64_t)c)];
+  if (!is_vd(r, n)) return;
+  if (threadIdx.x == 0) atomicAdd(&flags[FLAG_VD], 1);
+  const SubGrid g = dense_sub(r, n);
+  const int S = g.s[0] * g.s[1] * g.s[2];
+  const uint32_t *t = tab + (int64_t)blockIdx.x * stride;
+  const int lane = threadIdx.x & 31;
+  for (int sc = threadIdx.x >> 5; sc < S; sc += BLK / 32) {
+    const int64_t m0 = base + t[sc], m1 = base + t[sc + 1];
+    if (m1 - m0 < 2) continue;
+    const int lead = __float_as_int(dpos[m0].w);
+    int rp = -1;
+    for (int64_t k = m0 + 1 + lane; k < m1; k += 32) link_pair(parent, lead, __float_as_int(dpos[k].w), rp, flags);
+  }
+}
+
+// Very dense cells, step 2: merge sub-cells A (of cell c) and B (of c or of
+// a neighbour very dense cell; pairs of cells from the lower cell, in one
+// cell B > A) whose grid boxes come within `reach` are joined when any of
+// their pairs passes the exact test.  The pairs are tested only while the
+// two roots differ, 32 members of A at a time against each member of B
+// inside A's widened box, up to the first link: sub-cells already joined
+// cost two root look-ups, and linking one pair joins the whole of both.
+// A warp per sub-cell A, a block per dense cell.
+__global__ void __launch_bounds__(BLK) fof_vd_inter_kernel(
+    const uint32_t *__restrict__ list, const uint32_t *__restrict__ cs, const RegionDev *__restrict__ R,
+    const uint64_t *__restrict__ cell_off, int nreg, int stride, const uint32_t *__restrict__ tab,
+    const uint32_t *__restrict__ rank, const float4 *__restrict__ dpos, int *parent, LinkParams P,
+    float reach, int32_t *flags) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const uint32_t c = list[blockIdx.x];
+  const int64_t base = cs[c];
+  const int64_t n = (int64_t)cs[c + 1] - base;
+  const RegionDev &r = R[nreg == 1 ? 0 : region_of_key(cell_off, nreg, (uint64_t)c)];
+  if (!is_vd(r, n)) return;
+  const SubGrid g = dense_sub(r, n);
+  const int S = g.s[0] * g.s[1] * g.s[2];
+  const uint32_t *t = tab + (int64_t)blockIdx.x * stride;
+  const int lane = threadIdx.x & 31;
+  const int64_t local = (int64_t)c - (int64_t)r.cell_off;
+  const int64_t Nd[3] = {r.N[0], r.N[1], r.N[2]};
+  const int64_t ixyz[3] = {local % Nd[0], (local / Nd[0]) % Nd[1], local / (Nd[0] * Nd[1])};
+  const bool per = r.periodic != 0;
+  for (int A = threadIdx.x >> 5; A < S; A += BLK / 32) {
+    const int64_t a0 = base + t[A], a1 = base + t[A + 1];
+    if (a1 == a0) continue;
+    // A's bounding box from its members
+    float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
+    for (int64_t k = a0 + lane; k < a1; k += 32) {
+      const float4 v = dpos[k];
+      lo[0] = fminf(lo[0], v.x); lo[1] = fminf(lo[1], v.y); lo[2] = fminf(lo[2], v.z);
+      hi[0] = fmaxf(hi[0], v.x); hi[1] = fmaxf(hi[1], v.y); hi[2] = fmaxf(hi[2], v.z);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = fminf(lo[d], __shfl_xor_sync(FULL, lo[d], o));
+        hi[d] = fmaxf(hi[d], __shfl_xor_sync(FULL, hi[d], o));
+      }
+    const int leadA = __float_as_int(dpos[a0].w);
+    for (int nb = 0; nb < 27; ++nb) {
+      const int off[3] = {nb % 3 - 1, (nb / 3) % 3 - 1, nb / 9 - 1};
+      int64_t jcoord[3];
+      float sh[3] = {0.f, 0.f, 0.f};
+      bool ok = true;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        int64_t j = ixyz[d] + off[d];
+        if ((r.pdim >> d) & 1) {
+          if (j < 0) { j += Nd[d]; sh[d] = (float)P.L; } else if (j >= Nd[d]) { j -= Nd[d]; sh[d] = -(float)P.L; }
+        } else if (j < 0 || j >= Nd[d]) ok = false;
+        jcoord[d] = j;
+      }
+      if (!ok) continue;
+      const int64_t jl = jcoord[0] + Nd[0] * (jcoord[1] + Nd[1] * jcoord[2]);
+      if (jl < local) continue;
+      const uint64_t jc = r.cell_off + (uint64_t)jl;
+      const int64_t jb = cs[jc], nj = (int64_t)cs[jc + 1] - jb;
+      if (!is_vd(r, nj)) continue;
+      const SubGrid gj = dense_sub(r, nj);
+      const uint32_t *tj = tab + (int64_t)rank[jc] * stride;
+      float wl[3], wh[3];
+      int slo[3], shi[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        wl[d] = __fsub_rn(__fadd_rn(lo[d], sh[d]), reach);
+        wh[d] = __fadd_rn(__fadd_rn(hi[d], sh[d]), reach);
+        const float cl = cell_lower(r, d, jcoord[d]);
+        slo[d] = sub_of(wl[d], cl, gj.inv[d], gj.s[d]);
+        shi[d] = sub_of(wh[d], cl, gj.inv[d], gj.s[d]);
+      }
+      for (int bz = slo[2]; bz <= shi[2]; ++bz)
+        for (int by = slo[1]; by <= shi[1]; ++by)
+          for (int bx = slo[0]; bx <= shi[0]; ++bx) {
+            const int B = bx + gj.s[0] * (by + gj.s[1] * bz);
+            if (jl == local && B <= A) continue;
+            const int64_t b0 = jb + tj[B], b1 = jb + tj[B + 1];
+            if (b1 == b0) continue;
+            int same = 0;
+            if (lane == 0) same = dsu_find(parent, leadA) == dsu_find(parent, __float_as_int(dpos[b0].w));
+            if (__shfl_sync(FULL, same, 0)) continue;
+            bool done = false;
+            for (int64_t ka = a0; ka < a1 && !done; ka += 32) {
+              const int64_t k = ka + lane;
+              const bool valid = k < a1;
+              const float4 me = valid ? dpos[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+              for (int64_t kb = b0; kb < b1; ++kb) {
+                const float4 o = dpos[kb];
+                if (!(o.x >= wl[0] && o.x <= wh[0] && o.y >= wl[1] && o.y <= wh[1] && o.z >= wl[2] &&
+                      o.z <= wh[2]))
+                  continue;
+                const bool lk = valid && (per ? linked_pbc(me, o, P) : linked_open(me, o, P.rp2_open));
+                const unsigned m = __ballot_sync(FULL, lk);
+                if (m) {
+                  if (lane == __ffs(m) - 1) {
+                    int rp = -1;
+                    link_pair(parent, __float_as_int(me.w), __float_as_int(o.w), rp, flags);
+                  }
+                  done = true;
+                  break;
+                }
+              }
+            }
+          }
+    }
+  }
+}
+
 __global__ void fof_init_parent(int *parent, int64_t n) {
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
        p += (int64_t)gridDim.x * blockDim.x)
@@ -1080,6 +1239,25 @@ void region_geometry(double L, double link, int32_t np, const double *xmin, cons
   }
   r.sub_ok = prod > 1 ? 1 : 0;
   for (int d = 0; d < 3; ++d) r.inv_sub[d] = (float)((double)r.sub[d] / r.size[d]);
+  // merge sub-cells: width at most link/sqrt(3) * 0.999 less 8 FP32 ulps of
+  // the box size (the rounding of positions and sub-cell boundaries), so the
+  // largest distance inside one, as the FP32/FP64 test computes it, stays
+  // below the linking length; only where a cell holds at most SUB_MAX of
+  // them and no periodic axis has fewer than 3 cells
+  const double mw = link / std::sqrt(3.0) * 0.999 - 8.0 * 1.1920928955078125e-07 * (std::fabs(L) + 1.0);
+  int64_t km = 1;
+  int k[3] = {0, 0, 0};
+  bool vd = mw > 0.0 && std::isfinite(mw);
+  for (int d = 0; d < 3 && vd; ++d) {
+    const double kk = std::ceil(r.size[d] / mw);
+    if (!(kk >= 1.0) || kk > (double)SUB_MAX || (((pd >> d) & 1) && N[d] < 3)) vd = false;
+    else { k[d] = (int)kk; km *= k[d]; }
+  }
+  if (vd && km > SUB_MAX) vd = false;
+  for (int d = 0; d < 3; ++d) {
+    r.vd_k[d] = vd ? k[d] : 0;
+    r.vd_inv[d] = vd ? (float)((double)k[d] / r.size[d]) : 0.0f;
+  }
 }
 
 int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
@@ -1261,6 +1439,9 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
     P.rp2_lo = (float)(P.rp2 * (1.0 - 4e-6));
     P.rp2_hi = (float)(P.rp2 * (1.0 + 4e-6));
     DenseIndex D{};
+    const uint32_t *D_list = nullptr;  // dense cells in rank order
+    bool any_vd = false;               // a region where very dense cells can occur
+    for (int r = 0; r < nreg; ++r) any_vd = any_vd || (reg[r].active && reg[r].vd_k[0] > 0);
     int64_t ndense_p = 0;  // particles in dense cells (the head of D.order)
     int64_t ndense_chunks = 0;
     DenseChunk *dchunks = nullptr;
@@ -1270,7 +1451,10 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
     {
       int smax = 1;
       for (int r = 0; r < nreg; ++r)
-        if (reg[r].active) smax = std::max(smax, reg[r].sub[0] * reg[r].sub[1] * reg[r].sub[2]);
+        if (reg[r].active) {
+          smax = std::max(smax, reg[r].sub[0] * reg[r].sub[1] * reg[r].sub[2]);
+          smax = std::max(smax, reg[r].vd_k[0] * reg[r].vd_k[1] * reg[r].vd_k[2]);
+        }
       D.stride = smax + 1;
       const int64_t nc = (int64_t)total_cells;
       uint32_t *dflag = W.carve<uint32_t>(nc + 1);
@@ -1324,6 +1508,7 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
         PYFOF_CHECK_LAUNCH();
       }
       D.rank = drank;
+      D_list = list;
       D.tab = tab;
       D.dpos = dpos;
       D.order = order;
@@ -1332,6 +1517,18 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
     // dense-cell particles and the rest as two launches: the long pair loops
     // of the dense part do not hold back blocks of the short sparse work
     if (ctx.timing) cudaEventRecord(ctx.ev[0], s);
+    PYFOF_CUDA(cudaMemsetAsync(ctx.d_flags + FLAG_VD, 0, sizeof(int32_t), s));
+    if (ctx.last_dense > 0 && any_vd) {
+      fof_vd_intra_kernel<<<(unsigned)ctx.last_dense, BLK, 0, s>>>(D_list, cstart, dR, dcoff, nreg, D.stride,
+                                                                   D.tab, D.dpos, parent, ctx.d_flags);
+      PYFOF_CHECK_LAUNCH();
+      fof_vd_inter_kernel<<<(unsigned)ctx.last_dense, BLK, 0, s>>>(D_list, cstart, dR, dcoff, nreg, D.stride,
+                                                                   D.tab, D.rank, D.dpos, parent, P, D.reach,
+                                                                   ctx.d_flags);
+      PYFOF_CHECK_LAUNCH();
+    }
+    PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags + FLAG_VD, ctx.d_flags + FLAG_VD, sizeof(int32_t),
+                               cudaMemcpyDeviceToHost, s));
     if (ndense_chunks > 0) {
       const unsigned dgrid = (unsigned)std::min<int64_t>(ceil_div(ndense_chunks * 32, BLK), (int64_t)kNumSMs * 24);
       fof_link_dense_kernel<<<dgrid, BLK, 0, s>>>(pos, prid, dR, cstart, parent, dchunks, ndense_chunks, P, D,

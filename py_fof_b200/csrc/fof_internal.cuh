@@ -9,7 +9,8 @@
 namespace pyfof {
 
 // Slots of Context::d_flags.
-enum { FLAG_ERR = 0, FLAG_COUNT_A = 1, FLAG_COUNT_B = 2, FLAG_COUNT_C = 3, FLAG_COUNT = 8 };
+// FLAG_VD: very dense cells linked by merge sub-cells in the last call
+enum { FLAG_ERR = 0, FLAG_COUNT_A = 1, FLAG_COUNT_B = 2, FLAG_COUNT_C = 3, FLAG_VD = 4, FLAG_COUNT = 8 };
 
 // One input region (one element of xp_list) with its reference cell grid.
 struct RegionDev {
@@ -26,6 +27,11 @@ struct RegionDev {
   int32_t sub_ok;    // dense cells of this region have more than one sub-cell
   int32_t sub[3];    // sub-cells per axis (each at least one linking length)
   float inv_sub[3];  // sub-cells per unit length
+  // merge sub-cells of very dense cells (0: none in this region): per axis,
+  // at most link/sqrt(3) less a rounding margin wide, so that every two
+  // particles of one are linked by the exact distance test
+  int32_t vd_k[3];
+  float vd_inv[3];
 };
 
 struct Tile {

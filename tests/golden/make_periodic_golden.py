@@ -11,7 +11,8 @@ no test of the reference itself pins a result: boxes of 1, 2 and 3 cells per
 axis, clumps straddling faces and corners, pairs placed on either side of the
 linking length in FP32 (inside the box and across the periodic boundary),
 coordinates given outside [0, L), a region periodic along one axis only,
-and a list of regions mixing open and periodic ones.  Every input is seeded.
+a list of regions mixing open and periodic ones, and very dense clumps in
+link-sized cells (one across a corner of the box).  Every input is seeded.
 The fixture stores, per case, the positions, the region sizes, L, the
 linking length, np_halo_min and the expected in_halo / halo_id.
 """
@@ -158,6 +159,13 @@ def main():
     regs[1][0, :450] = np.mod(regs[1][0, :450] - 3.0, L)
     cases["list_mixed"] = dict(xp=np.hstack(regs), np_halo=[r.shape[1] for r in regs], L=L,
                                link=0.2, np_min=10)
+
+    # very dense clumps in a periodic box of link-sized cells (one across a
+    # corner): cells of hundreds of particles, linked by merge sub-cells
+    L = 2.0
+    cen = [(0.02, 1.98, 0.01), (1.0, 1.0, 1.0), (0.5, 1.4, 0.6)]
+    x = np.hstack([rng.uniform(0, L, (3, 600)), clumps(rng, L, cen, [1600, 1200, 500], 0.05)])
+    cases["pbc_very_dense"] = dict(xp=wrap_some(rng, x, L), np_halo=[x.shape[1]], L=L, link=0.2, np_min=5)
 
     out = {}
     for name, c in cases.items():

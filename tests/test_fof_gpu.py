@@ -275,3 +275,24 @@ def test_lognormal_field_partition(seed):
         _native.set_option("cell_order", 0)
     assert _native.get_stat("cell_sorts") == 1
     assert np.array_equal(g1[0], o[0]) and np.array_equal(g1[1], o[1])
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_very_dense_periodic_clumps(seed):
+    """Clumps dense enough that link-sized cells hold hundreds of particles,
+    one across a corner of the periodic box: those cells are linked by merge
+    sub-cells (all pairs inside one are linked) and sub-cell pairs; the
+    partition must still be the reference's, bit for bit."""
+    rng = np.random.default_rng(seed)
+    L = 6.0
+    cen = np.array([[0.03, 5.98, 0.02], [3.0, 3.0, 3.0], [1.5, 4.2, 2.0], [5.0, 1.0, 4.5]])
+    x = [rng.uniform(0, L, (3, 20000))]
+    for c, k, sc in zip(cen, [4000, 3000, 2000, 1500], [0.08, 0.1, 0.06, 0.15]):
+        x.append(c[:, None] + rng.normal(0.0, sc, (3, k)))
+    xp = np.mod(np.hstack(x), L)
+    kw = dict(L_Box=L, linking_length=0.2, np_halo_min=5)
+    g = P._fof_core(xp, **kw)
+    assert _native.get_stat("vd_cells") > 0
+    o = oracle_core(xp, **kw)
+    assert np.array_equal(g[0], o[0])
+    assert np.array_equal(g[1], o[1])

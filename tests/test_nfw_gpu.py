@@ -20,6 +20,7 @@ def test_nfw_list_fof_exact(seed):
     g = P._fof_core(xs, **kw)
     o = oracle_core(xs, **kw)
     assert _native.get_stat("dense_cells") > 0
+    assert _native.get_stat("vd_cells") > 0  # NFW cusps: cells linked by merge sub-cells
     assert np.array_equal(g[0], o[0])
     assert np.array_equal(g[1], o[1])
 

@@ -13,7 +13,7 @@ import pytest
 from tests.helpers import GOLDEN, oracle_core
 
 CASES = ["pbc_clumps", "pbc_dense", "pbc_1cell", "pbc_2cell", "pbc_3cell", "pbc_boundary_pairs",
-         "pbc_partial", "list_mixed"]
+         "pbc_partial", "list_mixed", "pbc_very_dense"]
 
 
 def _case(name):
@@ -59,6 +59,9 @@ def test_boundary_pairs_split_at_link():
 def test_gpu_matches_brute_force(name):
     import py_fof_b200 as P
     inp, kw, in_halo, halo_id = _case(name)
+    from py_fof_b200 import _native
     g = P._fof_core(inp, **kw)
+    if name == "pbc_very_dense":
+        assert _native.get_stat("vd_cells") > 0  # linked by merge sub-cells
     assert np.array_equal(np.asarray(g[0], np.int32), in_halo)
     assert np.array_equal(g[1], halo_id)
