@@ -201,11 +201,19 @@ constexpr size_t smem_bytes() {
   return sizeof(cplx_t<R>) * (size_t)(N + 2 * (kW<R> + 1) * N);
 }
 
-// Shared memory of the fused z pass: the tiles plus two staging buffers of
+// Shared memory of the line passes (k_lines): twiddles and one tile (the
+// plain passes write stage B straight to the spectrum; the fused pass runs
+// stage B in place, every thread rewriting exactly the column it read).
+template <typename R, int N>
+constexpr size_t smem_lines_bytes() {
+  return sizeof(cplx_t<R>) * (size_t)(N + (kW<R> + 1) * N);
+}
+
+// Shared memory of the fused z pass: the tile plus two staging buffers of
 // N/2+1 rows for the next halo's input.
 template <typename R, int N>
 constexpr size_t smem_conv_bytes() {
-  return smem_bytes<R, N>() + sizeof(cplx_t<R>) * (size_t)(2 * (N / 2 + 1) * kW<R>);
+  return smem_lines_bytes<R, N>() + sizeof(cplx_t<R>) * (size_t)(2 * (N / 2 + 1) * kW<R>);
 }
 
 // 16-byte asynchronous copy global -> shared (completion by wait_group)
@@ -440,12 +448,11 @@ __global__ void __launch_bounds__(Cfg<R, N>::T) k_lines(cplx_t<R> *__restrict__ 
     }
   }
   __syncthreads();
-  int parity = 0;
   // CONV: the input rows of the next halo are copied into a staging buffer
   // while the current one is transformed (two buffers of N/2+1 rows of W
   // complex; in_lim <= N/2+1 there)
   constexpr int SROWS = N / 2 + 1, CPR = (int)(W * sizeof(C) / 16);
-  C *const stage0 = buf0 + 2 * WP * N;
+  C *const stage0 = buf0 + WP * N;
   auto prefetch = [&](int bb, int slot) {
     const C *src = spec + (int64_t)bb * bstride + (int64_t)other * ostride + kx0;
     C *dst = stage0 + slot * (SROWS * W);
@@ -461,7 +468,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::T) k_lines(cplx_t<R> *__restrict__ 
   }
   for (int b = b0, i = 0; b < b1; ++b, ++i) {
     C *base = spec + (int64_t)b * bstride + (int64_t)other * ostride + kx0;
-    C *bA = buf0 + parity * (WP * N);
+    C *bA = buf0;
     const C *stg = stage0 + (i & 1) * (SROWS * W);
     if constexpr (CONV) {
       if (b + 1 < b1) {
@@ -495,8 +502,10 @@ __global__ void __launch_bounds__(Cfg<R, N>::T) k_lines(cplx_t<R> *__restrict__ 
       }
     }
     __syncthreads();
-    // stage B: DFT over s (and for CONV: Green, inverse DFT over k2, twiddle)
-    C *bB = buf0 + (parity ^ 1) * (WP * N);
+    // stage B: DFT over s (and for CONV: Green, inverse DFT over k2, twiddle,
+    // written back in place: unit (li, k1) reads and rewrites only its own
+    // elements li + WP (k1 + N1 s))
+    C *bB = buf0;
 #pragma unroll
     for (int it = 0; it < IB; ++it) {
       const int u = threadIdx.x + it * T;
@@ -548,10 +557,9 @@ __global__ void __launch_bounds__(Cfg<R, N>::T) k_lines(cplx_t<R> *__restrict__ 
         }
       }
     }
-    // CONV: the next stage A writes tile `parity` only after every thread
-    // passed the barrier above, i.e. finished reading it.  Plain passes
-    // alternate the tiles instead.
-    if constexpr (!CONV) parity ^= 1;
+    // the next halo's stage A rewrites the tile: every thread must have
+    // finished reading it (CONV: the barrier at the top of the loop)
+    if constexpr (!CONV) __syncthreads();
   }
 }
 
@@ -585,8 +593,8 @@ int32_t prepare() {
     if (r == kOk) r = allow_smem(k_x_r2c<R, N, true>, sm);
     if (r == kOk) r = allow_smem(k_x_c2r<R, N, N / 2 + 1>, sm);
     if (r == kOk) r = allow_smem(k_x_c2r<R, N, N>, sm);
-    if (r == kOk) r = allow_smem(k_lines<R, N, -1, false>, sm);
-    if (r == kOk) r = allow_smem(k_lines<R, N, +1, false>, sm);
+    if (r == kOk) r = allow_smem(k_lines<R, N, -1, false>, smem_lines_bytes<R, N>());
+    if (r == kOk) r = allow_smem(k_lines<R, N, +1, false>, smem_lines_bytes<R, N>());
     if (r == kOk) r = allow_smem(k_lines<R, N, -1, true>, smem_conv_bytes<R, N>());
     status = r;
   });
@@ -611,7 +619,7 @@ int32_t convolve_n(R *rho, cplx_t<R> *spec, const R *green, int sup, int batch, 
                                                                           nullptr);
   PYFOF_CHECK_LAUNCH();
   // y forward: lines (kx, z < sup), input y < sup, output all y
-  k_lines<R, N, -1, false><<<(unsigned)((int64_t)ntiles * sup * batch), T, sm, s>>>(
+  k_lines<R, N, -1, false><<<(unsigned)((int64_t)ntiles * sup * batch), T, smem_lines_bytes<R, N>(), s>>>(
       spec, nullptr, bstride, (int64_t)N * nhp, nhp, sup, ntiles, 1, batch, sup, N);
   PYFOF_CHECK_LAUNCH();
   // z: forward, Green, inverse; lines (kx, ky), input and output z < sup;
@@ -633,7 +641,7 @@ int32_t convolve_n(R *rho, cplx_t<R> *spec, const R *green, int sup, int batch, 
       spec, green, bstride, nhp, (int64_t)N * nhp, N, ntiles, nbb, batch, sup, sup);
   PYFOF_CHECK_LAUNCH();
   // y inverse: lines (kx, z < sup), input all y, output y < sup
-  k_lines<R, N, +1, false><<<(unsigned)((int64_t)ntiles * sup * batch), T, sm, s>>>(
+  k_lines<R, N, +1, false><<<(unsigned)((int64_t)ntiles * sup * batch), T, smem_lines_bytes<R, N>(), s>>>(
       spec, nullptr, bstride, (int64_t)N * nhp, nhp, sup, ntiles, 1, batch, N, sup);
   PYFOF_CHECK_LAUNCH();
   const R n3 = (R)((double)N * N * N);
@@ -654,10 +662,10 @@ int32_t c2r_full_n(const R *green, cplx_t<R> *spec, R *out, cudaStream_t s) {
   PYFOF_CHECK_LAUNCH();
   const int64_t bstride = (int64_t)N * N * nhp;
   // z inverse over all ky, then y inverse over all z
-  k_lines<R, N, +1, false><<<(unsigned)((int64_t)ntiles * N), T, sm, s>>>(
+  k_lines<R, N, +1, false><<<(unsigned)((int64_t)ntiles * N), T, smem_lines_bytes<R, N>(), s>>>(
       spec, nullptr, bstride, nhp, (int64_t)N * nhp, N, ntiles, 1, 1, N, N);
   PYFOF_CHECK_LAUNCH();
-  k_lines<R, N, +1, false><<<(unsigned)((int64_t)ntiles * N), T, sm, s>>>(
+  k_lines<R, N, +1, false><<<(unsigned)((int64_t)ntiles * N), T, smem_lines_bytes<R, N>(), s>>>(
       spec, nullptr, bstride, (int64_t)N * nhp, nhp, N, ntiles, 1, 1, N, N);
   PYFOF_CHECK_LAUNCH();
   const int64_t nlines = (int64_t)N * N;
