@@ -195,15 +195,11 @@ template <> struct Cfg<double, 128> { static constexpr int N1 = 16, N2 = 8, T = 
 template <> struct Cfg<double, 216> { static constexpr int N1 = 12, N2 = 18, T = 96; };
 template <> struct Cfg<double, 256> { static constexpr int N1 = 16, N2 = 16, T = 128; };
 
-template <typename R, int N>
-constexpr size_t smem_bytes() {
-  // twiddles + two tiles of N rows of W+1 complex (one pad column)
-  return sizeof(cplx_t<R>) * (size_t)(N + 2 * (kW<R> + 1) * N);
-}
-
-// Shared memory of the line passes (k_lines): twiddles and one tile (the
-// plain passes write stage B straight to the spectrum; the fused pass runs
-// stage B in place, every thread rewriting exactly the column it read).
+// Shared memory of the line kernels: twiddles and one tile of N rows of W+1
+// complex (one pad column).  Every stage runs in place: stage B rewrites
+// exactly the column each thread read, stage A reads all its inputs into
+// registers before a barrier (x passes); the plain y passes write stage B
+// straight to the spectrum.
 template <typename R, int N>
 constexpr size_t smem_lines_bytes() {
   return sizeof(cplx_t<R>) * (size_t)(N + (kW<R> + 1) * N);
@@ -235,35 +231,42 @@ __device__ __forceinline__ void load_twiddles(cplx_t<R> *tw) {
   }
 }
 
-// Stage A on a tile held in `src` (tile element (li, e) at li + (W+1) e),
-// result with twiddles into `dst` (element (li, s, k1) at li + (W+1)(k1 + N1 s)).
-// Elements e >= in_lim are zero.
+// Stage A in place on `buf`: every thread first reads all the elements of
+// its units into registers, then (after a barrier) writes the results over
+// the tile.
 template <typename R, int N, int SIGN>
-__device__ __forceinline__ void stage_a_smem(const cplx_t<R> *src, cplx_t<R> *dst, const cplx_t<R> *tw,
-                                             int in_lim) {
+__device__ __forceinline__ void stage_a_inplace(cplx_t<R> *buf, const cplx_t<R> *tw, int in_lim) {
   using C = cplx_t<R>;
   constexpr int N1 = Cfg<R, N>::N1, N2 = Cfg<R, N>::N2, T = Cfg<R, N>::T;
-  constexpr int W = kW<R>, WP = W + 1, UA = W * N2;
+  constexpr int W = kW<R>, WP = W + 1, UA = W * N2, IA = (UA + T - 1) / T;
+  C v[IA][N1];
 #pragma unroll
-  for (int it = 0; it < (UA + T - 1) / T; ++it) {
+  for (int it = 0; it < IA; ++it) {
+    const int u = threadIdx.x + it * T;
+    const int li = u % W, s = u / W;
+#pragma unroll
+    for (int q = 0; q < N1; ++q) {
+      const int e = s + N2 * q;
+      v[it][q] = (u < UA && e < in_lim) ? buf[li + WP * e] : mk<C>(0, 0);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < IA; ++it) {
     const int u = threadIdx.x + it * T;
     if (u < UA) {
       const int li = u % W, s = u / W;
-      C v[N1];
-#pragma unroll
-      for (int q = 0; q < N1; ++q) {
-        const int e = s + N2 * q;
-        v[q] = e < in_lim ? src[li + WP * e] : mk<C>(0, 0);
-      }
-      dft<N1, SIGN>(v);
+      dft<N1, SIGN>(v[it]);
 #pragma unroll
       for (int k1 = 0; k1 < N1; ++k1)
-        dst[li + WP * (k1 + N1 * s)] = SIGN < 0 ? cmul(v[k1], tw[s * k1]) : cmulc(v[k1], tw[s * k1]);
+        buf[li + WP * (k1 + N1 * s)] = SIGN < 0 ? cmul(v[it][k1], tw[s * k1]) : cmulc(v[it][k1], tw[s * k1]);
     }
   }
 }
 
 // Stage B from `src` (stage A layout) into tile layout `dst` (li + (W+1) k).
+// Unit (li, k1) reads and writes only the elements li + (W+1) (k1 + N1 j),
+// so src may equal dst.
 template <typename R, int N, int SIGN>
 __device__ __forceinline__ void stage_b_smem(const cplx_t<R> *src, cplx_t<R> *dst) {
   using C = cplx_t<R>;
@@ -302,7 +305,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::T) k_x_r2c(const R *__restrict__ rh
   constexpr int T = Cfg<R, N>::T, W = kW<R>, WP = W + 1, NH = N / 2 + 1, SUP = N / 2 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *tw = reinterpret_cast<C *>(smem_raw);
-  C *t0 = tw + N, *t1 = t0 + WP * N;
+  C *t0 = tw + N;
   load_twiddles<R, N, T>(tw);
   const int L0 = blockIdx.x * (2 * W);
   const int nl = min(2 * W, nlines - L0);
@@ -326,9 +329,9 @@ __global__ void __launch_bounds__(Cfg<R, N>::T) k_x_r2c(const R *__restrict__ rh
     }
   }
   __syncthreads();
-  stage_a_smem<R, N, -1>(t0, t1, tw, SUP);
+  stage_a_inplace<R, N, -1>(t0, tw, SUP);
   __syncthreads();
-  stage_b_smem<R, N, -1>(t1, t0);
+  stage_b_smem<R, N, -1>(t0, t0);
   __syncthreads();
 #pragma unroll
   for (int it = 0; it < (2 * W * NH + T - 1) / T; ++it) {
@@ -359,7 +362,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::T) k_x_c2r(const cplx_t<R> *__restr
   constexpr int T = Cfg<R, N>::T, W = kW<R>, WP = W + 1, NH = N / 2 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *tw = reinterpret_cast<C *>(smem_raw);
-  C *t0 = tw + N, *t1 = t0 + WP * N;
+  C *t0 = tw + N;
   load_twiddles<R, N, T>(tw);
   const int L0 = blockIdx.x * (2 * W);
   const int nl = min(2 * W, nlines - L0);
@@ -390,9 +393,9 @@ __global__ void __launch_bounds__(Cfg<R, N>::T) k_x_c2r(const cplx_t<R> *__restr
     }
   }
   __syncthreads();
-  stage_a_smem<R, N, +1>(t0, t1, tw, N);
+  stage_a_inplace<R, N, +1>(t0, tw, N);
   __syncthreads();
-  stage_b_smem<R, N, +1>(t1, t0);
+  stage_b_smem<R, N, +1>(t0, t0);
   __syncthreads();
   R *dst = out + (int64_t)L0 * OLIM;
 #pragma unroll
@@ -587,7 +590,7 @@ int32_t prepare() {
   static std::once_flag once;
   static int32_t status = kOk;
   std::call_once(once, [] {
-    const size_t sm = smem_bytes<R, N>();
+    const size_t sm = smem_lines_bytes<R, N>();
     int32_t r = kOk;
     if (r == kOk) r = allow_smem(k_x_r2c<R, N, false>, sm);
     if (r == kOk) r = allow_smem(k_x_r2c<R, N, true>, sm);
@@ -608,7 +611,7 @@ int32_t convolve_n(R *rho, cplx_t<R> *spec, const R *green, int sup, int batch, 
   constexpr int W = kW<R>, T = Cfg<R, N>::T;
   const int nhp = (int)spec_row<R>(N);
   const int ntiles = nhp / W;
-  const size_t sm = smem_bytes<R, N>();
+  const size_t sm = smem_lines_bytes<R, N>();
   const int64_t bstride = (int64_t)N * N * nhp;
   const int64_t nlines = (int64_t)batch * sup * sup;
   if (acc)
@@ -656,7 +659,7 @@ int32_t c2r_full_n(const R *green, cplx_t<R> *spec, R *out, cudaStream_t s) {
   constexpr int W = kW<R>, T = Cfg<R, N>::T;
   const int nhp = (int)spec_row<R>(N);
   const int ntiles = nhp / W;
-  const size_t sm = smem_bytes<R, N>();
+  const size_t sm = smem_lines_bytes<R, N>();
   const int64_t cnt = (int64_t)(N / 2 + 1) * N * N;
   k_real_to_cplx<R><<<(unsigned)std::min<int64_t>(ceil_div(cnt, 256), 4096), 256, 0, s>>>(green, spec, N, nhp);
   PYFOF_CHECK_LAUNCH();
