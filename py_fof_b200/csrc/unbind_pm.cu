@@ -491,7 +491,9 @@ __device__ __forceinline__ T c2_delta(T r, T ht, T hs) {
 // chunk is spatially compact).  Sources are scanned cell by cell in
 // coalesced batches of 32; a source enters the pair loop only if it lies
 // within the chunk's largest cutoff of the chunk's bounding box, so the
-// divergent pair arithmetic runs almost only on pairs that interact.
+// divergent pair arithmetic runs almost only on pairs that interact.  FP32
+// sums are compensated (Kahan); FP64 sums are plain, which keeps the
+// dependent chain per pair to one add.
 // FP32 product path of the short-range kernel: the spline-softened 1/r of
 // depth_c with its divisions replaced by products with per-h reciprocals and
 // 1/r from rsqrtf (a few ulps; the FP64 path keeps the divisions).
@@ -550,7 +552,7 @@ struct SrChunk {
 };
 
 template <typename R, bool UPDATE>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) sr_gather_kernel(
+__global__ void __launch_bounds__(256, 4) sr_gather_kernel(
     const PmHalo *__restrict__ H, const int32_t *__restrict__ mhalo, const uint8_t *__restrict__ keep,
     const uint8_t *__restrict__ pr, const SrChunk *__restrict__ chunks, int64_t nchunks,
     const uint32_t *__restrict__ cstart, const uint32_t *__restrict__ cmem, const float4 *__restrict__ src4,
@@ -683,10 +685,14 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) sr_gather_kernel(
                 const R d = sqrt(r2);
                 dphi = -(fac * (depth_c<R>(d, eps) - depth_c<R>(d, ai)));
               }
-              const R yv = (R)jw * dphi - comp;
-              const R tt = acc + yv;
-              comp = (tt - acc) - yv;
-              acc = tt;
+              if constexpr (sizeof(R) == 4) {  // FP32: compensated sum
+                const R yv = (R)jw * dphi - comp;
+                const R tt = acc + yv;
+                comp = (tt - acc) - yv;
+                acc = tt;
+              } else {  // FP64: a plain sum (one dependent add per pair)
+                acc += (R)jw * dphi;
+              }
             }
           }
         }
