@@ -314,7 +314,7 @@ __device__ __forceinline__ bool linked_pbc(float4 a, float4 b, const LinkParams 
 // exact distance test can accept.  Their particles, and every pair between
 // a dense and a sparse cell, are linked by the dense-cell kernel; pairs of
 // sparse cells by the per-particle kernel.
-constexpr int DENSE_T = 12;
+constexpr int DENSE_T = 24;
 constexpr int SUB_MAX = 216;
 
 struct DenseIndex {
