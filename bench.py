@@ -610,8 +610,8 @@ def run_b200(args):
             dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
         e2e_value = n_job / float(e2e_s.item()) / 1e6
         h2d = 24 * n + (24 * n if vp_h is not None else 0) + (8 * n if mp_h is not None else 0)
-        # halo_id (in_halo is derived from it on the host) and ang_mom
-        d2h = 4 * n + 24 * (len(d["regions"][0]) if d["regions"] is not None else 1)
+        # in_halo (one byte per particle: fof() returns no halo ids) and ang_mom
+        d2h = n + 24 * (len(d["regions"][0]) if d["regions"] is not None else 1)
 
     peak, peak_kind = _peaks()
 

@@ -108,7 +108,10 @@ int32_t pyfof_last_link_ms(float *ms);
  * "link" (the linking kernel), "fof" (binning, linking and labelling up to
  * the candidate list), "unbind" (unbinding and outputs with bound_check, the
  * ang_mom pass without), "call" (all of it), "pm_fft" (the particle-mesh
- * convolutions, summed over all solves). */
+ * convolutions, summed over all solves); after a host-memory call also
+ * "h2d_positions" (the copy of xp), "h2d_inputs" (from the first copy to the
+ * end of the last input copy), "d2h" (the output copy after the device work)
+ * and "host_call" (from the first input copy to the end of the output copy). */
 int32_t pyfof_last_stage_ms(const char *stage, float *ms);
 
 /* First-pass gravitational potential of one candidate, computed by the
@@ -198,6 +201,19 @@ int32_t pyfof_run_units(void *slot, const pyfof_units_t *units, const double *xp
                         int32_t bound_check, int32_t verbose, double softening, double a_val,
                         double b_val, double s_15_val, int32_t n_threads, int64_t ng_val,
                         double ng_global_val, int32_t *in_halo, int32_t *halo_id, double *ang_mom);
+
+/* py_fof.fof (py_fof/__init__.py:354-447) returns in_halo alone: this is
+ * pyfof_run_units with in_halo as one byte per particle (0 or 1, a numpy
+ * bool array's layout) and no halo_id, so a quarter of the output bytes
+ * cross back to the host.  ang_mom, units, slot and ierr as in
+ * pyfof_run_units; in_halo is written in full on success and zeroed on
+ * failure. */
+int32_t pyfof_run_mask(void *slot, const pyfof_units_t *units, const double *xp, const double *vp,
+                       const double *mp, int32_t layout, const int32_t *np_halo, int32_t nhalo,
+                       int64_t total_np, double L_Box, double linking_length, int32_t np_halo_min,
+                       int32_t bound_check, int32_t verbose, double softening, double a_val,
+                       double b_val, double s_15_val, int32_t n_threads, int64_t ng_val,
+                       double ng_global_val, uint8_t *in_halo, double *ang_mom);
 
 /* fof_with_info on the device (py_fof/__init__.py:481-518): pyfof_run
  * (without in_halo, which is halo_id > 0) that also returns the halo

@@ -289,12 +289,22 @@ def _finish(call: FofCall, in_halo_out, halo_id_out, ang_mom_out, ierr):
     return in_halo_out, halo_id_out, ang_mom_scaled
 
 
-def _native_call(call: FofCall):
+def _native_call(call: FofCall, mask_only=False):
     return _native.run(call.xp, call.vp, call.mp, call.np_halo, call.nhalo, call.L_Box,
                        call.link, call.np_halo_min, call.bound_check, call.verbose,
                        call.softening, call.a_val, call.b_val, call.s_15_val, call.n_threads,
                        call.total_np, ng_val=call.ng_val, ng_global_val=call.ng_global_val,
-                       units=call.units)
+                       units=call.units, mask_only=mask_only)
+
+
+def _run_public(mask_only, **kw):
+    """_prepare, the native call and _finish; with `mask_only` the library
+    returns in_halo alone (halo_id is None), which is all fof() needs."""
+    call = _prepare(check_masses=False, device_units=True, **kw)
+    if not isinstance(call, FofCall):
+        return call
+    in_halo, halo_id, ang_mom, ierr = _native_call(call, mask_only=mask_only)
+    return _finish(call, in_halo, halo_id, ang_mom, ierr)
 
 
 def _fof_core(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2,
@@ -305,17 +315,12 @@ def _fof_core(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2,
               ng=None, ng_global=None):
     """Validation, unit conversion and the native call; returns
     (in_halo, halo_id, ang_mom) like the reference wrapper core."""
-    call = _prepare(xp_list, vp_list=vp_list, L_Box=L_Box, linking_length=linking_length,
-                    np_halo_min=np_halo_min, bound_check=bound_check, verbose=verbose,
-                    return_ang_mom=return_ang_mom, n_threads=n_threads, mp_list=mp_list,
-                    softening=softening, z=z, box=box, h0=h0, omega_m=omega_m,
-                    omega_l=omega_l, n_sim=n_sim, units=units,
-                    include_hubble_flow=include_hubble_flow, ng=ng, ng_global=ng_global,
-                    check_masses=False, device_units=True)
-    if not isinstance(call, FofCall):
-        return call
-    in_halo, halo_id, ang_mom, ierr = _native_call(call)
-    return _finish(call, in_halo, halo_id, ang_mom, ierr)
+    return _run_public(False, xp_list=xp_list, vp_list=vp_list, L_Box=L_Box,
+                       linking_length=linking_length, np_halo_min=np_halo_min,
+                       bound_check=bound_check, verbose=verbose, return_ang_mom=return_ang_mom,
+                       n_threads=n_threads, mp_list=mp_list, softening=softening, z=z, box=box,
+                       h0=h0, omega_m=omega_m, omega_l=omega_l, n_sim=n_sim, units=units,
+                       include_hubble_flow=include_hubble_flow, ng=ng, ng_global=ng_global)
 
 
 def fof(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2,
@@ -330,8 +335,9 @@ def fof(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2,
     ``return_ang_mom=True``, the per-input-region angular momentum (3, nhalo).
     Parameters and units are those of the reference ``py_fof.fof``.
     """
-    in_halo, _, ang_mom = _fof_core(
-        xp_list=xp_list, vp_list=vp_list, L_Box=L_Box, linking_length=linking_length,
+    # the core of _fof_core with only in_halo crossing back from the device
+    in_halo, _, ang_mom = _run_public(
+        True, xp_list=xp_list, vp_list=vp_list, L_Box=L_Box, linking_length=linking_length,
         np_halo_min=np_halo_min, bound_check=bound_check, verbose=verbose,
         return_ang_mom=return_ang_mom, n_threads=n_threads, mp_list=mp_list,
         softening=softening, z=z, box=box, h0=h0, omega_m=omega_m, omega_l=omega_l,

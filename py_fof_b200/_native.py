@@ -47,7 +47,7 @@ EXPORTED = ("pyfof_version", "pyfof_init", "pyfof_shutdown", "pyfof_last_error",
             "pyfof_set_option", "pyfof_get_option", "pyfof_set_tile", "pyfof_get_tile", "pyfof_set_stream", "pyfof_get_stat", "pyfof_last_link_ms", "pyfof_last_stage_ms",
             "pyfof_halo_potential", "pyfof_halo_potential_direct_static", "pyfof_run",
             "pyfof_run_device", "pyfof_slot_create", "pyfof_slot_destroy", "pyfof_slot_run",
-            "pyfof_slot_stat", "pyfof_run_catalogue", "pyfof_run_units")
+            "pyfof_slot_stat", "pyfof_run_catalogue", "pyfof_run_units", "pyfof_run_mask")
 
 
 class NativeLibraryError(RuntimeError):
@@ -108,6 +108,9 @@ def load():
         L.pyfof_run_catalogue.restype = ctypes.c_int32
         L.pyfof_run_units.restype = ctypes.c_int32
         L.pyfof_run_units.argtypes = [ctypes.c_void_p, ctypes.POINTER(Units)] + list(_RUN_ARGS)
+        L.pyfof_run_mask.restype = ctypes.c_int32
+        L.pyfof_run_mask.argtypes = ([ctypes.c_void_p, ctypes.POINTER(Units)] + list(_RUN_ARGS[:19]) +
+                                     [ctypes.c_void_p, _dp])
         L.pyfof_run_catalogue.argtypes = ([ctypes.c_void_p, ctypes.POINTER(Units)] + list(_RUN_ARGS[:19]) +
                                           [_RUN_ARGS[20], _RUN_ARGS[21], ctypes.c_void_p,
                                            ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32)])
@@ -265,7 +268,8 @@ def last_link_ms() -> float:
 
 def last_stage_ms(stage: str) -> float:
     """Device time of one stage of the last call ("link", "fof", "unbind",
-    "call"); needs set_option("timing", 1)."""
+    "call", "pm_fft"; after a host-memory call also "h2d_positions",
+    "h2d_inputs", "d2h", "host_call"); needs set_option("timing", 1)."""
     v = ctypes.c_float(0.0)
     if load().pyfof_last_stage_ms(stage.encode(), ctypes.byref(v)) != 0:
         raise ValueError(last_error())
@@ -278,14 +282,16 @@ def _ptr(a):
 
 def run(xp, vp, mp, np_halo, nhalo, L_Box, link, np_halo_min, bound_check, verbose, softening,
         a_val, b_val, s_15_val, n_threads, total_np, ng_val=256, ng_global_val=512.0, slot=None,
-        units=None):
+        units=None, mask_only=False):
     """Host-memory call with the f2py argument order of fof_fortran.fof_fortran.
 
     xp, vp: (3,N) float64 arrays, C- or Fortran-contiguous (vp may be None);
     mp: (N,) float64 or None.  `slot`: a handle of slot_create, else the
     default context.  `units`: (x_div, v_mul, m_div, m_const), the inputs'
     conversion to code units done on the device, or None.  Returns
-    (in_halo, halo_id, ang_mom, ierr).
+    (in_halo, halo_id, ang_mom, ierr); with `mask_only` the library returns
+    in_halo alone, as bytes written into a numpy bool array, and halo_id is
+    None (pyfof_run_mask).
     """
     L = load()
     n = int(total_np)
@@ -305,13 +311,20 @@ def run(xp, vp, mp, np_halo, nhalo, L_Box, link, np_halo_min, bound_check, verbo
     # written in full by the library (zeros on every failure path); in_halo
     # is halo_id > 0, so only halo_id crosses back to the host
     in_halo = None
-    halo_id = np.empty(n, dtype=np.int32)
     ang_mom = np.zeros((3, max(int(nhalo), 0)), dtype=np.float64, order="F")
     args = (_ptr(xp), _ptr(vp), _ptr(mp), layout, nph.ctypes.data_as(_i32p),
             int(nhalo), n, float(L_Box), float(link), int(np_halo_min),
             int(bound_check), int(verbose), float(softening), float(a_val),
             float(b_val), float(s_15_val), int(n_threads), int(ng_val),
-            float(ng_global_val), None, _ptr(halo_id), ang_mom.ctypes.data_as(_dp))
+            float(ng_global_val))
+    if mask_only:
+        in_halo = np.empty(n, dtype=np.bool_)
+        ierr = L.pyfof_run_mask(ctypes.c_void_p(slot) if slot else None,
+                                None if units is None else _units_ptr(units), *args,
+                                _ptr(in_halo), ang_mom.ctypes.data_as(_dp))
+        return in_halo, None, ang_mom, int(ierr)
+    halo_id = np.empty(n, dtype=np.int32)
+    args = args + (None, _ptr(halo_id), ang_mom.ctypes.data_as(_dp))
     if units is not None:
         ierr = L.pyfof_run_units(ctypes.c_void_p(slot) if slot else None, _units_ptr(units), *args)
     elif slot is None:

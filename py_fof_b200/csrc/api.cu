@@ -54,9 +54,62 @@ Context::~Context() {
   if (ev_join) cudaEventDestroy(ev_join);
   if (ev_alloc) cudaEventDestroy(ev_alloc);
   if (ev_inputs) cudaEventDestroy(ev_inputs);
+  if (ev_masses) cudaEventDestroy(ev_masses);
+  if (ev_pack) cudaEventDestroy(ev_pack);
+  if (ev_vel) cudaEventDestroy(ev_vel);
   for (auto &e : ev) if (e) cudaEventDestroy(e);
   if (d_flags) cudaFree(d_flags);
   if (h_flags) cudaFreeHost(h_flags);
+  if (h_stage) cudaFreeHost(h_stage);
+  for (uint8_t *p : stage_retired) cudaFreeHost(p);
+}
+
+// dst[i] = src[i], src in mapped host memory at a 16-byte aligned address
+__global__ void upload_kernel(const uint8_t *__restrict__ src, uint8_t *__restrict__ dst, size_t bytes) {
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  size_t done = 0;
+  if ((reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+    const size_t n16 = bytes / 16;
+    for (size_t i = tid; i < n16; i += stride)
+      reinterpret_cast<uint4 *>(dst)[i] = reinterpret_cast<const uint4 *>(src)[i];
+    done = 16 * n16;
+  }
+  for (size_t i = done + tid; i < bytes; i += stride) dst[i] = src[i];
+}
+
+int32_t upload(Context &ctx, void *dst, const void *src, size_t bytes, cudaStream_t s) {
+  constexpr size_t kInline = 4096;
+  if (bytes == 0) return kOk;
+  if (bytes <= kInline) {
+    PYFOF_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+    return kOk;
+  }
+  size_t off = (ctx.stage_used + 15) & ~(size_t)15;
+  if (!ctx.h_stage || off + bytes > ctx.stage_cap) {
+    size_t cap = std::max(2 * ctx.stage_cap, std::max(bytes, (size_t)1 << 20));
+    cap = (cap + 4095) & ~(size_t)4095;
+    uint8_t *p = nullptr;
+    if (cudaHostAlloc(reinterpret_cast<void **>(&p), cap, cudaHostAllocMapped | cudaHostAllocPortable) !=
+        cudaSuccess) {
+      // no pinned memory to be had: a plain copy (ordered, possibly queued)
+      cudaGetLastError();
+      PYFOF_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+      return kOk;
+    }
+    if (ctx.h_stage) ctx.stage_retired.push_back(ctx.h_stage);
+    ctx.h_stage = p;
+    ctx.stage_cap = cap;
+    off = 0;
+  }
+  std::memcpy(ctx.h_stage + off, src, bytes);
+  uint8_t *dsrc = nullptr;
+  PYFOF_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&dsrc), ctx.h_stage + off, 0));
+  const unsigned grid = (unsigned)std::min<size_t>(bytes / 16 / 256 + 1, (size_t)kNumSMs * 2);
+  upload_kernel<<<grid, 256, 0, s>>>(dsrc, reinterpret_cast<uint8_t *>(dst), bytes);
+  PYFOF_CHECK_LAUNCH();
+  ctx.stage_used = off + bytes;
+  return kOk;
 }
 
 std::shared_ptr<GreenCache> g_green[64];
@@ -94,6 +147,9 @@ static int32_t create_context(int device, Context **out) {
   if ((e = cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
   if ((e = cudaEventCreateWithFlags(&c->ev_alloc, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
   if ((e = cudaEventCreateWithFlags(&c->ev_inputs, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+  if ((e = cudaEventCreateWithFlags(&c->ev_masses, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+  if ((e = cudaEventCreateWithFlags(&c->ev_pack, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+  if ((e = cudaEventCreateWithFlags(&c->ev_vel, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
   cudaMemPool_t pool;
   PYFOF_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
   uint64_t thr = UINT64_MAX;  // keep freed blocks cached in the pool
@@ -184,7 +240,21 @@ static void record_stage_times(Context &ctx) {
   cudaEventElapsedTime(&ctx.stage_ms[2], ctx.ev[3], ctx.ev[4]);
   cudaEventElapsedTime(&ctx.stage_ms[3], ctx.ev[2], ctx.ev[4]);
   ctx.stage_ms[4] = (float)ctx.conv_timer.ms;
+  // the part of "fof" before and after the (last region's) linking kernel
+  cudaEventElapsedTime(&ctx.stage_ms[9], ctx.ev[2], ctx.ev[0]);
+  cudaEventElapsedTime(&ctx.stage_ms[10], ctx.ev[1], ctx.ev[3]);
   cudaGetLastError();  // a region without linking leaves the link events unrecorded
+}
+
+// host-memory calls: [5] the position copy, [6] all input copies, [7] the
+// output copy, [8] the whole call from the first copy to the last
+static void record_copy_times(Context &ctx, bool side) {
+  cudaEventElapsedTime(&ctx.stage_ms[5], ctx.ev[5], ctx.ev[6]);
+  if (side) cudaEventElapsedTime(&ctx.stage_ms[6], ctx.ev[5], ctx.ev[8]);
+  else ctx.stage_ms[6] = ctx.stage_ms[5];
+  cudaEventElapsedTime(&ctx.stage_ms[7], ctx.ev[4], ctx.ev[7]);
+  cudaEventElapsedTime(&ctx.stage_ms[8], ctx.ev[5], ctx.ev[7]);
+  cudaGetLastError();
 }
 
 static int32_t run_common(Context &ctx, FofArgs &a) {
@@ -357,8 +427,10 @@ int32_t pyfof_last_stage_ms(const char *stage, float *ms) {
     return kInvalid;
   }
   if (get_context(g_default_device, &c) != kOk) return kInvalid;
-  static const char *names[5] = {"link", "fof", "unbind", "call", "pm_fft"};
-  for (int i = 0; i < 5; ++i)
+  static const char *names[11] = {"link", "fof", "unbind", "call", "pm_fft",
+                                  "h2d_positions", "h2d_inputs", "d2h", "host_call",
+                                  "before_link", "after_link"};
+  for (int i = 0; i < 11; ++i)
     if (!std::strcmp(stage, names[i])) {
       *ms = c->stage_ms[i];
       return kOk;
@@ -401,7 +473,7 @@ static int32_t run_host(Context &ctx, const double *xp, const double *vp, const 
                         int32_t verbose, double softening, double a_val, double b_val,
                         double s_15_val, int32_t n_threads, int64_t ng_val, double ng_global_val,
                         int32_t *in_halo, int32_t *halo_id, double *ang_mom, CatalogueOut *cat,
-                        const pyfof_units_t *units) {
+                        const pyfof_units_t *units, uint8_t *mask) {
   PYFOF_CUDA(cudaSetDevice(ctx.device));
   cudaStream_t s = ctx.stream;
   const size_t n = (size_t)total_np;
@@ -422,18 +494,20 @@ static int32_t run_host(Context &ctx, const double *xp, const double *vp, const 
     return kAlloc;
   }
   const bool side = vp || mp || fill_m;
-  if (side) {
-    // the buffers were allocated in the order of stream s
-    PYFOF_CUDA(cudaEventRecord(ctx.ev_alloc, s));
-    PYFOF_CUDA(cudaStreamWaitEvent(ctx.aux_stream, ctx.ev_alloc, 0));
-  }
   // conversions to code units run on the stream of their copy; the masses
   // are converted after their check, inside the call
+  ctx.timing = g_timing != 0;
+  if (ctx.timing) cudaEventRecord(ctx.ev[5], s);
   PYFOF_CUDA(cudaMemcpyAsync(xd, xp, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s));
   if (u.x_div != 1.0) PYFOF_TRY(divide_inplace(xd, (int64_t)(3 * n), u.x_div, s));
-  if (vp) {
-    PYFOF_CUDA(cudaMemcpyAsync(vd, vp, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx.aux_stream));
-    if (u.v_mul != 1.0) PYFOF_TRY(multiply_inplace(vd, (int64_t)(3 * n), u.v_mul, ctx.aux_stream));
+  if (ctx.timing) cudaEventRecord(ctx.ev[6], s);
+  if (side) {
+    // the other inputs follow the positions on the host link (the copies
+    // share its bandwidth, so the positions, which the linking needs, go
+    // first and the linking overlaps the rest); the buffers were allocated
+    // in the order of stream s
+    PYFOF_CUDA(cudaEventRecord(ctx.ev_alloc, s));
+    PYFOF_CUDA(cudaStreamWaitEvent(ctx.aux_stream, ctx.ev_alloc, 0));
   }
   if (mp) {
     PYFOF_CUDA(cudaMemcpyAsync(md, mp, sizeof(double) * n, cudaMemcpyHostToDevice, ctx.aux_stream));
@@ -441,9 +515,19 @@ static int32_t run_host(Context &ctx, const double *xp, const double *vp, const 
   } else if (fill_m) {
     PYFOF_TRY(fill_value(md, (int64_t)n, u.m_const, ctx.aux_stream));
   }
+  if (mp || fill_m) {
+    PYFOF_CUDA(cudaEventRecord(ctx.ev_masses, ctx.aux_stream));
+    a.masses_ready = ctx.ev_masses;
+  }
+  if (vp) {
+    PYFOF_CUDA(cudaMemcpyAsync(vd, vp, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx.aux_stream));
+    if (u.v_mul != 1.0) PYFOF_TRY(multiply_inplace(vd, (int64_t)(3 * n), u.v_mul, ctx.aux_stream));
+  }
   if (side) {
+    if (ctx.timing) cudaEventRecord(ctx.ev[8], ctx.aux_stream);
     PYFOF_CUDA(cudaEventRecord(ctx.ev_inputs, ctx.aux_stream));
     a.inputs_ready = ctx.ev_inputs;
+    a.input_stream = ctx.aux_stream;
   }
   PYFOF_CUDA(cudaMemsetAsync(a.in_halo, 0, sizeof(int32_t) * n, s));
   PYFOF_CUDA(cudaMemsetAsync(a.halo_id, 0, sizeof(int32_t) * n, s));
@@ -464,7 +548,6 @@ static int32_t run_host(Context &ctx, const double *xp, const double *vp, const 
   a.ng = ng_val;
   a.ng_global = ng_global_val;
   a.ang_mom = ang_mom;
-  ctx.timing = g_timing != 0;
   a.bound_fp64 = g_bound_fp64;
   a.bound_per_halo = g_bound_per_halo;
   a.big_np = g_big_np;
@@ -474,19 +557,42 @@ static int32_t run_host(Context &ctx, const double *xp, const double *vp, const 
   if (r == kOk && cat) r = build_catalogue(ctx, a.halo_id, (int64_t)n, cat->members, cat->offsets, cat->cap,
                                            cat->nfound);
   note_alloc_failure(ctx, r);
+  uint8_t *dmask = nullptr;
+  if (r == kOk && mask) {
+    dmask = ctx.work.carve<uint8_t>(n);
+    if (!dmask) {
+      set_error("device allocation failed for the membership mask");
+      r = kAlloc;
+    } else {
+      r = member_mask(a.halo_id, (int64_t)n, dmask, s);
+    }
+  }
   if (r == kOk) {
-    if (in_halo) cudaMemcpyAsync(in_halo, a.in_halo, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(halo_id, a.halo_id, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);
+    if (mask) {
+      cudaMemcpyAsync(mask, dmask, n, cudaMemcpyDeviceToHost, s);
+    } else {
+      if (in_halo) cudaMemcpyAsync(in_halo, a.in_halo, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(halo_id, a.halo_id, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s);
+    }
+    if (ctx.timing) cudaEventRecord(ctx.ev[7], s);
   }
   // an early failure may leave the side copies in flight: their buffers are
   // released in the order of stream s, after them
-  if (side) cudaStreamWaitEvent(s, ctx.ev_inputs, 0);
+  if (side) {
+    // everything the call queued on the input stream (its copies and the
+    // velocity pack of the unbinding)
+    cudaEventRecord(ctx.ev_inputs, ctx.aux_stream);
+    cudaStreamWaitEvent(s, ctx.ev_inputs, 0);
+  }
   cudaError_t e = cudaStreamSynchronize(s);
   if (r == kOk && e != cudaSuccess) {
     set_error("CUDA failure: %s", cudaGetErrorString(e));
     r = kCuda;
   }
-  if (ctx.timing && r == kOk) record_stage_times(ctx);
+  if (ctx.timing && r == kOk) {
+    record_stage_times(ctx);
+    record_copy_times(ctx, side);
+  }
   ctx.last_peak_bytes = (int64_t)ctx.work.peak;
   ctx.work.peak = 0;
   ctx.work.release();
@@ -503,12 +609,13 @@ static int32_t run_host_checked(Context *ctx, const double *xp, const double *vp
                                 double b_val, double s_15_val, int32_t n_threads, int64_t ng_val,
                                 double ng_global_val, int32_t *in_halo, int32_t *halo_id,
                                 double *ang_mom, CatalogueOut *cat = nullptr,
-                                const pyfof_units_t *units = nullptr) {
+                                const pyfof_units_t *units = nullptr, uint8_t *mask = nullptr) {
   // outputs are written in full on success and zeroed on every other path
   auto zero = [&]() {
     if (total_np > 0) {
       if (in_halo) std::memset(in_halo, 0, sizeof(int32_t) * (size_t)total_np);
       if (halo_id) std::memset(halo_id, 0, sizeof(int32_t) * (size_t)total_np);
+      if (mask) std::memset(mask, 0, (size_t)total_np);
     }
     if (ang_mom && nhalo > 0) std::memset(ang_mom, 0, sizeof(double) * 3 * (size_t)nhalo);
   };
@@ -521,7 +628,7 @@ static int32_t run_host_checked(Context *ctx, const double *xp, const double *vp
     }
     return kOk;
   }
-  if (r == kOk && (!xp || !halo_id || !ang_mom)) {
+  if (r == kOk && (!xp || !(halo_id || mask) || !ang_mom)) {
     set_error("null argument");
     r = kInvalid;
   }
@@ -535,7 +642,7 @@ static int32_t run_host_checked(Context *ctx, const double *xp, const double *vp
     std::lock_guard<std::mutex> lk(ctx->mu);
     r = run_host(*ctx, xp, vp, mp, layout, np_halo, nhalo, total_np, L_Box, linking_length,
                  np_halo_min, bound_check, verbose, softening, a_val, b_val, s_15_val, n_threads,
-                 ng_val, ng_global_val, in_halo, halo_id, ang_mom, cat, units);
+                 ng_val, ng_global_val, in_halo, halo_id, ang_mom, cat, units, mask);
   }
   if (r != kOk) zero();
   return r;
@@ -626,6 +733,26 @@ int32_t pyfof_run_units(void *slot, const pyfof_units_t *units, const double *xp
                           linking_length, np_halo_min, bound_check, verbose, softening, a_val, b_val,
                           s_15_val, n_threads, ng_val, ng_global_val, in_halo, halo_id, ang_mom, nullptr,
                           units);
+}
+
+int32_t pyfof_run_mask(void *slot, const pyfof_units_t *units, const double *xp, const double *vp,
+                       const double *mp, int32_t layout, const int32_t *np_halo, int32_t nhalo,
+                       int64_t total_np, double L_Box, double linking_length, int32_t np_halo_min,
+                       int32_t bound_check, int32_t verbose, double softening, double a_val,
+                       double b_val, double s_15_val, int32_t n_threads, int64_t ng_val,
+                       double ng_global_val, uint8_t *in_halo, double *ang_mom) {
+  if (slot && static_cast<Context *>(slot)->magic != Context::kMagic) {
+    set_error("pyfof_run_mask: not a slot");
+    return kInvalid;
+  }
+  if (!in_halo && total_np > 0 && nhalo > 0) {
+    set_error("pyfof_run_mask: null in_halo");
+    return kInvalid;
+  }
+  return run_host_checked(static_cast<Context *>(slot), xp, vp, mp, layout, np_halo, nhalo, total_np, L_Box,
+                          linking_length, np_halo_min, bound_check, verbose, softening, a_val, b_val,
+                          s_15_val, n_threads, ng_val, ng_global_val, nullptr, nullptr, ang_mom, nullptr,
+                          units, in_halo);
 }
 
 int32_t pyfof_run_catalogue(void *slot, const pyfof_units_t *units, const double *xp, const double *vp,

@@ -60,7 +60,12 @@ struct Context {
   // on first use); ev_fork/ev_join order it after and before `stream`
   cudaStream_t side_stream = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  cudaEvent_t ev_alloc = nullptr, ev_inputs = nullptr;
+  cudaEvent_t ev_alloc = nullptr, ev_inputs = nullptr, ev_masses = nullptr;
+  // unbinding: members packed (stream) and their velocities packed on the
+  // input stream; vel_wait is ev_vel while such a pack is pending, and
+  // every kernel that reads member velocities is ordered after it
+  // (wait_velocities)
+  cudaEvent_t ev_pack = nullptr, ev_vel = nullptr, vel_wait = nullptr;
   Arena work;    // per-call device memory, released at the end of every call
   int32_t *d_flags = nullptr;  // device status words (error codes, counters)
   int32_t *h_flags = nullptr;  // pinned mirror
@@ -68,7 +73,7 @@ struct Context {
   std::shared_ptr<GreenCache> green;
   size_t pm_budget = (size_t)8 << 30;  // particle-mesh grid batch bytes
   int64_t last_peak_bytes = 0;         // device memory the last call held at most
-  cudaEvent_t ev[8] = {};
+  cudaEvent_t ev[10] = {};
   // timing of the last call's stages (ms), filled when timing is enabled
   bool timing = false;
   float stage_ms[16] = {};
@@ -83,8 +88,32 @@ struct Context {
   int64_t last_max_cell = 0;    // particles in the fullest cell
   int64_t last_cell_sorts = 0;  // 1: cell order by per-cell sorts, 0: by the radix sort
   int64_t last_direct = 0, last_pm = 0, last_valid = 0, last_tl_regions = 0;
+  // host tables bound for the device: pinned, device-mapped staging that a
+  // kernel reads (see upload); bump-allocated within a call and reset by
+  // stage_reset at the start of the next one, when the previous call has
+  // synchronised.  A buffer outgrown during a call is kept until the
+  // context is destroyed (freeing pinned memory synchronises the device).
+  uint8_t *h_stage = nullptr;
+  size_t stage_cap = 0, stage_used = 0;
+  std::vector<uint8_t *> stage_retired;
+  void stage_reset() { stage_used = 0; }
   ~Context();
 };
+
+// Copies `bytes` of host memory to device memory in the order of stream s.
+// A copy of more than a few KB from the host is a copy-engine transfer that
+// queues behind the large input copies another stream has in flight (the
+// velocities and masses, or another slot's inputs); so the bytes go into
+// the context's pinned staging and a kernel reads them from there over the
+// host link, which nothing queues behind.  Small copies stay
+// cudaMemcpyAsync (the driver passes them inline).  `src` may be reused as
+// soon as upload returns.
+int32_t upload(Context &ctx, void *dst, const void *src, size_t bytes, cudaStream_t s);
+
+// Orders stream s after the pending velocity pack of the call, if any.
+inline cudaError_t wait_velocities(Context &ctx, cudaStream_t s) {
+  return ctx.vel_wait ? cudaStreamWaitEvent(s, ctx.vel_wait, 0) : cudaSuccess;
+}
 
 // Returns the context of `device`, creating it on first use.
 int32_t get_context(int device, Context **out);

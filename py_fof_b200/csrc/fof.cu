@@ -1293,15 +1293,13 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
   Tile *dT = W.carve<Tile>(std::max<int64_t>(ntiles, 1));
   unsigned long long *dbb = W.carve<unsigned long long>(6 * (size_t)nreg);
   if (!dR || !dT || !dbb) { set_error("workspace exhausted (regions)"); return kAlloc; }
-  PYFOF_CUDA(cudaMemcpyAsync(dR, reg.data(), sizeof(RegionDev) * nreg, cudaMemcpyHostToDevice, s));
-  if (ntiles)
-    PYFOF_CUDA(cudaMemcpyAsync(dT, tiles.data(), sizeof(Tile) * ntiles, cudaMemcpyHostToDevice, s));
+  PYFOF_TRY(upload(ctx, dR, reg.data(), sizeof(RegionDev) * nreg, s));
+  PYFOF_TRY(upload(ctx, dT, tiles.data(), sizeof(Tile) * ntiles, s));
   {
     std::vector<unsigned long long> init(6 * (size_t)nreg);
     for (int r = 0; r < nreg; ++r)
       for (int d = 0; d < 3; ++d) { init[6 * r + d] = ~0ull; init[6 * r + 3 + d] = 0ull; }
-    PYFOF_CUDA(cudaMemcpyAsync(dbb, init.data(), sizeof(unsigned long long) * init.size(),
-                               cudaMemcpyHostToDevice, s));
+    PYFOF_TRY(upload(ctx, dbb, init.data(), sizeof(unsigned long long) * init.size(), s));
   }
   PYFOF_CUDA(cudaMemsetAsync(ctx.d_flags, 0, sizeof(int32_t) * FLAG_COUNT, s));
   if (ntiles) {
@@ -1347,7 +1345,7 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
   st.total_cells = total_cells;
   ctx.last_cells = (int64_t)total_cells;
   ctx.last_active = n_active;
-  PYFOF_CUDA(cudaMemcpyAsync(dR, reg.data(), sizeof(RegionDev) * nreg, cudaMemcpyHostToDevice, s));
+  PYFOF_TRY(upload(ctx, dR, reg.data(), sizeof(RegionDev) * nreg, s));
   uint64_t *dcoff = W.carve<uint64_t>(nreg + 1);
   uint32_t *keys = W.carve<uint32_t>(std::max<int64_t>(n, 1));
   uint32_t *cstart = W.carve<uint32_t>(total_cells + 2);
@@ -1359,8 +1357,7 @@ int32_t fof_link_stage(Context &ctx, const FofArgs &a, FofState &st) {
     set_error("workspace exhausted (keys)");
     return kAlloc;
   }
-  PYFOF_CUDA(cudaMemcpyAsync(dcoff, cell_off.data(), sizeof(uint64_t) * (nreg + 1),
-                             cudaMemcpyHostToDevice, s));
+  PYFOF_TRY(upload(ctx, dcoff, cell_off.data(), sizeof(uint64_t) * (nreg + 1), s));
   PYFOF_CUDA(cudaMemsetAsync(cstart, 0, sizeof(uint32_t) * (total_cells + 2), s));
   const uint32_t sentinel = (uint32_t)total_cells;
   // slots within the cells go to va (radix scratch when the sort is needed)
@@ -1675,6 +1672,21 @@ __global__ void fill_kernel(double *__restrict__ x, int64_t n, double v) {
     x[i] = v;
 }
 
+// mask[i] = halo_id[i] > 0 as 0/1 bytes, four particles per thread
+__global__ void member_mask_kernel(const int32_t *__restrict__ id, int64_t n, uint8_t *__restrict__ mask) {
+  const int64_t n4 = n / 4;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+    const int4 v = reinterpret_cast<const int4 *>(id)[i];
+    const uint32_t w = (uint32_t)(v.x > 0) | ((uint32_t)(v.y > 0) << 8) | ((uint32_t)(v.z > 0) << 16) |
+                       ((uint32_t)(v.w > 0) << 24);
+    reinterpret_cast<uint32_t *>(mask)[i] = w;
+  }
+  if (blockIdx.x == 0 && threadIdx.x < (unsigned)(n - 4 * n4)) {
+    const int64_t i = 4 * n4 + threadIdx.x;
+    mask[i] = id[i] > 0 ? 1 : 0;
+  }
+}
+
 static unsigned stream_grid(int64_t n) {
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, BLK), (int64_t)kNumSMs * 8));
 }
@@ -1700,6 +1712,13 @@ int32_t fill_value(double *x, int64_t n, double v, cudaStream_t s) {
   return kOk;
 }
 
+int32_t member_mask(const int32_t *halo_id, int64_t n, uint8_t *mask, cudaStream_t s) {
+  if (n <= 0) return kOk;
+  member_mask_kernel<<<stream_grid(ceil_div(n, 4)), BLK, 0, s>>>(halo_id, n, mask);
+  PYFOF_CHECK_LAUNCH();
+  return kOk;
+}
+
 int32_t check_masses(Context &ctx, const double *mp, int64_t n, double m_div) {
   cudaStream_t s = ctx.stream;
   int32_t *bad = ctx.d_flags + FLAG_COUNT_C;
@@ -1719,17 +1738,23 @@ int32_t check_masses(Context &ctx, const double *mp, int64_t n, double m_div) {
 
 int32_t fof_run(Context &ctx, const FofArgs &a) {
   FofState st;
+  ctx.stage_reset();
   ctx.conv_timer.reset();
   ctx.last_pm_solves = 0;
   ctx.last_pm_fft_bytes = 0.0;
   if (ctx.timing) cudaEventRecord(ctx.ev[2], ctx.stream);
   PYFOF_TRY(fof_link_stage(ctx, a, st));
   PYFOF_TRY(fof_candidates_stage(ctx, a, st, !a.bound_check));
-  if (a.inputs_ready) PYFOF_CUDA(cudaStreamWaitEvent(ctx.stream, a.inputs_ready, 0));
+  if (a.masses_ready) PYFOF_CUDA(cudaStreamWaitEvent(ctx.stream, a.masses_ready, 0));
   if (a.mp) PYFOF_TRY(check_masses(ctx, a.mp, a.total_np, a.m_div));
   if (ctx.timing) cudaEventRecord(ctx.ev[3], ctx.stream);
-  if (!a.bound_check) PYFOF_TRY(fof_plain_angmom(ctx, a, st));
-  else PYFOF_TRY(unbind_stage(ctx, a, st));
+  if (!a.bound_check) {
+    if (a.inputs_ready) PYFOF_CUDA(cudaStreamWaitEvent(ctx.stream, a.inputs_ready, 0));
+    PYFOF_TRY(fof_plain_angmom(ctx, a, st));
+  } else {
+    // the velocities may still be copying: unbind_stage orders their use
+    PYFOF_TRY(unbind_stage(ctx, a, st));
+  }
   if (ctx.timing) cudaEventRecord(ctx.ev[4], ctx.stream);
   return kOk;
 }

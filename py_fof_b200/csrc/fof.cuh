@@ -46,9 +46,13 @@ struct FofArgs {
   // masses are divided by m_div right after their check (code units); only
   // with mp in the library's own scratch, which the check then rewrites
   double m_div = 1.0;
-  // recorded when vp and mp are on the device (they may still be copying
-  // while the linking runs); null when they are already there
-  cudaEvent_t inputs_ready = nullptr;
+  // host-memory calls: masses_ready is recorded on `input_stream` when mp
+  // is on the device, inputs_ready when vp is too (they copy while the
+  // linking runs; the velocities arrive last and are packed for the
+  // unbinding on that stream, see unbind_stage); null when the inputs are
+  // already on the device
+  cudaEvent_t masses_ready = nullptr, inputs_ready = nullptr;
+  cudaStream_t input_stream = nullptr;
   // outputs (device): in_halo, halo_id (N int32); ang_mom host (3,nhalo) F-order
   int32_t *in_halo = nullptr, *halo_id = nullptr;
   double *ang_mom = nullptr;
@@ -62,6 +66,9 @@ struct Context;
 int32_t divide_inplace(double *x, int64_t n, double d, cudaStream_t s);
 int32_t multiply_inplace(double *x, int64_t n, double f, cudaStream_t s);
 int32_t fill_value(double *x, int64_t n, double v, cudaStream_t s);
+// mask[i] = (halo_id[i] > 0) as 0/1 bytes; halo_id 16-byte aligned, mask
+// 4-byte aligned
+int32_t member_mask(const int32_t *halo_id, int64_t n, uint8_t *mask, cudaStream_t s);
 
 // Runs the whole call on ctx's stream; returns a reference ierr code (or
 // kCuda).  Synchronises the stream before returning.

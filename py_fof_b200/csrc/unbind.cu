@@ -49,7 +49,7 @@ __global__ void ub_fill_kernel(uint32_t *a, int64_t n, uint32_t v) {
 
 // xv packing (fof_fortran.f90:297-305): positions unwrapped about the
 // candidate's first CRS member in FP64, then rounded to FP32.
-__global__ void ub_pack_kernel(Coords xp, Coords vp, const double *__restrict__ mp,
+__global__ void ub_pack_kernel(Coords xp, const double *__restrict__ mp,
                                const uint32_t *__restrict__ mcand,
                                const uint32_t *__restrict__ midx,
                                const int64_t *__restrict__ cand_anchor, int64_t M, double L,
@@ -60,12 +60,20 @@ __global__ void ub_pack_kernel(Coords xp, Coords vp, const double *__restrict__ 
     const int64_t i = midx[k];
     const int64_t a = cand_anchor[c];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      m.q[d][k] = __double2float_rn(unwrap(xp.get(i, d), xp.get(a, d), half, L));
-      m.v[d][k] = __double2float_rn(vp.get(i, d));
-    }
+    for (int d = 0; d < 3; ++d) m.q[d][k] = __double2float_rn(unwrap(xp.get(i, d), xp.get(a, d), half, L));
     m.w[k] = mp ? __double2float_rn(mp[i]) : 1.0f;
     m.pid[k] = (int32_t)i;
+  }
+}
+
+// The members' velocities, packed apart from the rest: in a host-memory
+// call they are the last input to arrive.
+__global__ void ub_pack_v_kernel(Coords vp, const uint32_t *__restrict__ midx, int64_t M, Members m) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = midx[k];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) m.v[d][k] = __double2float_rn(vp.get(i, d));
   }
 }
 
@@ -416,7 +424,7 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
   std::vector<int64_t> hoff(ncand + 1, 0);
   for (int c = 0; c < ncand; ++c) hoff[c + 1] = hoff[c] + cnp[c];
   const int64_t M = hoff[ncand];
-  PYFOF_CUDA(cudaMemcpyAsync(off, hoff.data(), sizeof(int64_t) * (ncand + 1), cudaMemcpyHostToDevice, s));
+  PYFOF_TRY(upload(ctx, off, hoff.data(), sizeof(int64_t) * (ncand + 1), s));
   Members m;
   for (int d = 0; d < 3; ++d) {
     m.q[d] = W.carve<float>(M);
@@ -430,8 +438,32 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
   uint8_t *keep = W.carve<uint8_t>(M);
   if (!m.w || !m.pid || !lo || !span || !res || !keep) { set_error("workspace exhausted (xv)"); return kAlloc; }
   const unsigned grid_m = (unsigned)std::min<int64_t>(ceil_div(M, BLK), (int64_t)kNumSMs * 16);
-  ub_pack_kernel<<<grid_m, BLK, 0, s>>>(xp, vp, a.mp, mcand, midx, st.cand_anchor, M, L, half, m);
+  ub_pack_kernel<<<grid_m, BLK, 0, s>>>(xp, a.mp, mcand, midx, st.cand_anchor, M, L, half, m);
   PYFOF_CHECK_LAUNCH();
+  // The velocities of a host-memory call may still be copying: their pack
+  // runs on the input stream after the copy, and the kernels that read
+  // them wait for it (wait_velocities); every return orders `s` after it
+  // (the caller frees this call's memory on `s`).
+  struct VelocityJoin {
+    Context &c;
+    cudaStream_t s;
+    ~VelocityJoin() {
+      if (c.vel_wait) cudaStreamWaitEvent(s, c.vel_wait, 0);
+      c.vel_wait = nullptr;
+    }
+  } velocity_join{ctx, s};
+  if (a.inputs_ready && a.input_stream) {
+    PYFOF_CUDA(cudaEventRecord(ctx.ev_pack, s));
+    PYFOF_CUDA(cudaStreamWaitEvent(a.input_stream, ctx.ev_pack, 0));
+    PYFOF_CUDA(cudaStreamWaitEvent(a.input_stream, a.inputs_ready, 0));
+    ub_pack_v_kernel<<<grid_m, BLK, 0, a.input_stream>>>(vp, midx, M, m);
+    PYFOF_CHECK_LAUNCH();
+    PYFOF_CUDA(cudaEventRecord(ctx.ev_vel, a.input_stream));
+    ctx.vel_wait = ctx.ev_vel;
+  } else {
+    ub_pack_v_kernel<<<grid_m, BLK, 0, s>>>(vp, midx, M, m);
+    PYFOF_CHECK_LAUNCH();
+  }
   ub_span_kernel<<<ncand, BLK, 0, s>>>(m, off, lo, span);
   PYFOF_CHECK_LAUNCH();
 
@@ -492,8 +524,7 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
   if (!direct.empty()) {
     int32_t *dl = W.carve<int32_t>(direct.size());
     if (!dl) { set_error("workspace exhausted (direct list)"); return kAlloc; }
-    PYFOF_CUDA(cudaMemcpyAsync(dl, direct.data(), sizeof(int32_t) * direct.size(),
-                               cudaMemcpyHostToDevice, s));
+    PYFOF_TRY(upload(ctx, dl, direct.data(), sizeof(int32_t) * direct.size(), s));
     direct::DirectParams P;
     P.fac = a.a_val / (6.0 * kPi);
     P.app = a.softening;
@@ -523,7 +554,7 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
       double *phi1 = W.carve<double>((size_t)std::max<int64_t>(M, 1));
       int32_t *dbl = W.carve<int32_t>(direct.size());
       if (!dtl || !phi1 || !dbl) { set_error("workspace exhausted (direct potentials)"); return kAlloc; }
-      PYFOF_CUDA(cudaMemcpyAsync(dtl, tl.data(), sizeof(int2) * tl.size(), cudaMemcpyHostToDevice, s));
+      PYFOF_TRY(upload(ctx, dtl, tl.data(), sizeof(int2) * tl.size(), s));
       if (a.bound_fp64)
         direct::ub_direct_phi1_kernel<true><<<(unsigned)tl.size(), direct::PT, 0, s>>>(m, off, dl, dtl, P, phi1);
       else
@@ -542,11 +573,12 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
                          [&](int32_t x, int32_t y) { return tasks[x].np > tasks[y].np; });
         bstart[b + 1] = bl.size();
       }
-      PYFOF_CUDA(cudaMemcpyAsync(dbl, bl.data(), sizeof(int32_t) * bl.size(), cudaMemcpyHostToDevice, s));
+      PYFOF_TRY(upload(ctx, dbl, bl.data(), sizeof(int32_t) * bl.size(), s));
       // the removal loops run on the side stream, overlapping the
       // particle-mesh halos on `s` (disjoint halos, disjoint outputs)
       PYFOF_TRY(fork_side(ctx, s));
       side_forked = true;
+      PYFOF_CUDA(wait_velocities(ctx, ctx.side_stream));
       for (int b = 5; b >= 0; --b) {
         const unsigned nb = (unsigned)(bstart[b + 1] - bstart[b]);
         if (!nb) continue;
@@ -588,6 +620,9 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
     PYFOF_CUDA(cudaStreamWaitEvent(s, ctx.ev_join, 0));
     side_forked = false;
   }
+  // the outputs read the velocities too
+  PYFOF_CUDA(wait_velocities(ctx, s));
+  ctx.vel_wait = nullptr;
   PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   PYFOF_CUDA(cudaStreamSynchronize(s));
   if (ctx.h_flags[FLAG_ERR]) {
@@ -640,6 +675,7 @@ int32_t unbind_potential(Context &ctx, const float *q_soa, const float *w, int32
                          float *phi, int32_t *method) {
   cudaStream_t s = ctx.stream;
   Arena &W = ctx.work;
+  ctx.stage_reset();
   GridRules rules;
   rules.init(ng, s15);
   if (rules.ngrid != 4 || np <= 0) {

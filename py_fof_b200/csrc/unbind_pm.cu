@@ -1566,6 +1566,7 @@ int32_t big_removal(Context &ctx, const Members &m, BigHalo *dB, int nbig, const
     // iterations until every big halo left the inner loop; the host looks
     // every few iterations (an iteration removes >= 2 % of a halo, and a pass
     // ends after 20 %)
+    PYFOF_CUDA(wait_velocities(ctx, s));
     for (int it = 0; it < 1 << 20; it += 4) {
       for (int j = 0; j < 4; ++j) {
         big_com_kernel<<<nchb, 256, 0, s>>>(m, dCh, dB, keep, part);
@@ -1636,9 +1637,9 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
   }
   std::vector<int32_t> hl(nh);
   for (int h = 0; h < nh; ++h) hl[h] = h;
-  PYFOF_CUDA(cudaMemcpyAsync(dH, H.data(), sizeof(PmHalo) * nh, cudaMemcpyHostToDevice, s));
-  PYFOF_CUDA(cudaMemcpyAsync(dlist, hl.data(), sizeof(int32_t) * nh, cudaMemcpyHostToDevice, s));
-  PYFOF_CUDA(cudaMemcpyAsync(dselfs, selfs.data(), sizeof(R *) * nh, cudaMemcpyHostToDevice, s));
+  PYFOF_TRY(upload(ctx, dH, H.data(), sizeof(PmHalo) * nh, s));
+  PYFOF_TRY(upload(ctx, dlist, hl.data(), sizeof(int32_t) * nh, s));
+  PYFOF_TRY(upload(ctx, dselfs, selfs.data(), sizeof(R *) * nh, s));
   const unsigned gM = (unsigned)std::min<int64_t>(ceil_div(M, BLK), (int64_t)kNumSMs * 16);
   pm_fill_i32<<<gM, BLK, 0, s>>>(mhalo, M, -1);
   PYFOF_CHECK_LAUNCH();
@@ -1723,7 +1724,7 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
     ncell += c;
   }
   if (ncell >= 0xffffffffll) { set_error("too many C2 cells"); return kAlloc; }
-  PYFOF_CUDA(cudaMemcpyAsync(dH, H.data(), sizeof(PmHalo) * nh, cudaMemcpyHostToDevice, s));
+  PYFOF_TRY(upload(ctx, dH, H.data(), sizeof(PmHalo) * nh, s));
   uint32_t *ckey = W.carve<uint32_t>(M), *cstart = W.carve<uint32_t>(ncell + 2);
   uint32_t *ka = W.carve<uint32_t>(M), *va = W.carve<uint32_t>(M), *kb = W.carve<uint32_t>(M),
            *vb = W.carve<uint32_t>(M);
@@ -1785,8 +1786,8 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
     uint8_t *dregr = W.carve<uint8_t>((size_t)nh * 512);
     int32_t *dact_of = W.carve<int32_t>((size_t)nh * 512);
     if (!dregr || !dact_of) { set_error("workspace exhausted (two-level)"); return kAlloc; }
-    PYFOF_CUDA(cudaMemcpyAsync(dregr, region_r.data(), (size_t)nh * 512, cudaMemcpyHostToDevice, s));
-    PYFOF_CUDA(cudaMemcpyAsync(dact_of, act_of.data(), sizeof(int32_t) * nh * 512, cudaMemcpyHostToDevice, s));
+    PYFOF_TRY(upload(ctx, dregr, region_r.data(), (size_t)nh * 512, s));
+    PYFOF_TRY(upload(ctx, dact_of, act_of.data(), sizeof(int32_t) * nh * 512, s));
     tl_particle_kernel<<<gM, BLK, 0, s>>>(m, dH, mhalo, M, dregr, dact_of, pr, preg);
     PYFOF_CHECK_LAUNCH();
     if (na > 0) {
@@ -1795,7 +1796,7 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
       src_start = W.carve<uint32_t>(na + 1);
       tgt_start = W.carve<uint32_t>(na + 1);
       if (!dA || !cnt || !src_start || !tgt_start) { set_error("workspace exhausted (two-level)"); return kAlloc; }
-      PYFOF_CUDA(cudaMemcpyAsync(dA, act.data(), sizeof(TlRegion) * na, cudaMemcpyHostToDevice, s));
+      PYFOF_TRY(upload(ctx, dA, act.data(), sizeof(TlRegion) * na, s));
       // sources
       PYFOF_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (na + 1), s));
       tl_source_kernel<<<gM, BLK, 0, s>>>(m, dH, mhalo, M, dact_of, dA, cnt, nullptr, 0);
@@ -1924,8 +1925,8 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
       set_error("workspace exhausted (large halos)");
       return kAlloc;
     }
-    PYFOF_CUDA(cudaMemcpyAsync(dB, hbig.data(), sizeof(BigHalo) * nbig, cudaMemcpyHostToDevice, s));
-    PYFOF_CUDA(cudaMemcpyAsync(dCh, hch.data(), sizeof(BigChunk) * nchb, cudaMemcpyHostToDevice, s));
+    PYFOF_TRY(upload(ctx, dB, hbig.data(), sizeof(BigHalo) * nbig, s));
+    PYFOF_TRY(upload(ctx, dCh, hch.data(), sizeof(BigChunk) * nchb, s));
   }
   for (int pass = 1; pass <= kMaxPasses; ++pass) {
     std::vector<int32_t> pend;
@@ -1934,8 +1935,7 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
     std::vector<int32_t> pend_small;
     for (int h : pend) if (!is_big[h]) pend_small.push_back(h);
     if (!pend_small.empty()) {
-      PYFOF_CUDA(cudaMemcpyAsync(dpend, pend_small.data(), sizeof(int32_t) * pend_small.size(),
-                                 cudaMemcpyHostToDevice, s));
+      PYFOF_TRY(upload(ctx, dpend, pend_small.data(), sizeof(int32_t) * pend_small.size(), s));
       pm_mkeep_kernel<<<(unsigned)pend_small.size(), 256, 0, s>>>(m, dH, dpend, (int)pend_small.size(), keep);
       PYFOF_CHECK_LAUNCH();
     }
@@ -1956,8 +1956,8 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
         // the batch's halos, their member prefix and their first cmem position
         std::vector<uint32_t> bp((size_t)nb + 1, 0);
         for (int j = 0; j < nb; ++j) bp[j + 1] = bp[j] + (uint32_t)H[grp[g0 + j]].np;
-        PYFOF_CUDA(cudaMemcpyAsync(dbatch, grp.data() + g0, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s));
-        PYFOF_CUDA(cudaMemcpyAsync(dbpre, bp.data(), sizeof(uint32_t) * (nb + 1), cudaMemcpyHostToDevice, s));
+        PYFOF_TRY(upload(ctx, dbatch, grp.data() + g0, sizeof(int32_t) * nb, s));
+        PYFOF_TRY(upload(ctx, dbpre, bp.data(), sizeof(uint32_t) * (nb + 1), s));
         unsigned long long *acc = reinterpret_cast<unsigned long long *>(scratch);
         R *rho = reinterpret_cast<R *>(scratch);  // the convolved grids overwrite acc
         cplx_t<R> *spec = reinterpret_cast<cplx_t<R> *>(
@@ -2002,8 +2002,8 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
           bp[j + 1] = bp[j] + (hsrc[ia + 1] - hsrc[ia]);
           bp[nb + 1 + j + 1] = bp[nb + 1 + j] + (htgt[ia + 1] - htgt[ia]);
         }
-        PYFOF_CUDA(cudaMemcpyAsync(dbatch, regs.data() + g0, sizeof(int32_t) * nb, cudaMemcpyHostToDevice, s));
-        PYFOF_CUDA(cudaMemcpyAsync(dbpre, bp.data(), sizeof(uint32_t) * bp.size(), cudaMemcpyHostToDevice, s));
+        PYFOF_TRY(upload(ctx, dbatch, regs.data() + g0, sizeof(int32_t) * nb, s));
+        PYFOF_TRY(upload(ctx, dbpre, bp.data(), sizeof(uint32_t) * bp.size(), s));
         const int64_t ng = (int64_t)nb * sup * sup * sup;
         PYFOF_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * ng, s));
         pm_batch_scale_kernel<<<(unsigned)ceil_div(nb, 128), 128, 0, s>>>(dH, dbatch, nb, dA, dinv);
@@ -2038,6 +2038,7 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
       PYFOF_CHECK_LAUNCH();
     }
     if (!pend_small.empty()) {
+      PYFOF_CUDA(wait_velocities(ctx, s));
       pm_inner_kernel<R><<<(unsigned)pend_small.size(), IBLK, 0, s>>>(m, dH, dpend, (int)pend_small.size(), keep,
                                                                      jd, c1, phi_in, c2, phi, en,
                                                                      (float)a.b_val, a.np_halo_min, phi_only,
@@ -2062,7 +2063,7 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
     hr[h].np_bound = H[h].np_bound;
   }
   for (int h = 0; h < nh; ++h)
-    PYFOF_CUDA(cudaMemcpyAsync(res + list[h], &hr[h], sizeof(HaloResult), cudaMemcpyHostToDevice, s));
+    PYFOF_TRY(upload(ctx, res + list[h], &hr[h], sizeof(HaloResult), s));
   if (phi_out) PYFOF_CUDA(cudaMemcpyAsync(phi_out, phi, sizeof(float) * M, cudaMemcpyDeviceToDevice, s));
   PYFOF_CUDA(cudaStreamSynchronize(s));
   return kOk;

@@ -296,3 +296,50 @@ def test_very_dense_periodic_clumps(seed):
     o = oracle_core(xp, **kw)
     assert np.array_equal(g[0], o[0])
     assert np.array_equal(g[1], o[1])
+
+
+@pytest.mark.parametrize("n", [1, 3, 4, 5, 4099, 20 ** 3 + 3])
+def test_mask_entry_point_matches_halo_ids(n):
+    """pyfof_run_mask (what fof() calls) returns halo_id > 0 as bytes, for
+    sizes that leave 0-3 particles past the last group of four."""
+    rng = np.random.default_rng(n)
+    L = 20.0
+    xp = np.hstack([rng.uniform(0, L, (3, n // 2)),
+                    rng.normal(L / 2, 0.3, (3, n - n // 2))])
+    full = P._fof_core(xp, L_Box=L, linking_length=0.2, np_halo_min=2)
+    in_halo, hid, am, ierr = _native.run(xp, None, None, [n], 1, L, 0.2, 2, 0, 0, 0.1, 1.0, 0.0,
+                                         17.152, 0, n, mask_only=True)
+    assert ierr == 0 and hid is None and in_halo.dtype == np.bool_
+    assert np.array_equal(in_halo, full[1] > 0)
+    assert np.array_equal(P.fof(xp, L_Box=L, linking_length=0.2, np_halo_min=2), full[0])
+
+
+def test_mask_public_fof_with_unbinding_and_regions():
+    """fof() through the mask entry point against _fof_core: isolated bound
+    clumps as a list of regions (some below np_halo_min), with unbinding."""
+    from tests.test_unbind_gpu import clumps
+    xs, vs, ms = clumps(7, n_regions=12, nmin=5, nmax=600, masses=True)
+    xs.insert(3, xs[3][:, :4].copy())  # a region below np_halo_min
+    vs.insert(3, vs[3][:, :4].copy())
+    ms.insert(3, ms[3][:4].copy())
+    kw = dict(vp_list=vs, mp_list=ms, L_Box=512.0, linking_length=0.3, np_halo_min=10,
+              bound_check=True, return_ang_mom=True)
+    core = P._fof_core(xs, **kw)
+    ih, am = P.fof(xs, **kw)
+    assert core[1].max() > 0 and min(x.shape[1] for x in xs) < 10
+    assert ih.dtype == np.bool_
+    # ang_mom sums members with atomics: equal to rounding
+    assert np.array_equal(ih, core[0]) and angmom_close(am, core[2], np.abs(core[2]).max() + 1.0)
+    # one periodic box, positions only
+    d = W.plummer_box(24 ** 3, 24.0, 4, seed=21)
+    core = P._fof_core(d["xp"], L_Box=24.0, linking_length=0.2, np_halo_min=10)
+    assert core[1].max() > 0
+    assert np.array_equal(P.fof(d["xp"], L_Box=24.0, linking_length=0.2, np_halo_min=10), core[0])
+
+
+def test_mask_zeroed_on_failure():
+    xp = np.zeros((3, 6))
+    xp[0, 2] = np.nan
+    in_halo, _, am, ierr = _native.run(xp, None, None, [6], 1, 10.0, 0.2, 1, 0, 0, 0.1, 1.0, 0.0,
+                                       17.152, 0, 6, mask_only=True)
+    assert ierr == 4 and not in_halo.any() and not am.any()
