@@ -95,7 +95,8 @@ int32_t pyfof_set_stream(void *stream);
  * cell order came from per-cell sorts, 0 from the radix sort),
  * "direct_halos" / "pm_halos" (candidates unbound by direct summation / the
  * particle mesh), "valid_halos" (halos written to the output),
- * "refined_regions" (two-level inner regions), "pm_solves" (halo-grid
+ * "refined_regions" (two-level inner regions), "pm_passes" (passes of the
+ * particle-mesh removal loop), "pm_solves" (halo-grid
  * convolutions over all passes), "pm_fft_bytes" (their algorithmic bytes:
  * 4 s (n+2) n^2 per solve on an n^3 grid of s-byte reals: a read and a
  * write of the padded grid per transform, two transforms). */
@@ -108,7 +109,11 @@ int32_t pyfof_last_link_ms(float *ms);
  * "link" (the linking kernel), "fof" (binning, linking and labelling up to
  * the candidate list), "unbind" (unbinding and outputs with bound_check, the
  * ang_mom pass without), "call" (all of it), "pm_fft" (the particle-mesh
- * convolutions, summed over all solves); after a host-memory call also
+ * convolutions, summed over all solves), "pm_gaps" (device idle time
+ * between the passes of the particle-mesh removal loop, while the host reads
+ * a pass's results and launches the next), "before_link" / "after_link"
+ * (the parts of "fof" before and after the linking kernel); after a
+ * host-memory call also
  * "h2d_positions" (the copy of xp), "h2d_inputs" (from the first copy to the
  * end of the last input copy), "d2h" (the output copy after the device work)
  * and "host_call" (from the first input copy to the end of the output copy). */

@@ -240,6 +240,8 @@ static void record_stage_times(Context &ctx) {
   cudaEventElapsedTime(&ctx.stage_ms[2], ctx.ev[3], ctx.ev[4]);
   cudaEventElapsedTime(&ctx.stage_ms[3], ctx.ev[2], ctx.ev[4]);
   ctx.stage_ms[4] = (float)ctx.conv_timer.ms;
+  ctx.gap_timer.collect();
+  ctx.stage_ms[11] = (float)ctx.gap_timer.ms;
   // the part of "fof" before and after the (last region's) linking kernel
   cudaEventElapsedTime(&ctx.stage_ms[9], ctx.ev[2], ctx.ev[0]);
   cudaEventElapsedTime(&ctx.stage_ms[10], ctx.ev[1], ctx.ev[3]);
@@ -398,6 +400,7 @@ static int32_t context_stat(const Context *c, const char *key, int64_t *value) {
   if (!std::strcmp(key, "pm_halos")) { *value = c->last_pm; return kOk; }
   if (!std::strcmp(key, "valid_halos")) { *value = c->last_valid; return kOk; }
   if (!std::strcmp(key, "refined_regions")) { *value = c->last_tl_regions; return kOk; }
+  if (!std::strcmp(key, "pm_passes")) { *value = c->last_pm_passes; return kOk; }
   if (!std::strcmp(key, "pm_solves")) { *value = c->last_pm_solves; return kOk; }
   if (!std::strcmp(key, "pm_fft_bytes")) { *value = (int64_t)c->last_pm_fft_bytes; return kOk; }
   if (!std::strcmp(key, "peak_bytes")) { *value = c->last_peak_bytes; return kOk; }
@@ -427,10 +430,10 @@ int32_t pyfof_last_stage_ms(const char *stage, float *ms) {
     return kInvalid;
   }
   if (get_context(g_default_device, &c) != kOk) return kInvalid;
-  static const char *names[11] = {"link", "fof", "unbind", "call", "pm_fft",
+  static const char *names[12] = {"link", "fof", "unbind", "call", "pm_fft",
                                   "h2d_positions", "h2d_inputs", "d2h", "host_call",
-                                  "before_link", "after_link"};
-  for (int i = 0; i < 11; ++i)
+                                  "before_link", "after_link", "pm_gaps"};
+  for (int i = 0; i < 12; ++i)
     if (!std::strcmp(stage, names[i])) {
       *ms = c->stage_ms[i];
       return kOk;

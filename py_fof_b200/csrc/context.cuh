@@ -78,6 +78,11 @@ struct Context {
   bool timing = false;
   float stage_ms[16] = {};
   GroupTimer conv_timer;  // PM convolutions (the FFT kernels) of the last call
+  // the PM pass loop's device idle time between passes (from the end of a
+  // pass's last kernel to the first launch of the next, which waits for the
+  // host to read the pass's results), and its pass count
+  GroupTimer gap_timer;
+  int64_t last_pm_passes = 0;
   // statistics of the last call: PM solves and their algorithmic FFT bytes
   // (one read and one write of the padded (n+2) n^2 grid per transform, two
   // transforms per solve)

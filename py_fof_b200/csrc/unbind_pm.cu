@@ -1934,6 +1934,8 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
     if (pend.empty()) break;
     std::vector<int32_t> pend_small;
     for (int h : pend) if (!is_big[h]) pend_small.push_back(h);
+    ++ctx.last_pm_passes;
+    if (ctx.timing && pass > 1) ctx.gap_timer.end(s);
     if (!pend_small.empty()) {
       PYFOF_TRY(upload(ctx, dpend, pend_small.data(), sizeof(int32_t) * pend_small.size(), s));
       pm_mkeep_kernel<<<(unsigned)pend_small.size(), 256, 0, s>>>(m, dH, dpend, (int)pend_small.size(), keep);
@@ -2048,6 +2050,7 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
     if (nbig) PYFOF_TRY(big_removal<R>(ctx, m, dB, nbig, dCh, nchb, dH, keep, jd, c1, phi_in, c2, phi, en, bpart,
                                        bucount, bulist, beq, nactive, (float)a.b_val, a.np_halo_min,
                                        phi_only));
+    if (ctx.timing) ctx.gap_timer.begin(s);
     PYFOF_CUDA(cudaMemcpyAsync(H.data(), dH, sizeof(PmHalo) * nh, cudaMemcpyDeviceToHost, s));
     PYFOF_CUDA(cudaMemcpyAsync(ctx.h_flags, ctx.d_flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     PYFOF_CUDA(cudaStreamSynchronize(s));
