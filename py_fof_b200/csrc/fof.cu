@@ -392,6 +392,13 @@ __device__ __forceinline__ void link_pair(int *parent, int p, int q, int &rp, in
   }
 }
 
+// Root hints: a root of q's set found earlier in the call.  Sets only
+// merge, so a hint equal to p's cached root rp means p and q already share a
+// set and the pair needs neither its distance test nor a union; any other
+// hint decides nothing (either may have been hung under a lower root since).
+// The dense kernel finds the hints of a batch of 32 sources in parallel, one
+// find per lane, instead of one dependent parent read per source and pair.
+
 // Ordered-integer image of a float (monotone: a < b  <=>  key(a) < key(b)
 // for non-NaN values), so warp min/max reductions of coordinates can use the
 // integer reduction instructions.  The map is its own inverse.
@@ -570,8 +577,10 @@ __global__ void __launch_bounds__(BLK, 3) fof_link_dense_kernel(
     int64_t nchunks, LinkParams P, DenseIndex D, int32_t *flags) {
   constexpr unsigned FULL = 0xffffffffu;
   __shared__ float4 sbuf[BLK];
+  __shared__ int shint[BLK];
   const int lane = threadIdx.x & 31;
   float4 *wbuf = sbuf + (threadIdx.x & ~31);
+  int *whint = shint + (threadIdx.x & ~31);
   const int64_t nw = ((int64_t)gridDim.x * BLK) >> 5;
   for (int64_t ch = ((int64_t)blockIdx.x * BLK + threadIdx.x) >> 5; ch < nchunks; ch += nw) {
     const DenseChunk C = chunks[ch];
@@ -648,7 +657,7 @@ __global__ void __launch_bounds__(BLK, 3) fof_link_dense_kernel(
         }
       }
     }
-    int rp = -1;  // cached root of this lane's particle
+    int rp = valid ? dsu_find(parent, ip) : -1;  // cached root of this lane's particle
     // --- cells that are one source range (sparse cells, dense cells of one
     // sub-cell): their sources packed into shared batches of 32
     {
@@ -700,6 +709,7 @@ __global__ void __launch_bounds__(BLK, 3) fof_link_dense_kernel(
           }
           o.w = __int_as_float(oown ? ~q : q);  // own-cell sources carry their flag
           wbuf[lane] = o;
+          whint[lane] = cand ? dsu_find(parent, q) : -2;
         }
         __syncwarp();
         unsigned mask = __ballot_sync(FULL, cand);
@@ -710,7 +720,7 @@ __global__ void __launch_bounds__(BLK, 3) fof_link_dense_kernel(
           const int qw = __float_as_int(so.w);
           const bool sown = qw < 0;
           const int qs = sown ? ~qw : qw;
-          if (valid && !(sown && qs <= ip)) {
+          if (valid && whint[src] != rp && !(sown && qs <= ip)) {
             const bool lk = per ? linked_pbc(me, so, P) : linked_open(me, so, P.rp2_open);
             if (lk) link_pair(parent, ip, qs, rp, flags);
           }
@@ -758,13 +768,14 @@ __global__ void __launch_bounds__(BLK, 3) fof_link_dense_kernel(
           for (int64_t base = k0; base < k1; base += 32) {
             const int64_t t = base + lane;
             float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
-            int q = -1;
+            int q = -1, hq = -2;
             bool cand = false;
             if (t < k1) {
               o = D.dpos[b + t];
               q = __float_as_int(o.w);
               cand = o.x >= wl[0] && o.x <= wh[0] && o.y >= wl[1] && o.y <= wh[1] && o.z >= wl[2] &&
                      o.z <= wh[2];
+              if (cand) hq = dsu_find(parent, q);
             }
             unsigned mask = __ballot_sync(FULL, cand);
             while (mask) {
@@ -776,7 +787,8 @@ __global__ void __launch_bounds__(BLK, 3) fof_link_dense_kernel(
               so.z = __shfl_sync(FULL, o.z, src);
               so.w = 0.f;
               const int qs = __shfl_sync(FULL, q, src);
-              if (valid && !(own_n && qs <= ip)) {
+              const int hs = __shfl_sync(FULL, hq, src);
+              if (valid && hs != rp && !(own_n && qs <= ip)) {
                 const bool lk = per ? linked_pbc(me, so, P) : linked_open(me, so, P.rp2_open);
                 if (lk) link_pair(parent, ip, qs, rp, flags);
               }
