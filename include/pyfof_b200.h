@@ -86,6 +86,16 @@ int32_t pyfof_get_tile(const char *key, int64_t index, int64_t *value);
  * its own work and time them with events on that stream. */
 int32_t pyfof_set_stream(void *stream);
 
+/* Page-locked host memory for a caller's input staging: a list of regions
+ * is concatenated into one array before the call (the reference does so in
+ * NumPy, py_fof/__init__.py:213-231); concatenated into this memory, which
+ * a caller keeps and reuses, it is not page-faulted again on every call and
+ * copies to the device at the host link's full rate.  Free with
+ * pyfof_host_free. */
+int32_t pyfof_host_alloc(int64_t bytes, void **ptr);
+int32_t pyfof_host_free(void *ptr);
+
+
 /* Counters: "launches" (kernels launched by this process so far), and for
  * the last call on the selected device "cells" (reference cell grid size),
  * "active" (particles in linked regions), "candidates" (FoF groups with at

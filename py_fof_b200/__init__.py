@@ -71,12 +71,16 @@ class FofCall:
 _MASS_ERROR = "All particle masses in mp_list must be positive and finite"
 
 
-def _as_3n(xp_list_norm):
+def _as_3n(xp_list_norm, staging=None):
     if len(xp_list_norm) == 1:
         x = xp_list_norm[0]
         if x.dtype == np.float64 and (x.flags.c_contiguous or x.flags.f_contiguous):
             return x
         return np.ascontiguousarray(x, dtype=np.float64)
+    if staging is not None:
+        out = staging.take((3, sum(x.shape[1] for x in xp_list_norm)))
+        np.concatenate(xp_list_norm, axis=1, out=out)
+        return out
     return np.ascontiguousarray(np.hstack(xp_list_norm), dtype=np.float64)
 
 
@@ -84,13 +88,16 @@ def _prepare(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2, np_halo_min
              bound_check=False, verbose=0, return_ang_mom=False, n_threads=None, mp_list=None,
              softening=None, z=0.0, box=300.0, h0=0.67, omega_m=0.3, omega_l=0.7, n_sim=None,
              units='cube', include_hubble_flow=False, ng=None, ng_global=None,
-             check_masses=True, device_units=False):
+             check_masses=True, device_units=False, staging=None):
     """Validation and unit conversion of _fof_core (py_fof/__init__.py:168-329).
 
     Returns either a FofCall or, for total_np == 0, the final empty result.
     With check_masses=False the per-particle mass check (positive and
     finite) is left to the native library, which runs it on the device and
     reports it as ierr 5; _finish raises the same ValueError for it.
+    `staging` (an _native.Staging): lists of regions are concatenated into
+    its page-locked memory instead of new arrays; the arrays of the returned
+    call are then valid until the staging's next use.
     With device_units=True the arrays stay in the caller's units and the
     call carries their conversion (FofCall.units), which the library applies
     on the device; a scalar mass then travels as that constant instead of
@@ -125,7 +132,16 @@ def _prepare(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2, np_halo_min
         return (np.zeros(0, dtype=bool), np.zeros(0, dtype=np.int32),
                 np.zeros((3, nhalo), dtype=np.float64))
 
-    xp_halo = _as_3n(xp_list_norm)
+    if staging is not None:
+        multi = len(xp_list_norm) > 1
+        need = 24 * total_np if multi else 0
+        if multi and isinstance(vp_list, (list, tuple)):
+            need += 24 * total_np
+        if isinstance(mp_list, (list, tuple)):
+            need += 8 * total_np
+        if not staging.reserve(need + 1024):
+            staging = None
+    xp_halo = _as_3n(xp_list_norm, staging)
 
     if bound_check and vp_list is None:
         raise ValueError("vp_list is required when bound_check=True")
@@ -145,7 +161,7 @@ def _prepare(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2, np_halo_min
             if not isinstance(vp, np.ndarray) or vp.ndim != 2 or vp.shape != xp_list_norm[i].shape:
                 raise ValueError(f"vp_list[{i}] shape {getattr(vp, 'shape', None)} must match xp_list[{i}] shape {xp_list_norm[i].shape}")
 
-        vp_halo = _as_3n(vp_list_norm)
+        vp_halo = _as_3n(vp_list_norm, staging)
     else:
         vp_halo = None  # the reference passes zeros (py_fof/__init__.py:233)
 
@@ -169,7 +185,11 @@ def _prepare(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2, np_halo_min
                 raise ValueError(f"mp_list 1D array length ({len(mp_list)}) does not match total particles ({total_np})")
         elif isinstance(mp_list, (list, tuple)):
             if len(mp_list) == nhalo and all(isinstance(m, np.ndarray) and m.ndim == 1 and len(m) == np_halo[i] for i, m in enumerate(mp_list)):
-                mp_raw = np.concatenate(mp_list).astype(np.float64)
+                if staging is not None:
+                    mp_raw = staging.take((total_np,))
+                    np.concatenate(mp_list, out=mp_raw)
+                else:
+                    mp_raw = np.concatenate(mp_list).astype(np.float64)
             elif len(mp_list) == nhalo and all(np.isscalar(m) for m in mp_list):
                 scalars = np.array([float(m) for m in mp_list], dtype=np.float64)
                 mp_raw = np.repeat(scalars, np_halo)
@@ -300,7 +320,7 @@ def _native_call(call: FofCall, mask_only=False):
 def _run_public(mask_only, **kw):
     """_prepare, the native call and _finish; with `mask_only` the library
     returns in_halo alone (halo_id is None), which is all fof() needs."""
-    call = _prepare(check_masses=False, device_units=True, **kw)
+    call = _prepare(check_masses=False, device_units=True, staging=_native.thread_staging(), **kw)
     if not isinstance(call, FofCall):
         return call
     in_halo, halo_id, ang_mom, ierr = _native_call(call, mask_only=mask_only)
@@ -401,7 +421,7 @@ def fof_with_info(xp_list, vp_list=None, L_Box=512.0, linking_length=0.2,
                     softening=softening, z=z, box=box, h0=h0, omega_m=omega_m,
                     omega_l=omega_l, n_sim=n_sim, units=units,
                     include_hubble_flow=include_hubble_flow, ng=ng, ng_global=ng_global,
-                    check_masses=False, device_units=True)
+                    check_masses=False, device_units=True, staging=_native.thread_staging())
     if not isinstance(call, FofCall):
         return catalogue_from_ids(*call, return_ang_mom=return_ang_mom)
     return _catalogue_call(call, return_ang_mom)

@@ -47,7 +47,8 @@ EXPORTED = ("pyfof_version", "pyfof_init", "pyfof_shutdown", "pyfof_last_error",
             "pyfof_set_option", "pyfof_get_option", "pyfof_set_tile", "pyfof_get_tile", "pyfof_set_stream", "pyfof_get_stat", "pyfof_last_link_ms", "pyfof_last_stage_ms",
             "pyfof_halo_potential", "pyfof_halo_potential_direct_static", "pyfof_run",
             "pyfof_run_device", "pyfof_slot_create", "pyfof_slot_destroy", "pyfof_slot_run",
-            "pyfof_slot_stat", "pyfof_run_catalogue", "pyfof_run_units", "pyfof_run_mask")
+            "pyfof_slot_stat", "pyfof_run_catalogue", "pyfof_run_units", "pyfof_run_mask",
+            "pyfof_host_alloc", "pyfof_host_free")
 
 
 class NativeLibraryError(RuntimeError):
@@ -114,6 +115,10 @@ def load():
         L.pyfof_run_catalogue.argtypes = ([ctypes.c_void_p, ctypes.POINTER(Units)] + list(_RUN_ARGS[:19]) +
                                           [_RUN_ARGS[20], _RUN_ARGS[21], ctypes.c_void_p,
                                            ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32)])
+        L.pyfof_host_alloc.restype = ctypes.c_int32
+        L.pyfof_host_alloc.argtypes = [ctypes.c_int64, ctypes.POINTER(ctypes.c_void_p)]
+        L.pyfof_host_free.restype = ctypes.c_int32
+        L.pyfof_host_free.argtypes = [ctypes.c_void_p]
         L.pyfof_slot_stat.restype = ctypes.c_int32
         L.pyfof_slot_stat.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
         v = L.pyfof_version()
@@ -274,6 +279,66 @@ def last_stage_ms(stage: str) -> float:
     if load().pyfof_last_stage_ms(stage.encode(), ctypes.byref(v)) != 0:
         raise ValueError(last_error())
     return float(v.value)
+
+
+class Staging:
+    """Page-locked host memory that list inputs are concatenated into
+    (pyfof_host_alloc), one per thread (thread_staging).  Views handed out
+    by take() are valid until the next reserve() of the same object, which
+    the public calls make at their start: the previous call of the thread
+    has returned by then."""
+
+    def __init__(self):
+        self.ptr = None
+        self.cap = 0
+        self.used = 0
+
+    def reserve(self, nbytes):
+        """Room for `nbytes`; False when no page-locked memory could be had
+        (the caller then concatenates into ordinary arrays)."""
+        self.used = 0
+        if nbytes <= self.cap:
+            return True
+        L = load()
+        self.release()
+        cap = max(int(nbytes), 1 << 20)
+        p = ctypes.c_void_p()
+        if L.pyfof_host_alloc(cap, ctypes.byref(p)) != 0:
+            return False
+        self.ptr, self.cap = p.value, cap
+        return True
+
+    def take(self, shape):
+        """A float64 array of `shape` in the reserved memory (C order)."""
+        n = int(np.prod(shape))
+        off = (self.used + 255) // 256 * 256
+        if off + 8 * n > self.cap:
+            raise MemoryError("staging reservation exceeded")
+        self.used = off + 8 * n
+        buf = (ctypes.c_double * n).from_address(self.ptr + off)
+        return np.frombuffer(buf, dtype=np.float64, count=n).reshape(shape)
+
+    def release(self):
+        if self.ptr is not None and _lib is not None:
+            _lib.pyfof_host_free(ctypes.c_void_p(self.ptr))
+        self.ptr, self.cap, self.used = None, 0, 0
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+_tls = threading.local()
+
+
+def thread_staging():
+    """The calling thread's Staging."""
+    st = getattr(_tls, "staging", None)
+    if st is None:
+        st = _tls.staging = Staging()
+    return st
 
 
 def _ptr(a):

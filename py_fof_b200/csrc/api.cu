@@ -377,6 +377,28 @@ int32_t pyfof_get_tile(const char *key, int64_t index, int64_t *value) {
   return kOk;
 }
 
+int32_t pyfof_host_alloc(int64_t bytes, void **ptr) {
+  if (!ptr || bytes <= 0) {
+    set_error("pyfof_host_alloc: invalid arguments");
+    return kInvalid;
+  }
+  *ptr = nullptr;
+  const cudaError_t e = cudaHostAlloc(ptr, (size_t)bytes, cudaHostAllocPortable);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *ptr = nullptr;
+    set_error("pinned host allocation of %lld bytes failed: %s", (long long)bytes, cudaGetErrorString(e));
+    return kAlloc;
+  }
+  return kOk;
+}
+
+int32_t pyfof_host_free(void *ptr) {
+  if (ptr) cudaFreeHost(ptr);
+  cudaGetLastError();
+  return kOk;
+}
+
 int32_t pyfof_set_stream(void *stream) {
   Context *c;
   PYFOF_TRY(get_context(g_default_device, &c));

@@ -343,3 +343,23 @@ def test_mask_zeroed_on_failure():
     in_halo, _, am, ierr = _native.run(xp, None, None, [6], 1, 10.0, 0.2, 1, 0, 0, 0.1, 1.0, 0.0,
                                        17.152, 0, 6, mask_only=True)
     assert ierr == 4 and not in_halo.any() and not am.any()
+
+
+def test_list_inputs_through_page_locked_staging():
+    """Lists of regions (with velocity and mass lists) are concatenated into
+    the thread's page-locked staging; it is reused and grown from call to
+    call, and every call equals the oracle."""
+    rng = np.random.default_rng(33)
+    for nreg, per in ((5, 50), (40, 300), (3, 20), (60, 700)):
+        xs = [rng.normal(rng.uniform(5, 59, (3, 1)), 0.15, (3, int(rng.integers(per // 2, per + 1))))
+              for _ in range(nreg)]
+        vs = [rng.normal(0, 1, x.shape) for x in xs]
+        ms = [rng.lognormal(0, 0.2, x.shape[1]) for x in xs]
+        kw = dict(vp_list=vs, mp_list=ms, L_Box=64.0, linking_length=0.2, np_halo_min=5,
+                  return_ang_mom=True)
+        ih, am = P.fof(xs, **kw)
+        info = P.fof_with_info(xs, **kw)
+        o = oracle_core(xs, **kw)
+        assert np.array_equal(ih, o[0]) and np.array_equal(info["in_halo"], o[0])
+        assert angmom_close(am, o[2], np.abs(o[2]).max() + 1.0)
+    assert _native.thread_staging().cap > 0
