@@ -152,8 +152,8 @@ int32_t pyfof_halo_potential(const float *q, const float *w, int32_t np, double 
  * per GPU, held until exit); inputs q (3,np), w (np) and the output phi (np)
  * are host arrays as in pyfof_halo_potential; `stream` is a cudaStream_t
  * (NULL = legacy default stream).  Returns 1 for np > 1000.  The first call
- * on a device looks up the array's address (make it before any stream
- * capture); calls share the array, so calls that overlap on the GPU race. */
+ * on a device looks up the array's address; calls share the array, so calls
+ * that overlap on the GPU race. */
 int32_t pyfof_halo_potential_direct_static(const float *q, const float *w, int32_t np,
                                            double softening, double a_val, int32_t fp64,
                                            float *phi, void *stream);

@@ -13,8 +13,8 @@
 // library holds its kStaticMaxMembers-member capacity (about 42 KiB) until
 // the process exits.  Host code cannot use the symbol itself as a device
 // address; its address is looked up once per device with
-// cudaGetSymbolAddress on the first call made on that device (so make that
-// first call before any stream capture).  All calls share the one array:
+// cudaGetSymbolAddress on the first call made on that device.  All calls
+// share the one array:
 // calls that overlap on the GPU race and must be serialised by the caller
 // (the entry point itself synchronises the stream before it returns).
 #include <cstring>
