@@ -122,7 +122,10 @@ int32_t pyfof_last_link_ms(float *ms);
  * convolutions, summed over all solves), "pm_gaps" (device idle time
  * between the passes of the particle-mesh removal loop, while the host reads
  * a pass's results and launches the next), "before_link" / "after_link"
- * (the parts of "fof" before and after the linking kernel); after a
+ * (the parts of "fof" before and after the linking kernel), "direct_loops"
+ * / "pm_path" (from the fork of the direct-summation removal loops onto
+ * their side stream: the loops, and the particle-mesh halos on the call
+ * stream; 0 when nothing forked); after a
  * host-memory call also
  * "h2d_positions" (the copy of xp), "h2d_inputs" (from the first copy to the
  * end of the last input copy), "d2h" (the output copy after the device work)

@@ -242,6 +242,11 @@ static void record_stage_times(Context &ctx) {
   ctx.stage_ms[4] = (float)ctx.conv_timer.ms;
   ctx.gap_timer.collect();
   ctx.stage_ms[11] = (float)ctx.gap_timer.ms;
+  // from the fork of the direct-summation removal loops: their side stream,
+  // and the particle-mesh halos on the call stream (0 when nothing forked)
+  if (!ctx.side_timed || cudaEventElapsedTime(&ctx.stage_ms[12], ctx.ev[9], ctx.ev[10]) != cudaSuccess ||
+      cudaEventElapsedTime(&ctx.stage_ms[13], ctx.ev[9], ctx.ev[11]) != cudaSuccess)
+    ctx.stage_ms[12] = ctx.stage_ms[13] = 0.0f;
   // the part of "fof" before and after the (last region's) linking kernel
   cudaEventElapsedTime(&ctx.stage_ms[9], ctx.ev[2], ctx.ev[0]);
   cudaEventElapsedTime(&ctx.stage_ms[10], ctx.ev[1], ctx.ev[3]);
@@ -452,10 +457,11 @@ int32_t pyfof_last_stage_ms(const char *stage, float *ms) {
     return kInvalid;
   }
   if (get_context(g_default_device, &c) != kOk) return kInvalid;
-  static const char *names[12] = {"link", "fof", "unbind", "call", "pm_fft",
+  static const char *names[14] = {"link", "fof", "unbind", "call", "pm_fft",
                                   "h2d_positions", "h2d_inputs", "d2h", "host_call",
-                                  "before_link", "after_link", "pm_gaps"};
-  for (int i = 0; i < 12; ++i)
+                                  "before_link", "after_link", "pm_gaps", "direct_loops",
+                                  "pm_path"};
+  for (int i = 0; i < 14; ++i)
     if (!std::strcmp(stage, names[i])) {
       *ms = c->stage_ms[i];
       return kOk;

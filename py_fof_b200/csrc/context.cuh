@@ -73,7 +73,7 @@ struct Context {
   std::shared_ptr<GreenCache> green;
   size_t pm_budget = (size_t)8 << 30;  // particle-mesh grid batch bytes
   int64_t last_peak_bytes = 0;         // device memory the last call held at most
-  cudaEvent_t ev[10] = {};
+  cudaEvent_t ev[12] = {};
   // timing of the last call's stages (ms), filled when timing is enabled
   bool timing = false;
   float stage_ms[16] = {};
@@ -83,6 +83,7 @@ struct Context {
   // host to read the pass's results), and its pass count
   GroupTimer gap_timer;
   int64_t last_pm_passes = 0;
+  bool side_timed = false;  // ev[9..11] hold this call's fork timing
   // statistics of the last call: PM solves and their algorithmic FFT bytes
   // (one read and one write of the padded (n+2) n^2 grid per transform, two
   // transforms per solve)

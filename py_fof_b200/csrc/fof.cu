@@ -1754,6 +1754,7 @@ int32_t fof_run(Context &ctx, const FofArgs &a) {
   ctx.conv_timer.reset();
   ctx.gap_timer.reset();
   ctx.last_pm_passes = 0;
+  ctx.side_timed = false;
   ctx.last_pm_solves = 0;
   ctx.last_pm_fft_bytes = 0.0;
   if (ctx.timing) cudaEventRecord(ctx.ev[2], ctx.stream);

@@ -578,6 +578,10 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
       // particle-mesh halos on `s` (disjoint halos, disjoint outputs)
       PYFOF_TRY(fork_side(ctx, s));
       side_forked = true;
+      if (ctx.timing) {
+        cudaEventRecord(ctx.ev[9], ctx.side_stream);
+        ctx.side_timed = true;
+      }
       PYFOF_CUDA(wait_velocities(ctx, ctx.side_stream));
       for (int b = 5; b >= 0; --b) {
         const unsigned nb = (unsigned)(bstart[b + 1] - bstart[b]);
@@ -587,6 +591,7 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
                                      dbl + bstart[b], P, res, keep, st.phi_out, ctx.d_flags, phi1,
                                      ctx.side_stream));
       }
+      if (ctx.timing) cudaEventRecord(ctx.ev[10], ctx.side_stream);
       PYFOF_CUDA(cudaEventRecord(ctx.ev_join, ctx.side_stream));
     }
     PYFOF_CHECK_LAUNCH();
@@ -617,6 +622,7 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
     }
   }
   if (side_forked) {
+    if (ctx.timing) cudaEventRecord(ctx.ev[11], s);
     PYFOF_CUDA(cudaStreamWaitEvent(s, ctx.ev_join, 0));
     side_forked = false;
   }
