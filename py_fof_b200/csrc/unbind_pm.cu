@@ -557,11 +557,17 @@ __global__ void __launch_bounds__(256, 4) sr_gather_kernel(
     const uint8_t *__restrict__ pr, const SrChunk *__restrict__ chunks, int64_t nchunks,
     const uint32_t *__restrict__ cstart, const uint32_t *__restrict__ cmem, const float4 *__restrict__ src4,
     const uint32_t *__restrict__ rpos, const uint32_t *__restrict__ rsrc, double a_val, double app,
-    R *__restrict__ phi_sr) {
+    R *__restrict__ phi_sr, unsigned *__restrict__ next) {
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t ch = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; ch < nchunks; ch += nw) {
+  // chunks come heaviest first; each warp takes the next one when it is
+  // free (the sums of a chunk do not depend on which warp runs it)
+  auto fetch = [&]() -> int64_t {
+    unsigned v = 0;
+    if (lane == 0) v = atomicAdd(next, 1u);
+    return (int64_t)__shfl_sync(FULL, v, 0);
+  };
+  for (int64_t ch = fetch(); ch < nchunks; ch = fetch()) {
     const SrChunk C = chunks[ch];
     const uint32_t cend = cstart[C.cell + 1];
     const uint32_t e = C.e0 + lane;
@@ -730,6 +736,23 @@ __global__ void sr_chunk_fill_kernel(const uint32_t *__restrict__ cstart, const 
     const uint32_t n = (cstart[c + 1] - cstart[c] + 31u) / 32u;
     for (uint32_t i = 0; i < n; ++i) chunks[coff[c] + i] = SrChunk{(uint32_t)c, cstart[c] + 32u * i};
   }
+}
+
+// Work order of the target chunks: heaviest first, the weight being the
+// occupancy of the chunk's cell (the density its targets' cutoff spheres
+// sample), so the dynamically fetched chunks end together.
+__global__ void sr_chunk_key_kernel(const SrChunk *__restrict__ chunks, int64_t n,
+                                    const uint32_t *__restrict__ cstart, uint32_t *__restrict__ key) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t c = chunks[i].cell;
+    key[i] = 65535u - min(cstart[c + 1] - cstart[c], 65535u);
+  }
+}
+
+__global__ void sr_chunk_order_kernel(const SrChunk *__restrict__ chunks, const uint32_t *__restrict__ idx,
+                                      int64_t n, SrChunk *__restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = chunks[idx[i]];
 }
 
 // Members removed since the previous pass, in cell order: flag (and clear
@@ -1767,8 +1790,27 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
   PYFOF_CHECK_LAUNCH();
   sr_chunk_fill_kernel<<<gC, BLK, 0, s>>>(cstart, chcnt, ncell, chunks);
   PYFOF_CHECK_LAUNCH();
+  {
+    // heaviest chunks first (a stable sort on the 16-bit weight key)
+    const int64_t nc = std::max<uint32_t>(nchunk, 1);
+    uint32_t *ck = W.carve<uint32_t>(nc), *c1k = W.carve<uint32_t>(nc), *c1v = W.carve<uint32_t>(nc),
+             *c2k = W.carve<uint32_t>(nc), *c2v = W.carve<uint32_t>(nc);
+    SrChunk *sorted = W.carve<SrChunk>(nc);
+    if (!ck || !c1k || !c1v || !c2k || !c2v || !sorted) { set_error("workspace exhausted (C2 chunks)"); return kAlloc; }
+    const unsigned gK = (unsigned)std::min<int64_t>(ceil_div(nc, BLK), 148 * 16);
+    sr_chunk_key_kernel<<<gK, BLK, 0, s>>>(chunks, nchunk, cstart, ck);
+    PYFOF_CHECK_LAUNCH();
+    uint32_t *sk2, *order;
+    PYFOF_TRY(radix_sort_pairs(ck, nullptr, nchunk, 16, c1k, c1v, c2k, c2v, &sk2, &order, W, s));
+    sr_chunk_order_kernel<<<gK, BLK, 0, s>>>(chunks, order, nchunk, sorted);
+    PYFOF_CHECK_LAUNCH();
+    chunks = sorted;
+  }
+  unsigned *sr_next = W.carve<unsigned>(1);
+  if (!sr_next) { set_error("workspace exhausted (C2 chunks)"); return kAlloc; }
+  // persistent warps: the blocks that fit on the GPU at once (4 per SM)
   const unsigned gS = (unsigned)std::min<int64_t>(ceil_div((int64_t)std::max<uint32_t>(nchunk, 1) * 32, 256),
-                                                  148 * 32);
+                                                  148 * 4);
   // per-member refinement ratio, refined-region sources and targets
   const int na = (int)act.size();
   uint8_t *pr = W.carve<uint8_t>(M);
@@ -2025,9 +2067,10 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
         PYFOF_CHECK_LAUNCH();
       }
     }
+    PYFOF_CUDA(cudaMemsetAsync(sr_next, 0, sizeof(unsigned), s));
     if (pass == 1) {
       sr_gather_kernel<R, false><<<gS, 256, 0, s>>>(dH, mhalo, keep, pr, chunks, nchunk, cstart, cmem, src4,
-                                                    nullptr, nullptr, a.a_val, a.softening, c2);
+                                                    nullptr, nullptr, a.a_val, a.softening, c2, sr_next);
       PYFOF_CHECK_LAUNCH();
     } else {
       sr_removed_flag_kernel<<<gP, BLK, 0, s>>>(cmem, npm, jd, rflag);
@@ -2036,7 +2079,7 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
       sr_removed_fill_kernel<<<gP, BLK, 0, s>>>(rflag, rpos, npm, rsrc);
       PYFOF_CHECK_LAUNCH();
       sr_gather_kernel<R, true><<<gS, 256, 0, s>>>(dH, mhalo, keep, pr, chunks, nchunk, cstart, cmem, src4,
-                                                   rpos, rsrc, a.a_val, a.softening, c2);
+                                                   rpos, rsrc, a.a_val, a.softening, c2, sr_next);
       PYFOF_CHECK_LAUNCH();
     }
     if (!pend_small.empty()) {
