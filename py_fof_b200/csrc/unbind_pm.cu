@@ -261,37 +261,66 @@ __global__ void pm_setup_kernel(const Members m, const PmHalo *__restrict__ H,
   }
 }
 
-// u = q/spacing extent of every PM halo (bound_build_cells :3134-3138)
-__global__ void __launch_bounds__(BLK) pm_extent_kernel(const Members m, const PmHalo *__restrict__ H,
-                                                        int nh, double *__restrict__ ext) {
-  const int h = blockIdx.x;
+// u = q/spacing extent of every PM halo (bound_build_cells :3134-3138).
+// Division by the positive spacing is monotone and correctly rounded, so
+// min_k (q_k / s) = (min_k q_k) / s exactly: the members' FP32 extremes are
+// found first (order-free integer atomics on the ordered images of the
+// floats, many blocks per halo), then divided once.
+__device__ __forceinline__ uint32_t flt_to_ord(float v) {
+  const uint32_t b = __float_as_uint(v);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float ord_to_flt(uint32_t o) {
+  return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+}
+
+constexpr int64_t kExtentChunk = 16384;  // members per block
+
+// blockIdx.y = halo, blockIdx.x = chunk of its members; omin/omax (3 nh)
+// start at 0xffffffff / 0
+__global__ void __launch_bounds__(BLK) pm_extent_kernel(const Members m, const PmHalo *__restrict__ H, int nh,
+                                                        uint32_t *__restrict__ omin, uint32_t *__restrict__ omax) {
+  const int h = blockIdx.y;
   if (h >= nh) return;
   const PmHalo &p = H[h];
-  double lo[3] = {1e30, 1e30, 1e30}, hi[3] = {-1e30, -1e30, -1e30};
-  for (int64_t k = p.off + threadIdx.x; k < p.off + p.np; k += BLK)
+  const int64_t k0 = (int64_t)blockIdx.x * kExtentChunk;
+  if (k0 >= p.np) return;
+  const int64_t k1 = min((int64_t)p.np, k0 + kExtentChunk);
+  uint32_t lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, hi[3] = {0u, 0u, 0u};
+  for (int64_t k = p.off + k0 + threadIdx.x; k < p.off + k1; k += BLK)
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const double u = (double)m.q[d][k] / (double)p.spacing;
-      lo[d] = fmin(lo[d], u);
-      hi[d] = fmax(hi[d], u);
+      const uint32_t o = flt_to_ord(m.q[d][k]);
+      lo[d] = min(lo[d], o);
+      hi[d] = max(hi[d], o);
     }
-  __shared__ double slo[3][BLK / 32], shi[3][BLK / 32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
   for (int d = 0; d < 3; ++d) {
-    for (int o = 16; o > 0; o >>= 1) {
-      lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
-      hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+    lo[d] = __reduce_min_sync(0xffffffffu, lo[d]);
+    hi[d] = __reduce_max_sync(0xffffffffu, hi[d]);
+  }
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      atomicMin(&omin[3 * h + d], lo[d]);
+      atomicMax(&omax[3 * h + d], hi[d]);
     }
-    if (lane == 0) { slo[d][warp] = lo[d]; shi[d][warp] = hi[d]; }
+}
+
+__global__ void pm_extent_final_kernel(const PmHalo *__restrict__ H, int nh, const uint32_t *__restrict__ omin,
+                                       const uint32_t *__restrict__ omax, double *__restrict__ ext) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3 * nh) return;
+  const int h = i / 3, d = i % 3;
+  const PmHalo &p = H[h];
+  if (p.np <= 0) {
+    ext[6 * h + d] = 1e30;
+    ext[6 * h + 3 + d] = -1e30;
+    return;
   }
-  __syncthreads();
-  if (threadIdx.x < 3) {
-    const int d = threadIdx.x;
-    double a = slo[d][0], b = shi[d][0];
-    for (int w = 1; w < BLK / 32; ++w) { a = fmin(a, slo[d][w]); b = fmax(b, shi[d][w]); }
-    ext[6 * h + d] = a;
-    ext[6 * h + 3 + d] = b;
-  }
+  const double sp = (double)p.spacing;
+  ext[6 * h + d] = (double)ord_to_flt(omin[i]) / sp;
+  ext[6 * h + 3 + d] = (double)ord_to_flt(omax[i]) / sp;
 }
 
 // C2 cell key of every PM member (bound_build_cells :3166-3172), and a sort
@@ -1727,8 +1756,19 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
     ctx.last_tl_regions = (int64_t)act.size();
   }
   // C2 cells (3.5 grid cells)
-  pm_extent_kernel<<<nh, BLK, 0, s>>>(m, dH, nh, ext);
-  PYFOF_CHECK_LAUNCH();
+  {
+    uint32_t *omin = W.carve<uint32_t>(3 * (size_t)nh), *omax = W.carve<uint32_t>(3 * (size_t)nh);
+    if (!omin || !omax) { set_error("workspace exhausted (extents)"); return kAlloc; }
+    int64_t maxnp = 1;
+    for (int h = 0; h < nh; ++h) maxnp = std::max<int64_t>(maxnp, H[h].np);
+    PYFOF_CUDA(cudaMemsetAsync(omin, 0xff, sizeof(uint32_t) * 3 * nh, s));
+    PYFOF_CUDA(cudaMemsetAsync(omax, 0, sizeof(uint32_t) * 3 * nh, s));
+    const dim3 ge((unsigned)ceil_div(maxnp, kExtentChunk), (unsigned)nh);
+    pm_extent_kernel<<<ge, BLK, 0, s>>>(m, dH, nh, omin, omax);
+    PYFOF_CHECK_LAUNCH();
+    pm_extent_final_kernel<<<(unsigned)ceil_div(3 * (int64_t)nh, 128), 128, 0, s>>>(dH, nh, omin, omax, ext);
+    PYFOF_CHECK_LAUNCH();
+  }
   std::vector<double> hext(6 * (size_t)nh);
   PYFOF_CUDA(cudaMemcpyAsync(hext.data(), ext, sizeof(double) * 6 * nh, cudaMemcpyDeviceToHost, s));
   PYFOF_CUDA(cudaStreamSynchronize(s));
