@@ -78,48 +78,103 @@ __global__ void ub_pack_v_kernel(Coords vp, const uint32_t *__restrict__ midx, i
 }
 
 // Span and lower corner of every candidate (bound_classify :2955-2965): the
-// anchor member sits at q = 0; lo and hi start at 0.
+// anchor member sits at q = 0; lo and hi start at 0.  The FP32 extremes of
+// min/max are order-free, so many blocks per candidate (one per chunk of
+// kSpanChunk members, the (candidate, chunk) pairs of `work`) fold theirs
+// in with integer atomics on the ordered images of the floats; a
+// non-finite coordinate marks the candidate.
+constexpr int64_t kSpanChunk = 16384;
+
+__device__ __forceinline__ uint32_t span_ord(float v) {
+  const uint32_t b = __float_as_uint(v);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float span_flt(uint32_t o) {
+  return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+}
+
+// olo/ohi (3 per candidate) start at the ordered image of 0.0f, bad at 0
+__global__ void span_init_kernel(uint32_t *__restrict__ olo, uint32_t *__restrict__ ohi, int32_t *__restrict__ bad,
+                                 int ncand) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * ncand; i += gridDim.x * blockDim.x) {
+    olo[i] = ohi[i] = 0x80000000u;
+    if (i < ncand) bad[i] = 0;
+  }
+}
+
 __global__ void __launch_bounds__(BLK) ub_span_kernel(Members m, const int64_t *__restrict__ off,
-                                                      float *__restrict__ lo_out,
-                                                      float *__restrict__ span_out) {
-  const int c = blockIdx.x;
-  const int64_t b = off[c], e = off[c + 1];
-  float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
+                                                      const int2 *__restrict__ work, uint32_t *__restrict__ olo,
+                                                      uint32_t *__restrict__ ohi, int32_t *__restrict__ badc) {
+  const int c = work[blockIdx.x].x;
+  const int64_t b = off[c] + (int64_t)work[blockIdx.x].y * kSpanChunk;
+  const int64_t e = min(off[c + 1], b + kSpanChunk);
+  uint32_t lo[3] = {0x80000000u, 0x80000000u, 0x80000000u}, hi[3] = {0x80000000u, 0x80000000u, 0x80000000u};
   bool bad = false;
   for (int64_t k = b + threadIdx.x; k < e; k += BLK)
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const float v = m.q[d][k];
-      bad |= !isfinite(v);
-      lo[d] = fminf(lo[d], v);
-      hi[d] = fmaxf(hi[d], v);
+      if (!isfinite(v)) {
+        bad = true;
+        continue;
+      }
+      const uint32_t o = span_ord(v);
+      lo[d] = min(lo[d], o);
+      hi[d] = max(hi[d], o);
     }
-  __shared__ float slo[3][BLK / 32], shi[3][BLK / 32];
-  __shared__ int sbad;
-  if (threadIdx.x == 0) sbad = 0;
-  __syncthreads();
-  if (bad) sbad = 1;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    for (int o = 16; o > 0; o >>= 1) {
-      lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
-      hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
-    }
-    if (lane == 0) { slo[d][warp] = lo[d]; shi[d][warp] = hi[d]; }
+    lo[d] = __reduce_min_sync(0xffffffffu, lo[d]);
+    hi[d] = __reduce_max_sync(0xffffffffu, hi[d]);
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  bad = __any_sync(0xffffffffu, bad);
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      atomicMin(&olo[3 * c + d], lo[d]);
+      atomicMax(&ohi[3 * c + d], hi[d]);
+    }
+    if (bad) atomicOr(&badc[c], 1);
+  }
+}
+
+__global__ void ub_span_final_kernel(const uint32_t *__restrict__ olo, const uint32_t *__restrict__ ohi,
+                                     const int32_t *__restrict__ bad, int ncand, float *__restrict__ lo_out,
+                                     float *__restrict__ span_out) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncand; c += gridDim.x * blockDim.x) {
     float span = 0.f;
     for (int d = 0; d < 3; ++d) {
-      float a = slo[d][0], z = shi[d][0];
-      for (int w = 1; w < BLK / 32; ++w) { a = fminf(a, slo[d][w]); z = fmaxf(z, shi[d][w]); }
+      const float a = span_flt(olo[3 * c + d]), z = span_flt(ohi[3 * c + d]);
       lo_out[3 * c + d] = a;
-      const float s = z - a;
-      span = d == 0 ? s : fmaxf(span, s);
+      const float sd = z - a;
+      span = d == 0 ? sd : fmaxf(span, sd);
     }
-    span_out[c] = sbad ? NAN : span;
+    span_out[c] = bad[c] ? NAN : span;
   }
+}
+
+// Launches the span kernels for candidates with member counts np (host).
+static int32_t candidate_spans(Context &ctx, const Members &m, const int64_t *off, const int32_t *np, int ncand,
+                               float *lo, float *span, cudaStream_t s) {
+  Arena &W = ctx.work;
+  std::vector<int2> work;
+  for (int c = 0; c < ncand; ++c)
+    for (int64_t k = 0; k * kSpanChunk < std::max<int64_t>(np[c], 1); ++k) work.push_back(make_int2(c, (int)k));
+  uint32_t *olo = W.carve<uint32_t>(3 * (size_t)ncand), *ohi = W.carve<uint32_t>(3 * (size_t)ncand);
+  int32_t *bad = W.carve<int32_t>(ncand);
+  int2 *dwork = W.carve<int2>(std::max<size_t>(work.size(), 1));
+  if (!olo || !ohi || !bad || !dwork) { set_error("workspace exhausted (spans)"); return kAlloc; }
+  PYFOF_TRY(upload(ctx, dwork, work.data(), sizeof(int2) * work.size(), s));
+  const unsigned g = (unsigned)std::min<int64_t>(ceil_div(3 * (int64_t)ncand, BLK), (int64_t)kNumSMs * 8);
+  span_init_kernel<<<g, BLK, 0, s>>>(olo, ohi, bad, ncand);
+  PYFOF_CHECK_LAUNCH();
+  if (!work.empty()) {
+    ub_span_kernel<<<(unsigned)work.size(), BLK, 0, s>>>(m, off, dwork, olo, ohi, bad);
+    PYFOF_CHECK_LAUNCH();
+  }
+  ub_span_final_kernel<<<g, BLK, 0, s>>>(olo, ohi, bad, ncand, lo, span);
+  PYFOF_CHECK_LAUNCH();
+  return kOk;
 }
 
 // ---------------------------------------------------------------- direct
@@ -464,8 +519,7 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
     ub_pack_v_kernel<<<grid_m, BLK, 0, s>>>(vp, midx, M, m);
     PYFOF_CHECK_LAUNCH();
   }
-  ub_span_kernel<<<ncand, BLK, 0, s>>>(m, off, lo, span);
-  PYFOF_CHECK_LAUNCH();
+  PYFOF_TRY(candidate_spans(ctx, m, off, cnp.data(), ncand, lo, span, s));
 
   // 2. classification, in candidate order (first error wins)
   std::vector<float> hlo(3 * (size_t)ncand), hspan(ncand);
@@ -710,8 +764,7 @@ int32_t unbind_potential(Context &ctx, const float *q_soa, const float *w, int32
   PYFOF_CUDA(cudaMemcpyAsync(m.w, w, sizeof(float) * np, cudaMemcpyHostToDevice, s));
   const int64_t hoff[2] = {0, np};
   PYFOF_CUDA(cudaMemcpyAsync(off, hoff, sizeof(hoff), cudaMemcpyHostToDevice, s));
-  ub_span_kernel<<<1, BLK, 0, s>>>(m, off, lo, span);
-  PYFOF_CHECK_LAUNCH();
+  PYFOF_TRY(candidate_spans(ctx, m, off, &np, 1, lo, span, s));
   float hlo[3], hspan;
   PYFOF_CUDA(cudaMemcpyAsync(hlo, lo, sizeof(hlo), cudaMemcpyDeviceToHost, s));
   PYFOF_CUDA(cudaMemcpyAsync(&hspan, span, sizeof(float), cudaMemcpyDeviceToHost, s));

@@ -276,14 +276,14 @@ __device__ __forceinline__ float ord_to_flt(uint32_t o) {
 
 constexpr int64_t kExtentChunk = 16384;  // members per block
 
-// blockIdx.y = halo, blockIdx.x = chunk of its members; omin/omax (3 nh)
-// start at 0xffffffff / 0
-__global__ void __launch_bounds__(BLK) pm_extent_kernel(const Members m, const PmHalo *__restrict__ H, int nh,
+// One block per (halo, chunk of kExtentChunk members) of `work`; omin/omax
+// (3 nh) start at 0xffffffff / 0
+__global__ void __launch_bounds__(BLK) pm_extent_kernel(const Members m, const PmHalo *__restrict__ H,
+                                                        const int2 *__restrict__ work,
                                                         uint32_t *__restrict__ omin, uint32_t *__restrict__ omax) {
-  const int h = blockIdx.y;
-  if (h >= nh) return;
+  const int h = work[blockIdx.x].x;
   const PmHalo &p = H[h];
-  const int64_t k0 = (int64_t)blockIdx.x * kExtentChunk;
+  const int64_t k0 = (int64_t)work[blockIdx.x].y * kExtentChunk;
   if (k0 >= p.np) return;
   const int64_t k1 = min((int64_t)p.np, k0 + kExtentChunk);
   uint32_t lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, hi[3] = {0u, 0u, 0u};
@@ -1759,13 +1759,18 @@ int32_t run_pm(Context &ctx, const FofArgs &a, const GridRules &rules, const Mem
   {
     uint32_t *omin = W.carve<uint32_t>(3 * (size_t)nh), *omax = W.carve<uint32_t>(3 * (size_t)nh);
     if (!omin || !omax) { set_error("workspace exhausted (extents)"); return kAlloc; }
-    int64_t maxnp = 1;
-    for (int h = 0; h < nh; ++h) maxnp = std::max<int64_t>(maxnp, H[h].np);
+    std::vector<int2> work;
+    for (int h = 0; h < nh; ++h)
+      for (int64_t c = 0; c * kExtentChunk < std::max<int64_t>(H[h].np, 1); ++c) work.push_back(make_int2(h, (int)c));
+    int2 *dwork = W.carve<int2>(work.size());
+    if (!dwork) { set_error("workspace exhausted (extents)"); return kAlloc; }
+    PYFOF_TRY(upload(ctx, dwork, work.data(), sizeof(int2) * work.size(), s));
     PYFOF_CUDA(cudaMemsetAsync(omin, 0xff, sizeof(uint32_t) * 3 * nh, s));
     PYFOF_CUDA(cudaMemsetAsync(omax, 0, sizeof(uint32_t) * 3 * nh, s));
-    const dim3 ge((unsigned)ceil_div(maxnp, kExtentChunk), (unsigned)nh);
-    pm_extent_kernel<<<ge, BLK, 0, s>>>(m, dH, nh, omin, omax);
-    PYFOF_CHECK_LAUNCH();
+    if (!work.empty()) {
+      pm_extent_kernel<<<(unsigned)work.size(), BLK, 0, s>>>(m, dH, dwork, omin, omax);
+      PYFOF_CHECK_LAUNCH();
+    }
     pm_extent_final_kernel<<<(unsigned)ceil_div(3 * (int64_t)nh, 128), 128, 0, s>>>(dH, nh, omin, omax, ext);
     PYFOF_CHECK_LAUNCH();
   }
