@@ -590,6 +590,7 @@ int32_t unbind_stage(Context &ctx, const FofArgs &a, FofState &st) {
       // plain baseline: one halo per launch, waited for before the next
       PYFOF_CUDA(cudaFuncSetAttribute(direct::ub_direct_kernel<true>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      PYFOF_CUDA(wait_velocities(ctx, s));
       for (size_t i = 0; i < direct.size(); ++i) {
         direct::ub_direct_kernel<true><<<1, BLK, smem, s>>>(m, off, dl + i, P, res, keep, st.phi_out,
                                                             ctx.d_flags);
