@@ -119,3 +119,59 @@ def test_catalogue_from_ids():
     assert res["nhalo_found"] == 3
     assert [list(h) for h in res["halo_indices"]] == [[2, 5], [1, 3], [6]]
     assert list(res["np_per_halo"]) == [2, 2, 1]
+
+
+class _HostStaging:
+    """Stand-in for _native.Staging with ordinary memory: the same reserve /
+    take contract (views into one buffer, reset by reserve)."""
+
+    def __init__(self):
+        self.buf = np.zeros(0, np.uint8)
+        self.used = 0
+        self.reserved = []
+
+    def reserve(self, nbytes):
+        self.reserved.append(nbytes)
+        self.used = 0
+        if nbytes > self.buf.size:
+            self.buf = np.zeros(nbytes, np.uint8)
+        return True
+
+    def take(self, shape):
+        n = int(np.prod(shape))
+        off = (self.used + 255) // 256 * 256
+        assert off + 8 * n <= self.buf.size
+        self.used = off + 8 * n
+        return self.buf[off:off + 8 * n].view(np.float64).reshape(shape)
+
+
+def test_list_inputs_concatenated_into_staging():
+    """Lists of regions (positions, velocities, masses) land in the staging
+    buffer with the values np.hstack gives; single arrays are not copied."""
+    rng = np.random.default_rng(5)
+    xs = [rng.normal(size=(3, int(k))) for k in rng.integers(1, 400, 25)]
+    vs = [rng.normal(size=x.shape) for x in xs]
+    ms = [rng.uniform(0.5, 2.0, x.shape[1]) for x in xs]
+    kw = dict(vp_list=vs, mp_list=ms, L_Box=50.0, bound_check=True, softening=0.1,
+              check_masses=False, device_units=True)
+    plain = P._prepare(xs, **kw)
+    st = _HostStaging()
+    staged = P._prepare(xs, staging=st, **kw)
+    n = sum(x.shape[1] for x in xs)
+    assert st.reserved and st.reserved[-1] >= 56 * n
+    for a, b in ((plain.xp, staged.xp), (plain.vp, staged.vp), (plain.mp, staged.mp)):
+        assert np.array_equal(a, b)
+    for arr in (staged.xp, staged.vp, staged.mp):
+        assert np.shares_memory(arr, st.buf)
+    # one array: used as it is
+    one = P._prepare(xs[0], L_Box=50.0, staging=_HostStaging(), device_units=True)
+    assert one.xp is xs[0] or np.shares_memory(one.xp, xs[0])
+
+
+def test_staging_unavailable_falls_back():
+    class _NoStaging(_HostStaging):
+        def reserve(self, nbytes):
+            return False
+    xs = [np.ones((3, 4)), np.zeros((3, 6))]
+    c = P._prepare(xs, L_Box=10.0, staging=_NoStaging(), device_units=True)
+    assert np.array_equal(c.xp, np.hstack(xs))
